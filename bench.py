@@ -1,0 +1,366 @@
+"""Benchmark: 32-qubit random circuit on one B200 (and N replicas on N GPUs).
+
+Workload: 32 qubits, complex64 state (32 GiB, far larger than L2, so no flush
+between steps), depth 16; each layer an RX/RY/RZ on every qubit (axis and
+angle seeded) then a two-qubit gate on every pair of a seeded random perfect
+matching: CNOT, or iSWAP on 10% of the pairs.  768 gates.
+
+A step = reset to |0...0> and run the whole circuit.  `value` is circuits per
+second over all ranks (each rank runs its own replica: the state does not
+shard at 32 qubits); `e2e` is the same metric through the C ABI with the gate
+list and the shot uniforms copied from pinned host memory each step and 1024
+sampled bitstrings copied back.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--path plain|fused]
+  python bench.py --impl reference      # the reference CPU backend on the host
+"""
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "32q random-circuit time & HBM GB/s: fused-TC vs plain per-gate, 1 B200, fid≥1-1e-6"
+N_QUBITS, DEPTH, ISWAP_FRAC, SEED = 32, 16, 0.1, 20240601
+SHOTS = 1024
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--path", default="plain", choices=["plain", "fused"])
+    ap.add_argument("--qubits", type=int, default=N_QUBITS)
+    ap.add_argument("--depth", type=int, default=DEPTH)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+# ----------------------------------------------------------------- distributed
+def dist_setup():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def dist_init(ws, backend):
+    import datetime
+
+    import torch.distributed as dist
+    if ws > 1 and not dist.is_initialized():
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
+
+
+def barrier(ws):
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(x, ws, device=None):
+    if ws == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ----------------------------------------------------------------- clocks
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_id):
+        self.proc = None
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "--query-gpu=" + self.FIELDS, "--format=csv,noheader,nounits",
+                 "-lms", "200", "-i", str(gpu_id)],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        out, _ = self.proc.communicate(timeout=10)
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.strip().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ----------------------------------------------------------------- workload
+def workload(n, depth):
+    from qpanda_b200 import circuits
+    return circuits.random_layers(n, depth, SEED, iswap_frac=ISWAP_FRAC)
+
+
+def kernel_kind(g):
+    from qpanda_b200.capi import OP
+    op = int(g["op"])
+    if op in (OP["H"], OP["X"], OP["RX"], OP["RY"], OP["RZ"]) and int(g["nctrl"]) == 0:
+        return "k_pair (1-qubit, dense 2x2)"
+    if op in (OP["CNOT"], OP["ISWAP"], OP["SQISWAP"], OP["SWAP"], OP["TOFFOLI"], OP["CSWAP"]):
+        return "k_pair (controlled / exchange)"
+    if op == OP["CR"]:
+        return "k_phase"
+    return "other"
+
+
+def load_traffic():
+    """Per-launch DRAM traffic of the bench kernels from the committed ncu
+    summary (profiles/traffic.json), or None."""
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    try:
+        with open(p) as f:
+            return json.load(f)
+    except Exception:
+        return None
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+# ----------------------------------------------------------------- reference arm
+def cpu_reference_sample(n_sample, layers_sample, omp=True):
+    """Time the reference CPU backend (compiled from its sources) on a sample of
+    the workload: the same layer structure at n_sample qubits, layers_sample
+    layers, complex128 (its only precision).  Returns seconds."""
+    from oracle.pyoracle import RefState, ref_available
+    from qpanda_b200 import circuits
+    if not ref_available(omp):
+        raise FileNotFoundError("oracle/_ref not built")
+    g = circuits.random_layers(n_sample, layers_sample, SEED, iswap_frac=ISWAP_FRAC)
+    r = RefState(n_sample, omp=omp)
+    t0 = time.perf_counter()
+    r.apply(g)
+    return time.perf_counter() - t0
+
+
+def cpu_baseline_entry(n, depth, n_sample=26, layers_sample=2):
+    cores = os.cpu_count() or 1
+    secs = cpu_reference_sample(n_sample, layers_sample, omp=True)
+    scale = (2 ** (n - n_sample)) * (depth / layers_sample)
+    circuit_s = secs * scale
+    return {"value": 1.0 / circuit_s, "unit": "circuits/s", "cores": cores, "kind": "reference",
+            "sample": (f"reference CPUQuantumGates.cpp (-O3 -fopenmp, {cores} threads, complex128) on the "
+                       f"same layer structure at {n_sample} qubits x {layers_sample} layers: {secs:.2f} s; "
+                       f"extrapolated x{scale:.0f} (state size 2^{n - n_sample}, layers {depth}/{layers_sample}) "
+                       f"to {circuit_s:.0f} s per {n}-qubit circuit; a {n}-qubit complex128 state "
+                       f"({16 << n >> 30} GiB) does not fit the host and the reference caps programs at 30 qubits")}
+
+
+def run_reference(args):
+    ws, rank, _ = dist_setup()
+    if rank != 0:
+        return
+    n, depth = args.qubits, args.depth
+    n_sample, layers_sample = 24, 2
+    cores = os.cpu_count() or 1
+    times = []
+    for i in range(args.warmup + args.steps):
+        t = cpu_reference_sample(n_sample, layers_sample, omp=True)
+        if i >= args.warmup:
+            times.append(t)
+    scale = (2 ** (n - n_sample)) * (depth / layers_sample)
+    circuit_s = statistics.median(times) * scale
+    value = 1.0 / circuit_s
+    sample = (f"reference CPUQuantumGates.cpp (-O3 -fopenmp, {cores} threads, complex128); each step = "
+              f"{n_sample} qubits x {layers_sample} layers of the same circuit structure, "
+              f"extrapolated x{scale:.0f} to a {n}-qubit depth-{depth} circuit")
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "circuits/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": statistics.median(times) * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": f"random-circuit-{n}q-depth{depth}", "qubits": n, "depth": depth,
+                   "iswap_frac": ISWAP_FRAC, "seed": SEED, "sample_qubits": n_sample,
+                   "sample_layers": layers_sample},
+        "cpu_baseline": {"value": value, "unit": "circuits/s", "cores": cores, "kind": "reference",
+                         "sample": sample},
+        "e2e": {"value": value, "unit": "circuits/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }))
+
+
+# ----------------------------------------------------------------- B200 arm
+def run_b200(args):
+    import torch
+    ws, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    dist_init(ws, "nccl")
+    from qpanda_b200 import StateVector, circuits, lib
+    from qpanda_b200.capi import GATE_DTYPE, check
+    import ctypes as C
+
+    n, depth = args.qubits, args.depth
+    gates = workload(n, depth)
+    ng = len(gates)
+    amp_b = 8
+    sv = StateVector(n, "c64")
+    L = lib()
+    h = sv.handle
+    stream = torch.cuda.current_stream()
+    gptr = [gates[i:i + 1].ctypes.data for i in range(ng)]
+
+    def step(events=None):
+        check(L.qs_reset_zero(h))
+        for i in range(ng):
+            check(L.qs_gate_apply(h, C.c_void_p(gptr[i])))
+            if events is not None:
+                events[i].record(stream)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+
+    # timed region
+    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(ng)] for _ in range(args.steps)]
+    start = torch.cuda.Event(enable_timing=True)
+    end = torch.cuda.Event(enable_timing=True)
+    barrier(ws)
+    torch.cuda.synchronize()
+    props = torch.cuda.get_device_properties(local)
+    gpu_id = "GPU-" + str(props.uuid) if getattr(props, "uuid", None) else str(local)
+    clocks = ClockSampler(gpu_id)
+    start.record(stream)
+    step_starts = []
+    for k in range(args.steps):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        step_starts.append(e0)
+        step(ev[k])
+    end.record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    barrier(ws)
+    elapsed = start.elapsed_time(end) / 1e3
+    elapsed = max_over_ranks(elapsed, ws, device=f"cuda:{local}")
+    launches = args.steps * (ng + 1)
+
+    # per-kernel durations from the events inside the timed region
+    kinds = {}
+    for k in range(args.steps):
+        prev = step_starts[k]
+        for i in range(ng):
+            dt = prev.elapsed_time(ev[k][i]) / 1e3
+            prev = ev[k][i]
+            kinds.setdefault(kernel_kind(gates[i]), []).append(dt)
+    dom = "k_pair (1-qubit, dense 2x2)"
+    dom_t = statistics.mean(kinds[dom])
+    dom_bytes = 2 * amp_b * (1 << n)          # algorithmic: read + write every amplitude
+    peak, peak_kind = peaks()
+    achieved = dom_bytes / dom_t / 1e9
+    traffic = None
+    tr = load_traffic()
+    if tr and dom in tr.get("kernels", {}):
+        traffic = tr["kernels"][dom]["bytes_per_launch_at_32q"]
+
+    circuit_s = elapsed / args.steps
+    alg_bytes = circuits.gate_bytes(gates, n, amp_b)
+
+    # e2e through the C ABI with host buffers
+    import torch as _t
+    pin_g = _t.empty(gates.nbytes, dtype=_t.uint8).pin_memory()
+    pin_g.numpy()[:] = np.frombuffer(gates.tobytes(), dtype=np.uint8)
+    qs = np.arange(n, dtype=np.int32)
+    rng = np.random.default_rng(SEED)
+    pin_u = _t.empty(SHOTS * n, dtype=_t.float64).pin_memory()
+    pin_u.numpy()[:] = rng.uniform(size=SHOTS * n)
+    pin_o = _t.empty(SHOTS, dtype=_t.int64).pin_memory()
+    e2e_steps = max(1, min(args.steps, 2))
+    barrier(ws)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        check(L.qs_reset_zero(h))
+        check(L.qs_gates_apply(h, C.c_void_p(pin_g.data_ptr()), ng))
+        check(L.qs_sample(h, qs.ctypes.data_as(C.POINTER(C.c_int)), n,
+                          C.cast(C.c_void_p(pin_u.data_ptr()), C.POINTER(C.c_double)), SHOTS,
+                          C.cast(C.c_void_p(pin_o.data_ptr()), C.POINTER(C.c_uint64))))
+    torch.cuda.synchronize()
+    e2e_s = (time.perf_counter() - t0) / e2e_steps
+    e2e_s = max_over_ranks(e2e_s, ws, device=f"cuda:{local}")
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        try:
+            cpu = cpu_baseline_entry(n, depth)
+        except Exception as ex:   # the reference build is absent
+            cpu = {"value": None, "unit": "circuits/s", "cores": os.cpu_count(), "kind": "reference",
+                   "sample": f"unavailable: {ex}"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": ws / circuit_s, "unit": "circuits/s", "n_gpus": ws,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": circuit_s * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic",
+            "config": {"workload": f"random-circuit-{n}q-depth{depth}-c64", "qubits": n, "depth": depth,
+                       "gates": ng, "iswap_frac": ISWAP_FRAC, "seed": SEED, "path": args.path,
+                       "state_bytes": amp_b << n, "l2": "inputs larger than L2 (32 GiB state), no flush",
+                       "parallelism": f"replicas x{ws}"},
+            "circuit_s": circuit_s,
+            "hbm_gbs_effective": alg_bytes / circuit_s / 1e9,
+            "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_source": peak_kind, "traffic": traffic,
+                         "algorithmic_bytes_per_launch": dom_bytes, "launch_s": dom_t},
+            "kernels": {k: {"launches": len(v), "mean_ms": statistics.mean(v) * 1e3,
+                            "share": sum(v) / sum(sum(x) for x in kinds.values())} for k, v in kinds.items()},
+            "cpu_baseline": cpu,
+            "e2e": {"value": ws / e2e_s, "unit": "circuits/s", "h2d_bytes_per_step": int(gates.nbytes + SHOTS * n * 8),
+                    "d2h_bytes_per_step": SHOTS * 8, "shots": SHOTS},
+            "gpu_launches": launches,
+            "clocks": clk,
+        }
+        print(json.dumps(line))
+    sv.close()
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_b200(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,175 @@
+/*
+ * qpanda_b200.h - C ABI of the B200 state-vector gate backend.
+ *
+ * This is the thin, plain-C layer between the C++ host code (the QuantumGates
+ * subclass in qpanda_b200/host/) and the sm_100a CUDA kernels.  Every entry
+ * point takes plain pointers and sizes; no C++ or torch types cross it.
+ *
+ * Each entry point below cites the reference interface it replaces, as
+ * "path:line" inside the QPanda 2018 SDK tree (QPandaSDK/...).  The reference
+ * reached its GPU code through dlsym() by name with C++ reference arguments
+ * (QPandaSDK/GPUEmulator/GPUGatesDecl.h:38-75); this header replaces that
+ * with a real extern "C" ABI.
+ *
+ * Conventions
+ *  - Qubit q is bit q of the amplitude index (little-endian), as in
+ *    QPandaSDK/QuantumInstructionHandle/CPUQuantumGates.cpp.
+ *  - Amplitudes are interleaved complex (re, im): complex64 = 2 x float,
+ *    complex128 = 2 x double.
+ *  - Return value: QS_OK (0) on success, a negative QS_ERR_* code otherwise;
+ *    qs_last_error() then holds a message for the calling thread.
+ *  - Calls that return host-visible results (measure, probabilities, samples,
+ *    get_state, norms) synchronize the state's stream.  Gate calls are
+ *    asynchronous on that stream; an error in an asynchronous kernel is
+ *    reported by the next synchronizing call.
+ */
+#ifndef QPANDA_B200_H
+#define QPANDA_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define QS_OK               0
+#define QS_ERR_ARG         -1   /* bad argument: qubit out of range, duplicate qubit, bad dtype */
+#define QS_ERR_CUDA        -2   /* CUDA runtime error */
+#define QS_ERR_OOM         -3   /* device memory exhausted */
+#define QS_ERR_UNSUPPORTED -4   /* valid request this build does not provide */
+#define QS_ERR_NOT_UNITARY -5   /* matrix failed the |det|==1 check (CPUQuantumGates.cpp:1182-1186) */
+#define QS_ERR_STATE       -6   /* state handle is unusable (e.g. a measured probability of 0) */
+
+/* ---- element types ----------------------------------------------------- */
+#define QS_C64   0              /* complex64: float re, float im  */
+#define QS_C128  1              /* complex128: double re, double im */
+
+/* ---- gate records (one per reference QuantumGates method) -------------- */
+/* Operation codes.  Each names the QuantumGates virtual it reproduces
+ * (QPandaSDK/QuantumInstructionHandle/QuantumGates.h). */
+#define QS_OP_H         1   /* Hadamard(qn)                         QuantumGates.h:56,87   */
+#define QS_OP_X         2   /* NOT(qn)                              QuantumGates.h:396,409 */
+#define QS_OP_RX        3   /* RX(qn, theta, dagger)                QuantumGates.h:115,146 */
+#define QS_OP_RY        4   /* RY(qn, theta, dagger)                QuantumGates.h:163,176 */
+#define QS_OP_RZ        5   /* RZ(qn, theta, dagger)                QuantumGates.h:194,211 */
+#define QS_OP_CNOT      6   /* CNOT(q[0]=control, q[1]=target)      QuantumGates.h:229,242 */
+#define QS_OP_CR        7   /* CR(q[0], q[1], theta, dagger)        QuantumGates.h:261     */
+#define QS_OP_ISWAP     8   /* iSWAP(q[0], q[1], dagger)            QuantumGates.h:274,292 */
+#define QS_OP_SQISWAP   9   /* sqiSWAP(q[0], q[1], dagger)          QuantumGates.h:310,328 */
+#define QS_OP_TOFFOLI  10   /* toffoli(q[0], q[1] controls, q[2])   QuantumGates.h:425     */
+#define QS_OP_CSWAP    11   /* controlSwap(q[0] control, q[1], q[2]) QuantumGates.h:345    */
+#define QS_OP_SWAP     12   /* SWAP(q[0], q[1]); no reference method: QRunes writes it as 3 CNOTs */
+
+#define QS_MAX_CTRL    16
+
+/* One gate.  q[] holds the operands in the order of the reference method's
+ * arguments; ctrl[0..nctrl) are the extra control qubits of a QRunes CONTROL
+ * block (the reference passes them with the target appended,
+ * QPandaSDK/QuantumInstructionHandle/Instruction.cpp:62,155,243); the gate then
+ * acts on the subspace where every control qubit is 1.  dagger follows the
+ * reference's iDagger argument.  96 bytes, 8-byte aligned. */
+typedef struct qs_gate {
+    int32_t op;
+    int32_t dagger;
+    int32_t q[3];
+    int32_t nctrl;
+    int32_t ctrl[QS_MAX_CTRL];
+    double  theta;
+} qs_gate;
+
+typedef struct qs_state qs_state;   /* opaque: one state vector resident in HBM */
+
+/* ---- errors ------------------------------------------------------------- */
+/* Message for the last failing call on this thread ("" if none). */
+const char *qs_last_error(void);
+/* Library build string (architecture, version). */
+const char *qs_version(void);
+
+/* ---- state lifetime ----------------------------------------------------- */
+/* Allocate 2^n_qubits amplitudes of dtype on the current CUDA device and set
+ * |0...0>.  stream: a cudaStream_t (NULL = the legacy default stream).
+ * Replaces QuantumGates::initState (QuantumGates.h:376;
+ * CPUQuantumGates.cpp:1136-1157; GPU: GPUEmulator/GPUGates.cu:1208-1299). */
+int qs_create(int n_qubits, int dtype, void *stream, qs_state **out);
+/* Free the state.  Replaces QuantumGates::destroyState (QuantumGates.h:438). */
+int qs_destroy(qs_state *s);
+int qs_num_qubits(const qs_state *s, int *n_qubits);
+int qs_dtype(const qs_state *s, int *dtype);
+/* Device address of the amplitude array (for zero-copy interop). */
+int qs_device_ptr(const qs_state *s, void **dev_ptr);
+int qs_set_stream(qs_state *s, void *stream);
+int qs_synchronize(qs_state *s);
+
+/* |0...0>.  Replaces endGate, which the dispatcher sends before every run
+ * (CPUQuantumGates.cpp:1445-1453; QuantumInstructionHandleAPI.cpp:96-100). */
+int qs_reset_zero(qs_state *s);
+/* Copy a host state in (host_dtype QS_C64 or QS_C128; converted as needed). */
+int qs_set_state(qs_state *s, const void *host_amps, int host_dtype);
+/* Copy the state out.  Replaces getQState's data path (QuantumGates.h:46;
+ * CPUQuantumGates.cpp:64-82; GPUGates.cu:2160-2169) without the 6-digit text. */
+int qs_get_state(qs_state *s, void *host_out, int host_dtype);
+
+/* ---- gates (reference conventions, CPUQuantumGates.cpp) ----------------- */
+/* Apply one gate record.  Conventions follow CPUQuantumGates.cpp: RZ is
+ * diag(e^{-i t/2}, e^{+i t/2}) (:524-570), CR multiplies |11> by e^{+i t}
+ * (:773-825), iSWAP maps |01> -> +i|10> (:838-899), H and sqiSWAP use
+ * SQ2 = 0.707106781186548 (:36).  Controlled iSWAP / sqiSWAP, which the
+ * reference leaves as no-ops (:914-922, :1054-1062), act on the control=1
+ * subspace here. */
+int qs_gate_apply(qs_state *s, const qs_gate *g);
+/* Apply count gate records in order (one launch per gate, no fusion). */
+int qs_gates_apply(qs_state *s, const qs_gate *g, size_t count);
+
+/* ---- generic unitaries (the kernels the gate records lower to) --------- */
+/* Dense 2x2 on qubit q, row-major complex m = {m00, m01, m10, m11} as 8
+ * doubles (re, im), acting where all bits of ctrl_mask are 1.  Replaces
+ * unitarySingleQubitGate (QuantumGates.h:367; CPUQuantumGates.cpp:1170-1212),
+ * whose stride is POW2(qn-1) in the reference; this entry uses 2^q. */
+int qs_apply_1q(qs_state *s, int q, const double m[8], uint64_t ctrl_mask);
+/* Same with the reference's unitarity check |det| within 1e-6 of 1. */
+int qs_apply_unitary_1q(qs_state *s, int q, const double m[8]);
+/* Dense 4x4 on (q0, q1); basis index b = bit(q0) + 2*bit(q1); row-major
+ * complex m as 32 doubles. */
+int qs_apply_2q(qs_state *s, int q0, int q1, const double m[32], uint64_t ctrl_mask);
+/* 2x2 on the pair {|a=1,b=0>, |a=0,b=1>} (iSWAP / sqiSWAP / SWAP family),
+ * m row-major over (a-set, b-set). */
+int qs_apply_exchange(qs_state *s, int a, int b, const double m[8], uint64_t ctrl_mask);
+/* Multiply every amplitude whose index has all bits of mask set by
+ * (re + i im): CR / CZ / controlled phase. */
+int qs_apply_phase(qs_state *s, uint64_t mask, double re, double im);
+
+/* ---- measurement and probabilities (FP64 accumulation) ------------------ */
+/* P(qubit q == 0) = sum |a|^2 over bit q == 0. */
+int qs_prob_zero(qs_state *s, int q, double *p0);
+/* qubitMeasure with the uniform u supplied by the caller (QuantumGates.h:356;
+ * CPUQuantumGates.cpp:1071-1126): outcome = ((float)u > p0), then the kept
+ * half is scaled by 1/sqrt(p) and the other half zeroed.  The reference draws
+ * u from its 16807 generator (QuantumGates.cpp:46-85). */
+int qs_measure(qs_state *s, int q, double u, int *outcome);
+/* Full marginal distribution over m qubits: out[idx] (2^m doubles, host),
+ * idx bit j = qubit qubits[j].  This is the un-truncated vector that
+ * pMeasure builds (QuantumGates.h:75; CPUQuantumGates.cpp:159-190). */
+int qs_probs(qs_state *s, const int *qubits, int m, double *out);
+/* pMeasure as the reference returns it: the marginal sorted by descending
+ * probability and cut to the first 10 entries (CPUQuantumGates.cpp:178-189).
+ * idx_out/p_out hold up to 10 entries; *count receives how many. */
+int qs_pmeasure(qs_state *s, const int *qubits, int m, uint64_t *idx_out,
+                double *p_out, int *count);
+/* Shots: for each shot s, measure qubits[0], qubits[1], ... in order with
+ * uniforms u[s*m + k] under qubitMeasure semantics (sequential collapse and
+ * renormalisation), without modifying the state.  out[s] bit k = outcome of
+ * qubits[k].  Equivalent to re-running the circuit once per shot with
+ * terminal MEASUREs, as QPandaSDK::run does (QPandaAPI.cpp:173-182). */
+int qs_sample(qs_state *s, const int *qubits, int m, const double *u,
+              size_t shots, uint64_t *out);
+/* sum |a|^2 */
+int qs_norm2(qs_state *s, double *norm2);
+/* <a|b> = sum conj(a_i) b_i, FP64 accumulation; a and b may differ in dtype. */
+int qs_inner(qs_state *a, qs_state *b, double *re, double *im);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* QPANDA_B200_H */

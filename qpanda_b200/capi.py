@@ -1,0 +1,217 @@
+"""ctypes binding of the C ABI in include/qpanda_b200.h.
+
+This is the Python view of the same entry points the C++ QuantumGates
+subclass calls.  It loads the in-tree library qpanda_b200/_lib/libqsb200.so and
+raises if it is missing: there is no CPU fallback.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "_lib", "libqsb200.so")
+
+QS_OK = 0
+QS_C64 = 0
+QS_C128 = 1
+
+OP = dict(H=1, X=2, RX=3, RY=4, RZ=5, CNOT=6, CR=7, ISWAP=8, SQISWAP=9, TOFFOLI=10, CSWAP=11, SWAP=12)
+MAX_CTRL = 16
+
+# struct qs_gate (96 bytes)
+GATE_DTYPE = np.dtype([("op", "<i4"), ("dagger", "<i4"), ("q", "<i4", (3,)), ("nctrl", "<i4"),
+                       ("ctrl", "<i4", (MAX_CTRL,)), ("theta", "<f8")], align=True)
+assert GATE_DTYPE.itemsize == 96
+
+
+class QSError(RuntimeError):
+    """A C-ABI call returned a non-zero status."""
+
+    def __init__(self, code, msg):
+        super().__init__(f"qpanda_b200 error {code}: {msg}")
+        self.code = code
+
+
+_lib = None
+
+
+def lib():
+    """The loaded library (loads on first use, raises if it was not built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is missing: build it with `python -m qpanda_b200.build` "
+                          "(the CUDA extension is required; there is no CPU path)")
+    L = C.CDLL(LIB_PATH)
+    vp, i, d, u64, sz = C.c_void_p, C.c_int, C.c_double, C.c_uint64, C.c_size_t
+    dp, ip = C.POINTER(C.c_double), C.POINTER(C.c_int)
+    sig = {
+        "qs_last_error": (C.c_char_p, []),
+        "qs_version": (C.c_char_p, []),
+        "qs_create": (i, [i, i, vp, C.POINTER(vp)]),
+        "qs_destroy": (i, [vp]),
+        "qs_num_qubits": (i, [vp, ip]),
+        "qs_dtype": (i, [vp, ip]),
+        "qs_device_ptr": (i, [vp, C.POINTER(vp)]),
+        "qs_set_stream": (i, [vp, vp]),
+        "qs_synchronize": (i, [vp]),
+        "qs_reset_zero": (i, [vp]),
+        "qs_set_state": (i, [vp, vp, i]),
+        "qs_get_state": (i, [vp, vp, i]),
+        "qs_gate_apply": (i, [vp, vp]),
+        "qs_gates_apply": (i, [vp, vp, sz]),
+        "qs_apply_1q": (i, [vp, i, dp, u64]),
+        "qs_apply_unitary_1q": (i, [vp, i, dp]),
+        "qs_apply_2q": (i, [vp, i, i, dp, u64]),
+        "qs_apply_exchange": (i, [vp, i, i, dp, u64]),
+        "qs_apply_phase": (i, [vp, u64, d, d]),
+        "qs_prob_zero": (i, [vp, i, dp]),
+        "qs_measure": (i, [vp, i, d, ip]),
+        "qs_probs": (i, [vp, ip, i, dp]),
+        "qs_pmeasure": (i, [vp, ip, i, C.POINTER(C.c_uint64), dp, ip]),
+        "qs_sample": (i, [vp, ip, i, dp, sz, C.POINTER(C.c_uint64)]),
+        "qs_norm2": (i, [vp, dp]),
+        "qs_inner": (i, [vp, vp, dp, dp]),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(L, name)
+        f.restype = res
+        f.argtypes = args
+    _lib = L
+    return L
+
+
+def check(code):
+    if code != QS_OK:
+        raise QSError(code, lib().qs_last_error().decode(errors="replace"))
+
+
+def _dptr(a):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def _iptr(a):
+    return a.ctypes.data_as(C.POINTER(C.c_int))
+
+
+class StateVector:
+    """One state vector resident in HBM, driven through the C ABI."""
+
+    def __init__(self, n, dtype="c64", stream=None):
+        self.n = int(n)
+        self.dtype = QS_C64 if dtype in ("c64", QS_C64, np.complex64) else QS_C128
+        h = C.c_void_p()
+        check(lib().qs_create(self.n, self.dtype, stream, C.byref(h)))
+        self._h = h
+
+    @property
+    def handle(self):
+        return self._h
+
+    def close(self):
+        if self._h:
+            lib().qs_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # -- state
+    def reset(self):
+        check(lib().qs_reset_zero(self._h))
+
+    def set_state(self, amps):
+        a = np.ascontiguousarray(amps)
+        dt = QS_C64 if a.dtype == np.complex64 else QS_C128
+        if dt == QS_C128:
+            a = np.ascontiguousarray(a, dtype=np.complex128)
+        assert a.size == (1 << self.n)
+        check(lib().qs_set_state(self._h, a.ctypes.data, dt))
+
+    def get_state(self, dtype=np.complex128):
+        out = np.empty(1 << self.n, dtype=dtype)
+        check(lib().qs_get_state(self._h, out.ctypes.data, QS_C64 if dtype == np.complex64 else QS_C128))
+        return out
+
+    def synchronize(self):
+        check(lib().qs_synchronize(self._h))
+
+    # -- gates
+    def apply(self, gates):
+        g = np.ascontiguousarray(gates, dtype=GATE_DTYPE)
+        check(lib().qs_gates_apply(self._h, g.ctypes.data, g.size))
+
+    def apply_1q(self, q, m, ctrl_mask=0):
+        m = np.ascontiguousarray(np.asarray(m, dtype=np.complex128).reshape(2, 2)).view(np.float64)
+        check(lib().qs_apply_1q(self._h, q, _dptr(m), ctrl_mask))
+
+    def apply_unitary_1q(self, q, m):
+        m = np.ascontiguousarray(np.asarray(m, dtype=np.complex128).reshape(2, 2)).view(np.float64)
+        check(lib().qs_apply_unitary_1q(self._h, q, _dptr(m)))
+
+    def apply_2q(self, q0, q1, m, ctrl_mask=0):
+        m = np.ascontiguousarray(np.asarray(m, dtype=np.complex128).reshape(4, 4)).view(np.float64)
+        check(lib().qs_apply_2q(self._h, q0, q1, _dptr(m), ctrl_mask))
+
+    def apply_exchange(self, a, b, m, ctrl_mask=0):
+        m = np.ascontiguousarray(np.asarray(m, dtype=np.complex128).reshape(2, 2)).view(np.float64)
+        check(lib().qs_apply_exchange(self._h, a, b, _dptr(m), ctrl_mask))
+
+    def apply_phase(self, mask, phase):
+        check(lib().qs_apply_phase(self._h, mask, float(np.real(phase)), float(np.imag(phase))))
+
+    # -- measurement
+    def prob_zero(self, q):
+        p = C.c_double()
+        check(lib().qs_prob_zero(self._h, q, C.byref(p)))
+        return p.value
+
+    def measure(self, q, u):
+        o = C.c_int()
+        check(lib().qs_measure(self._h, q, float(u), C.byref(o)))
+        return o.value
+
+    def probs(self, qubits=None):
+        qs = np.arange(self.n, dtype=np.int32) if qubits is None else np.asarray(qubits, dtype=np.int32)
+        out = np.empty(1 << len(qs), dtype=np.float64)
+        check(lib().qs_probs(self._h, _iptr(qs), len(qs), _dptr(out)))
+        return out
+
+    def pmeasure(self, qubits):
+        qs = np.asarray(qubits, dtype=np.int32)
+        idx = np.zeros(10, dtype=np.uint64)
+        p = np.zeros(10, dtype=np.float64)
+        cnt = C.c_int()
+        check(lib().qs_pmeasure(self._h, _iptr(qs), len(qs), idx.ctypes.data_as(C.POINTER(C.c_uint64)),
+                                _dptr(p), C.byref(cnt)))
+        return list(zip(idx[:cnt.value].tolist(), p[:cnt.value].tolist()))
+
+    def sample(self, qubits, u):
+        qs = np.asarray(qubits, dtype=np.int32)
+        u = np.ascontiguousarray(u, dtype=np.float64)
+        shots = u.size // len(qs)
+        out = np.empty(shots, dtype=np.uint64)
+        check(lib().qs_sample(self._h, _iptr(qs), len(qs), _dptr(u), shots,
+                              out.ctypes.data_as(C.POINTER(C.c_uint64))))
+        return out
+
+    def norm2(self):
+        d = C.c_double()
+        check(lib().qs_norm2(self._h, C.byref(d)))
+        return d.value
+
+    def inner(self, other):
+        re, im = C.c_double(), C.c_double()
+        check(lib().qs_inner(self._h, other._h, C.byref(re), C.byref(im)))
+        return complex(re.value, im.value)
