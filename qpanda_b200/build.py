@@ -1,8 +1,9 @@
 """Build the sm_100a CUDA library in-tree: qpanda_b200/_lib/libqsb200.so.
 
 Every .cu under qpanda_b200/csrc is compiled for sm_100a only
-(-gencode arch=compute_100a,code=sm_100a) and linked into one shared library
-that exports the C ABI declared in include/qpanda_b200.h.
+(-gencode arch=compute_100a,code=sm_100a), every host-only .cpp with g++, and
+all are linked into one shared library that exports the C ABI declared in
+include/qpanda_b200.h.
 """
 import concurrent.futures as cf
 import os
@@ -27,11 +28,19 @@ def _newer(src_list, target):
     return any(os.path.getmtime(s) > t for s in src_list)
 
 
+CXX = os.environ.get("CXX_HOST", "g++")
+CXXFLAGS = ["-O2", "-std=c++17", "-fPIC", "-Wall", "-I" + os.path.join(ROOT, "include"),
+            "-I/usr/local/cuda/include"]
+
+
 def _compile(src, deps):
     obj = os.path.join(OBJ, os.path.basename(src) + ".o")
     if not _newer([src] + deps, obj):
         return obj, None
-    cmd = [NVCC] + ARCH + FLAGS + ["-c", src, "-o", obj]
+    if src.endswith(".cpp"):
+        cmd = [CXX] + CXXFLAGS + ["-c", src, "-o", obj]
+    else:
+        cmd = [NVCC] + ARCH + FLAGS + ["-c", src, "-o", obj]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         return obj, "$ " + " ".join(cmd) + "\n" + r.stdout + r.stderr
@@ -41,7 +50,7 @@ def _compile(src, deps):
 def build(verbose=False):
     os.makedirs(OBJ, exist_ok=True)
     os.makedirs(LIB, exist_ok=True)
-    srcs = sorted(os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith(".cu"))
+    srcs = sorted(os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cu", ".cpp")))
     deps = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".h"))]
     deps.append(os.path.join(ROOT, "include", "qpanda_b200.h"))
     with cf.ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 1)) as ex:

@@ -2,16 +2,7 @@
 // gate records (QPandaSDK/QuantumInstructionHandle/QuantumGates.h methods)
 // onto the generic kernels of qs_gates.cu.
 //
-// The matrices below restate the conventions of CPUQuantumGates.cpp:
-//   H       (alpha+beta)*SQ2, (alpha-beta)*SQ2, SQ2 = 0.707106781186548  (:92-117, :36)
-//   RX      [[c, -is], [-is, c]], dagger +is, c = cos(t/2), s = sin(t/2) (:271-309)
-//   RY      [[c, -s], [s, c]], dagger transposed                        (:473-511)
-//   RZ      diag(c - is, c + is), dagger conjugated                     (:524-570)
-//   CR      |11> times (cos t + i sin t), dagger conjugated             (:773-825)
-//   iSWAP   |01> <-> |10> with factor +i, dagger -i                     (:838-899)
-//   sqiSWAP [[SQ2, i SQ2], [i SQ2, SQ2]] on {|01>,|10>}, dagger -i      (:978-1039)
-//   NOT/CNOT/Toffoli: X on the target where every control is 1          (:668-737, :1277-1435)
-//   controlSwap(c, a, b): exchange |a=1,b=0> and |a=0,b=1> where c = 1  (:934-965)
+// The reference conventions live in qs_lower.cpp (qs_lower_gate).
 #include <algorithm>
 #include <cmath>
 #include <cstdarg>
@@ -20,6 +11,7 @@
 #include <vector>
 
 #include "qs_common.cuh"
+#include "qs_prim.h"
 
 int qs_copy_in(qs_state *s, const void *host, int host_dtype);
 int qs_copy_out(qs_state *s, void *host, int host_dtype);
@@ -243,114 +235,19 @@ extern "C" int qs_apply_phase(qs_state *s, uint64_t mask, double re, double im)
 }
 
 // ------------------------------------------------------------------ gate records
-static const double kSQ2 = 0.707106781186548;     // CPUQuantumGates.cpp:36
-
-static int gate_ctrl_mask(const qs_state *s, const qs_gate *g, uint64_t *mask)
+int qs_launch_prim(qs_state *s, const qs_prim &p)
 {
-    *mask = 0;
-    if (g->nctrl < 0 || g->nctrl > QS_MAX_CTRL) return qs_fail(QS_ERR_ARG, "gate: bad control count %d", g->nctrl);
-    for (int j = 0; j < g->nctrl; ++j) {
-        int c = g->ctrl[j];
-        if (c < 0 || c >= s->n) return qs_fail(QS_ERR_ARG, "gate: control %d out of range", c);
-        if (*mask & (1ull << c)) return qs_fail(QS_ERR_ARG, "gate: control %d listed twice", c);
-        *mask |= 1ull << c;
-    }
-    return QS_OK;
-}
-
-static int add_ctrl(const qs_state *s, uint64_t *mask, int q)
-{
-    if (q < 0 || q >= s->n) return qs_fail(QS_ERR_ARG, "gate: qubit %d out of range", q);
-    if (*mask & (1ull << q)) return qs_fail(QS_ERR_ARG, "gate: qubit %d used twice", q);
-    *mask |= 1ull << q;
-    return QS_OK;
-}
-
-// Fill the 2x2 matrix of a 1-qubit reference gate.
-int qs_gate_matrix_1q(const qs_gate *g, double m[8])
-{
-    const double t = g->theta;
-    memset(m, 0, 8 * sizeof(double));
-    switch (g->op) {
-    case QS_OP_H:
-        m[0] = kSQ2; m[2] = kSQ2; m[4] = kSQ2; m[6] = -kSQ2;
-        return 1;
-    case QS_OP_X:
-    case QS_OP_CNOT:
-    case QS_OP_TOFFOLI:
-        m[2] = 1; m[4] = 1;
-        return 1;
-    case QS_OP_RX: {
-        double c = cos(t / 2), sn = sin(t / 2), sg = g->dagger ? 1.0 : -1.0;
-        m[0] = c; m[3] = sg * sn; m[5] = sg * sn; m[6] = c;
-        return 1;
-    }
-    case QS_OP_RY: {
-        double c = cos(t / 2), sn = sin(t / 2);
-        if (g->dagger) { m[0] = c; m[2] = sn; m[4] = -sn; m[6] = c; }
-        else { m[0] = c; m[2] = -sn; m[4] = sn; m[6] = c; }
-        return 1;
-    }
-    case QS_OP_RZ: {
-        double c = cos(t / 2), sn = sin(t / 2), sg = g->dagger ? -1.0 : 1.0;
-        m[0] = c; m[1] = -sg * sn; m[6] = c; m[7] = sg * sn;
-        return 1;
-    }
-    default:
-        return 0;
-    }
+    if (p.kind == QS_PRIM_PHASE) return launch_phase(s, p.holes, p.m[0], p.m[1]);
+    return launch_pair(s, p.holes, p.cmask, p.off0, p.off1, p.m);
 }
 
 extern "C" int qs_gate_apply(qs_state *s, const qs_gate *g)
 {
     int r = qs_check_state(s);
     if (r) return r;
-    if (!g) return qs_fail(QS_ERR_ARG, "qs_gate_apply: null gate");
-    uint64_t cm;
-    if ((r = gate_ctrl_mask(s, g, &cm))) return r;
-    double m[8];
-    switch (g->op) {
-    case QS_OP_H: case QS_OP_X: case QS_OP_RX: case QS_OP_RY: case QS_OP_RZ: {
-        int t = g->q[0];
-        if ((r = check_q(s, t, "gate"))) return r;
-        if (cm & (1ull << t)) return qs_fail(QS_ERR_ARG, "gate: target %d is also a control", t);
-        qs_gate_matrix_1q(g, m);
-        return launch_pair(s, cm | (1ull << t), cm, 0, 1ull << t, m);
-    }
-    case QS_OP_CNOT: case QS_OP_TOFFOLI: {
-        int nc = g->op == QS_OP_CNOT ? 1 : 2, t = g->q[nc];
-        for (int j = 0; j < nc; ++j)
-            if ((r = add_ctrl(s, &cm, g->q[j]))) return r;
-        if ((r = check_q(s, t, "gate"))) return r;
-        if (cm & (1ull << t)) return qs_fail(QS_ERR_ARG, "gate: target %d is also a control", t);
-        qs_gate_matrix_1q(g, m);
-        return launch_pair(s, cm | (1ull << t), cm, 0, 1ull << t, m);
-    }
-    case QS_OP_CR: {
-        uint64_t mask = cm;
-        if ((r = add_ctrl(s, &mask, g->q[0])) || (r = add_ctrl(s, &mask, g->q[1]))) return r;
-        double sn = g->dagger ? -sin(g->theta) : sin(g->theta);
-        return launch_phase(s, mask, cos(g->theta), sn);
-    }
-    case QS_OP_ISWAP: case QS_OP_SQISWAP: case QS_OP_SWAP: case QS_OP_CSWAP: {
-        int a = g->q[0], b = g->q[1];
-        if (g->op == QS_OP_CSWAP) {
-            if ((r = add_ctrl(s, &cm, g->q[0]))) return r;
-            a = g->q[1]; b = g->q[2];
-        }
-        uint64_t ab = 0;
-        if ((r = add_ctrl(s, &ab, a)) || (r = add_ctrl(s, &ab, b))) return r;
-        if (cm & ab) return qs_fail(QS_ERR_ARG, "gate: exchanged qubit is also a control");
-        memset(m, 0, sizeof(m));
-        double sg = g->dagger ? -1.0 : 1.0;
-        if (g->op == QS_OP_ISWAP) { m[3] = sg; m[5] = sg; }
-        else if (g->op == QS_OP_SQISWAP) { m[0] = kSQ2; m[3] = sg * kSQ2; m[5] = sg * kSQ2; m[6] = kSQ2; }
-        else { m[2] = 1; m[4] = 1; }
-        return launch_pair(s, cm | ab, cm, 1ull << a, 1ull << b, m);
-    }
-    default:
-        return qs_fail(QS_ERR_ARG, "qs_gate_apply: unknown op %d", g->op);
-    }
+    qs_prim p;
+    if ((r = qs_lower_gate(s->n, g, &p))) return r;
+    return qs_launch_prim(s, p);
 }
 
 extern "C" int qs_gates_apply(qs_state *s, const qs_gate *g, size_t count)

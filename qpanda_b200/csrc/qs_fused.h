@@ -1,0 +1,16 @@
+// qs_fused.h - host interface of the fused-block tensor-core kernel.
+#pragma once
+#include <stdint.h>
+
+struct qs_state;
+
+// One fused 5-qubit block: qubits ascending, and the device address of its
+// matrix as BF16 bits [2][64][64] (hi then lo) of the real form R of U.
+struct qs_fused_desc {
+    int qpos[5];
+    const void *mat_dev;
+};
+
+// Launch one block on a complex64 state (n >= 12) on the state's stream.
+// err_dev: device int set to 1 if a bounded wait inside the kernel expired.
+int qs_launch_fused(qs_state *s, const qs_fused_desc *d, int *err_dev);

@@ -407,9 +407,9 @@ int measure_t(qs_state *s, int q, double u, int *outcome)
     return QS_OK;
 }
 
-// Marginal over qubits[0..m) into the device buffer dev_out (2^m doubles).
-template <typename T>
-int marginal_t(qs_state *s, const int *qubits, int m, double *dev_out, size_t part_off)
+// Marginal over qubits[0..m): plan the launch.  *part_bytes receives the
+// scratch the partial slices need (0 when one slice covers the space).
+MargParams marginal_plan(const qs_state *s, const int *qubits, int m, size_t *part_bytes)
 {
     MargParams P;
     memset(&P, 0, sizeof(P));
@@ -434,13 +434,18 @@ int marginal_t(qs_state *s, const int *qubits, int m, double *dev_out, size_t pa
     while (G < uspace && ohi * G < (uint64_t)QS_SM_COUNT * 4) G <<= 1;
     P.G = G;
     P.R = uspace / G;
-    double *part = dev_out;
-    if (G > 1) {
-        size_t need = part_off + G * (8ull << m);
-        int r = qs_ensure_scratch(s, need);
-        if (r) return r;
-        part = reinterpret_cast<double *>(static_cast<char *>(s->scratch) + part_off);
-    }
+    *part_bytes = G > 1 ? G * (8ull << m) : 0;
+    return P;
+}
+
+// Launch a planned marginal into dev_out (2^m doubles, device).  part must
+// hold part_bytes from marginal_plan (unused when that was 0).  Neither
+// pointer may move during the call: this function does not touch scratch.
+template <typename T>
+int marginal_launch(qs_state *s, const MargParams &P, double *dev_out, double *part)
+{
+    const uint64_t ohi = 1ull << P.mhi, G = P.G;
+    if (G == 1) part = dev_out;
     size_t smem = marginal_smem(P);
     QS_CUDA_TRY(cudaFuncSetAttribute(k_marginal<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024));
     uint64_t ctas = ohi * G;
@@ -448,7 +453,7 @@ int marginal_t(qs_state *s, const int *qubits, int m, double *dev_out, size_t pa
     k_marginal<T><<<(unsigned)ctas, kThreads, smem, s->stream>>>(static_cast<const T *>(s->amp), P, part);
     QS_LAUNCH_CHECK("k_marginal");
     if (G > 1) {
-        uint64_t nout = 1ull << m;
+        uint64_t nout = 1ull << P.m;
         k_marginal_combine<<<grid_for(nout, kThreads), kThreads, 0, s->stream>>>(part, G, nout, dev_out);
         QS_LAUNCH_CHECK("k_marginal_combine");
     }
@@ -471,11 +476,14 @@ int check_qubit_list(const qs_state *s, const int *qubits, int m, const char *wh
 template <typename T>
 int probs_t(qs_state *s, const int *qubits, int m, double *out)
 {
-    size_t outb = 8ull << m;
-    int r = qs_ensure_scratch(s, kBufOff + outb);
+    size_t outb = 8ull << m, part_b = 0;
+    MargParams P = marginal_plan(s, qubits, m, &part_b);
+    const size_t o_part = kBufOff + ((outb + 255) & ~255ull);
+    int r = qs_ensure_scratch(s, o_part + part_b);
     if (r) return r;
-    double *dev = reinterpret_cast<double *>(static_cast<char *>(s->scratch) + kBufOff);
-    if ((r = marginal_t<T>(s, qubits, m, dev, kBufOff + ((outb + 255) & ~255ull)))) return r;
+    char *sc = static_cast<char *>(s->scratch);
+    double *dev = reinterpret_cast<double *>(sc + kBufOff);
+    if ((r = marginal_launch<T>(s, P, dev, reinterpret_cast<double *>(sc + o_part)))) return r;
     QS_CUDA_TRY(cudaMemcpyAsync(out, dev, outb, cudaMemcpyDeviceToHost, s->stream));
     QS_CUDA_TRY(cudaStreamSynchronize(s->stream));
     return QS_OK;
@@ -494,14 +502,15 @@ int sample_t(qs_state *s, const int *qubits, int m, const double *u, size_t shot
     auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
     size_t o_tree = kBufOff, o_u = o_tree + al(tree_b), o_out = o_u + al(u_b),
            o_deep = o_out + al(out_b), o_q = o_deep + al(deep_b), o_part = o_q + al(q_b);
-    int r = qs_ensure_scratch(s, o_part);
+    size_t part_b = 0;
+    MargParams P = marginal_plan(s, qubits, K0, &part_b);
+    // Size scratch once, before any pointer into it is taken.
+    int r = qs_ensure_scratch(s, o_part + part_b);
     if (r) return r;
     char *sc = static_cast<char *>(s->scratch);
     double *tree = reinterpret_cast<double *>(sc + o_tree);
     // Level K0 = marginal over the first K0 measured qubits, stored at tree + 2^K0.
-    if ((r = marginal_t<T>(s, qubits, K0, tree + (1ull << K0), o_part))) return r;
-    sc = static_cast<char *>(s->scratch);          // marginal_t may grow scratch
-    tree = reinterpret_cast<double *>(sc + o_tree);
+    if ((r = marginal_launch<T>(s, P, tree + (1ull << K0), reinterpret_cast<double *>(sc + o_part)))) return r;
     for (int k = K0 - 1; k >= 0; --k) {
         k_fold<<<grid_for(1ull << k, kThreads), kThreads, 0, s->stream>>>(tree, k);
         QS_LAUNCH_CHECK("k_fold");

@@ -140,3 +140,19 @@ def test_norm_and_inner(need_gpu):
     assert abs(abs(ip) ** 2 - 1) < 1e-6
     ref = np.vdot(a.get_state(), b.get_state())
     assert abs(ip - ref) < 1e-12
+
+
+def test_probs_and_shots_with_scratch_growth(need_gpu):
+    """22 qubits with 20+ measured: the partial slices outgrow the initial
+    scratch, which must be sized before any pointer into it is taken."""
+    n = 22
+    g = circuits.random_layers(n, 2, 31)
+    sv = StateVector(n, "c128")
+    sv.apply(g)
+    o = OracleState(n)
+    o.apply(g)
+    qs = list(range(2, 22))
+    assert np.abs(sv.probs(qs) - o.probs(qs)).max() < 1e-12
+    qa = np.arange(n, dtype=np.int32)[::-1].copy()
+    u = np.random.default_rng(3).uniform(size=(12, n))
+    assert np.array_equal(sv.sample(qa, u), o.sample(qa, u))
