@@ -5,11 +5,16 @@ between steps), depth 16; each layer an RX/RY/RZ on every qubit (axis and
 angle seeded) then a two-qubit gate on every pair of a seeded random perfect
 matching: CNOT, or iSWAP on 10% of the pairs.  768 gates.
 
-A step = reset to |0...0> and run the whole circuit.  `value` is circuits per
-second over all ranks (each rank runs its own replica: the state does not
-shard at 32 qubits); `e2e` is the same metric through the C ABI with the gate
-list and the shot uniforms copied from pinned host memory each step and 1024
-sampled bitstrings copied back.
+A step = reset to |0...0> and run the whole circuit: on the fused path
+(default) the gate list fused into dense 5-qubit blocks applied on the tensor
+cores, on the plain path one kernel per gate.  The other path runs one step in
+the same process for the comparison, and a 30-qubit run of the same circuit
+structure checks the fused complex64 result against the complex128 per-gate
+path (fidelity, max amplitude error).  `value` is circuits per second over
+all ranks (each rank runs its own replica: the state does not shard at 32
+qubits); `e2e` is the same metric through the C ABI with the gate list and
+the shot uniforms copied from pinned host memory each step and 1024 sampled
+bitstrings copied back.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--path plain|fused]
   python bench.py --impl reference      # the reference CPU backend on the host
@@ -39,7 +44,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--path", default="plain", choices=["plain", "fused"])
+    ap.add_argument("--path", default="fused", choices=["plain", "fused"])
     ap.add_argument("--qubits", type=int, default=N_QUBITS)
     ap.add_argument("--depth", type=int, default=DEPTH)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -218,103 +223,156 @@ def run_reference(args):
 
 
 # ----------------------------------------------------------------- B200 arm
+def timed_steps(L, h, gates, plan, steps, stream, torch, kinds, path):
+    """Run `steps` circuits on the device with an event after every launch.
+    Returns per-step device seconds; appends per-launch durations to kinds."""
+    import ctypes as C
+    from qpanda_b200.capi import check
+    ng = len(gates)
+    nb = plan.num_blocks() if plan is not None else 0
+    nl = nb if path == "fused" else ng
+    gptr = [gates[i:i + 1].ctypes.data for i in range(ng)]
+    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(nl + 1)] for _ in range(steps)]
+    for k in range(steps):
+        check(L.qs_reset_zero(h))
+        ev[k][0].record(stream)
+        for i in range(nl):
+            if path == "fused":
+                check(L.qs_plan_apply_range(h, plan.handle, i, 1))
+            else:
+                check(L.qs_gate_apply(h, C.c_void_p(gptr[i])))
+            ev[k][i + 1].record(stream)
+    torch.cuda.synchronize()
+    out = []
+    for k in range(steps):
+        out.append(ev[k][0].elapsed_time(ev[k][nl]) / 1e3)
+        for i in range(nl):
+            kind = "k_fused_tc (5-qubit block)" if path == "fused" else kernel_kind(gates[i])
+            kinds.setdefault(kind, []).append(ev[k][i].elapsed_time(ev[k][i + 1]) / 1e3)
+    return out
+
+
+def kernel_table(kinds):
+    tot = sum(sum(v) for v in kinds.values())
+    return {k: {"launches": len(v), "mean_ms": statistics.mean(v) * 1e3, "share": sum(v) / tot}
+            for k, v in kinds.items()}
+
+
 def run_b200(args):
+    import ctypes as C
+
     import torch
     ws, rank, local = dist_setup()
     torch.cuda.set_device(local)
     dist_init(ws, "nccl")
-    from qpanda_b200 import StateVector, circuits, lib
-    from qpanda_b200.capi import GATE_DTYPE, check
-    import ctypes as C
+    from qpanda_b200 import FusionPlan, StateVector, circuits, lib
+    from qpanda_b200.capi import check
 
     n, depth = args.qubits, args.depth
     gates = workload(n, depth)
     ng = len(gates)
     amp_b = 8
-    sv = StateVector(n, "c64")
     L = lib()
-    h = sv.handle
     stream = torch.cuda.current_stream()
-    gptr = [gates[i:i + 1].ctypes.data for i in range(ng)]
+    sv = StateVector(n, "c64")
+    h = sv.handle
+    plan = FusionPlan(n, gates)
+    nb = plan.num_blocks()
+    path = args.path
 
-    def step(events=None):
-        check(L.qs_reset_zero(h))
-        for i in range(ng):
-            check(L.qs_gate_apply(h, C.c_void_p(gptr[i])))
-            if events is not None:
-                events[i].record(stream)
+    # warm-up (untimed)
+    wk = {}
+    timed_steps(L, h, gates, plan, args.warmup, stream, torch, wk, path)
 
-    for _ in range(args.warmup):
-        step()
-    torch.cuda.synchronize()
-
-    # timed region
-    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(ng)] for _ in range(args.steps)]
-    start = torch.cuda.Event(enable_timing=True)
-    end = torch.cuda.Event(enable_timing=True)
-    barrier(ws)
-    torch.cuda.synchronize()
+    # timed region: barrier + sync on both sides, events on the launching stream
     props = torch.cuda.get_device_properties(local)
     gpu_id = "GPU-" + str(props.uuid) if getattr(props, "uuid", None) else str(local)
+    barrier(ws)
+    torch.cuda.synchronize()
     clocks = ClockSampler(gpu_id)
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     start.record(stream)
-    step_starts = []
-    for k in range(args.steps):
-        e0 = torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        step_starts.append(e0)
-        step(ev[k])
+    kinds = {}
+    timed_steps(L, h, gates, plan, args.steps, stream, torch, kinds, path)
     end.record(stream)
     torch.cuda.synchronize()
     clk = clocks.stop()
     barrier(ws)
-    elapsed = start.elapsed_time(end) / 1e3
-    elapsed = max_over_ranks(elapsed, ws, device=f"cuda:{local}")
-    launches = args.steps * (ng + 1)
+    elapsed = max_over_ranks(start.elapsed_time(end) / 1e3, ws, device=f"cuda:{local}")
+    launches = args.steps * (1 + (nb if path == "fused" else ng))
+    circuit_s = elapsed / args.steps
 
-    # per-kernel durations from the events inside the timed region
-    kinds = {}
-    for k in range(args.steps):
-        prev = step_starts[k]
-        for i in range(ng):
-            dt = prev.elapsed_time(ev[k][i]) / 1e3
-            prev = ev[k][i]
-            kinds.setdefault(kernel_kind(gates[i]), []).append(dt)
-    dom = "k_pair (1-qubit, dense 2x2)"
-    dom_t = statistics.mean(kinds[dom])
-    dom_bytes = 2 * amp_b * (1 << n)          # algorithmic: read + write every amplitude
     peak, peak_kind = peaks()
+    dom = max(kinds, key=lambda k: sum(kinds[k]))
+    dom_t = statistics.mean(kinds[dom])
+    dom_bytes = 2 * amp_b * (1 << n)          # algorithmic: read + write every amplitude once
     achieved = dom_bytes / dom_t / 1e9
     traffic = None
     tr = load_traffic()
     if tr and dom in tr.get("kernels", {}):
-        traffic = tr["kernels"][dom]["bytes_per_launch_at_32q"]
+        traffic = tr["kernels"][dom].get("bytes_per_launch")
+    pass_bytes = (nb * dom_bytes) if path == "fused" else circuits.gate_bytes(gates, n, amp_b)
 
-    circuit_s = elapsed / args.steps
-    alg_bytes = circuits.gate_bytes(gates, n, amp_b)
+    # the other path, one step, for the fused-vs-plain comparison
+    other = "plain" if path == "fused" else "fused"
+    okinds = {}
+    ot = timed_steps(L, h, gates, plan, 1, stream, torch, okinds, other)[0]
+    odom = max(okinds, key=lambda k: sum(okinds[k]))
+    o_ach = dom_bytes / statistics.mean(okinds[odom]) / 1e9
+    other_line = {"circuit_s": ot, "launches": (nb if other == "fused" else ng) + 1,
+                  "hbm_gbs_effective": ((nb * dom_bytes) if other == "fused"
+                                        else circuits.gate_bytes(gates, n, amp_b)) / ot / 1e9,
+                  "dominant_kernel": odom, "dominant_gbs": o_ach, "dominant_frac": o_ach / peak,
+                  "kernels": kernel_table(okinds)}
 
-    # e2e through the C ABI with host buffers
-    import torch as _t
-    pin_g = _t.empty(gates.nbytes, dtype=_t.uint8).pin_memory()
+    # fidelity of the fused complex64 run against the complex128 per-gate path
+    # (the FP64 oracle on the GPU) at 30 qubits on the same circuit structure
+    fid = None
+    if rank == 0 and n >= 30:
+        nf = 30
+        gf = workload(nf, depth)
+        pf = FusionPlan(nf, gf)
+        a = StateVector(nf, "c64")
+        pf.apply(a)
+        pf.status(a)
+        d = StateVector(nf, "c128")
+        d.apply(gf)
+        ip = a.inner(d)
+        fidelity = abs(ip) ** 2 / (a.norm2() * d.norm2())
+        mx, ss = a.diff(d)
+        fid = {"qubits": nf, "fidelity": fidelity, "infidelity": 1 - fidelity, "max_abs_err": mx,
+               "l2_err": math.sqrt(ss), "blocks": pf.num_blocks(), "oracle": "complex128 per-gate path"}
+        a.close()
+        d.close()
+        pf.close()
+
+    # e2e through the C ABI: host gate list + host uniforms in, host shots out
+    pin_g = torch.empty(gates.nbytes, dtype=torch.uint8).pin_memory()
     pin_g.numpy()[:] = np.frombuffer(gates.tobytes(), dtype=np.uint8)
     qs = np.arange(n, dtype=np.int32)
     rng = np.random.default_rng(SEED)
-    pin_u = _t.empty(SHOTS * n, dtype=_t.float64).pin_memory()
+    pin_u = torch.empty(SHOTS * n, dtype=torch.float64).pin_memory()
     pin_u.numpy()[:] = rng.uniform(size=SHOTS * n)
-    pin_o = _t.empty(SHOTS, dtype=_t.int64).pin_memory()
+    pin_o = torch.empty(SHOTS, dtype=torch.int64).pin_memory()
     e2e_steps = max(1, min(args.steps, 2))
     barrier(ws)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     for _ in range(e2e_steps):
         check(L.qs_reset_zero(h))
-        check(L.qs_gates_apply(h, C.c_void_p(pin_g.data_ptr()), ng))
+        if path == "fused":
+            ph = C.c_void_p()
+            check(L.qs_plan_create(n, C.c_void_p(pin_g.data_ptr()), ng, 5, C.byref(ph)))
+            check(L.qs_plan_apply(h, ph))
+        else:
+            check(L.qs_gates_apply(h, C.c_void_p(pin_g.data_ptr()), ng))
         check(L.qs_sample(h, qs.ctypes.data_as(C.POINTER(C.c_int)), n,
                           C.cast(C.c_void_p(pin_u.data_ptr()), C.POINTER(C.c_double)), SHOTS,
                           C.cast(C.c_void_p(pin_o.data_ptr()), C.POINTER(C.c_uint64))))
+        if path == "fused":
+            L.qs_plan_destroy(ph)
     torch.cuda.synchronize()
-    e2e_s = (time.perf_counter() - t0) / e2e_steps
-    e2e_s = max_over_ranks(e2e_s, ws, device=f"cuda:{local}")
+    e2e_s = max_over_ranks((time.perf_counter() - t0) / e2e_steps, ws, device=f"cuda:{local}")
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
@@ -328,27 +386,33 @@ def run_b200(args):
         line = {
             "metric": METRIC, "value": ws / circuit_s, "unit": "circuits/s", "n_gpus": ws,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": circuit_s * 1e3,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "bf16x3->f32 (complex64 state)" if path == "fused" else "f32 (complex64 state)",
             "data": "synthetic",
             "config": {"workload": f"random-circuit-{n}q-depth{depth}-c64", "qubits": n, "depth": depth,
-                       "gates": ng, "iswap_frac": ISWAP_FRAC, "seed": SEED, "path": args.path,
+                       "gates": ng, "fused_blocks": nb, "iswap_frac": ISWAP_FRAC, "seed": SEED, "path": path,
                        "state_bytes": amp_b << n, "l2": "inputs larger than L2 (32 GiB state), no flush",
                        "parallelism": f"replicas x{ws}"},
             "circuit_s": circuit_s,
-            "hbm_gbs_effective": alg_bytes / circuit_s / 1e9,
+            "hbm_gbs_effective": pass_bytes / circuit_s / 1e9,
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_source": peak_kind, "traffic": traffic,
                          "algorithmic_bytes_per_launch": dom_bytes, "launch_s": dom_t},
-            "kernels": {k: {"launches": len(v), "mean_ms": statistics.mean(v) * 1e3,
-                            "share": sum(v) / sum(sum(x) for x in kinds.values())} for k, v in kinds.items()},
+            "kernels": kernel_table(kinds),
+            other: other_line,
+            "speedup_fused_vs_plain": (ot / circuit_s) if path == "fused" else (circuit_s / ot),
+            "fidelity_check": fid,
             "cpu_baseline": cpu,
-            "e2e": {"value": ws / e2e_s, "unit": "circuits/s", "h2d_bytes_per_step": int(gates.nbytes + SHOTS * n * 8),
-                    "d2h_bytes_per_step": SHOTS * 8, "shots": SHOTS},
+            "e2e": {"value": ws / e2e_s, "unit": "circuits/s",
+                    "h2d_bytes_per_step": int(gates.nbytes + SHOTS * n * 8),
+                    "d2h_bytes_per_step": SHOTS * 8, "shots": SHOTS,
+                    "includes": "plan build on the host, circuit, 1024-shot sampling"},
             "gpu_launches": launches,
             "clocks": clk,
         }
         print(json.dumps(line))
     sv.close()
+    plan.close()
     if ws > 1:
         import torch.distributed as dist
         dist.destroy_process_group()

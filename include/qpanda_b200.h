@@ -168,6 +168,32 @@ int qs_sample(qs_state *s, const int *qubits, int m, const double *u,
 int qs_norm2(qs_state *s, double *norm2);
 /* <a|b> = sum conj(a_i) b_i, FP64 accumulation; a and b may differ in dtype. */
 int qs_inner(qs_state *a, qs_state *b, double *re, double *im);
+/* max_i |a_i - b_i| and sum_i |a_i - b_i|^2 on the device (dtypes may differ). */
+int qs_diff(qs_state *a, qs_state *b, double *max_abs, double *sum_sq);
+
+/* ---- fused path: gate runs -> dense 5-qubit blocks on the tensor cores ---- */
+/* The reference applies every gate as its own pass over the state
+ * (QuantumInstructionGet.cpp:104-124 -> one CPUQuantumGates method each).  A
+ * plan groups the gate list into dense blocks of up to max_k (<= 5) qubits,
+ * each applied in one pass as a 32x32 complex contraction on the tensor cores
+ * (split-BF16 x3 products, FP32 accumulation) for complex64 states of at
+ * least 12 qubits; other states run the plan's gates through the per-gate
+ * kernels.  No reference counterpart (the reference has no gate fusion). */
+typedef struct qs_plan qs_plan;
+int qs_plan_create(int n_qubits, const qs_gate *gates, size_t count, int max_k, qs_plan **out);
+int qs_plan_destroy(qs_plan *plan);
+int qs_plan_info(const qs_plan *plan, size_t *n_blocks, size_t *n_gates);
+/* Block i: its 5 qubits (ascending) and its 32x32 unitary, row-major complex
+ * as 2048 doubles (either output may be NULL).  Row/column index bit b is
+ * qubit qubits[b]. */
+int qs_plan_block(const qs_plan *plan, size_t i, int *k, int *qubits, double *matrix);
+/* Apply every block in order (asynchronous, on the state's stream). */
+int qs_plan_apply(qs_state *s, qs_plan *plan);
+/* Apply blocks [first, first + count) only (for timing or interleaving). */
+int qs_plan_apply_range(qs_state *s, qs_plan *plan, size_t first, size_t count);
+/* Synchronize and report whether a bounded wait inside a fused pass expired
+ * since the last qs_plan_apply (QS_ERR_STATE) - a watchdog, not expected. */
+int qs_plan_status(qs_state *s);
 
 #ifdef __cplusplus
 }

@@ -74,6 +74,14 @@ def lib():
         "qs_sample": (i, [vp, ip, i, dp, sz, C.POINTER(C.c_uint64)]),
         "qs_norm2": (i, [vp, dp]),
         "qs_inner": (i, [vp, vp, dp, dp]),
+        "qs_plan_create": (i, [i, vp, sz, i, C.POINTER(vp)]),
+        "qs_plan_destroy": (i, [vp]),
+        "qs_plan_info": (i, [vp, C.POINTER(sz), C.POINTER(sz)]),
+        "qs_plan_block": (i, [vp, sz, ip, ip, dp]),
+        "qs_plan_apply": (i, [vp, vp]),
+        "qs_plan_apply_range": (i, [vp, vp, sz, sz]),
+        "qs_diff": (i, [vp, vp, dp, dp]),
+        "qs_plan_status": (i, [vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -211,7 +219,61 @@ class StateVector:
         check(lib().qs_norm2(self._h, C.byref(d)))
         return d.value
 
+    def diff(self, other):
+        """(max |a_i - b_i|, sum |a_i - b_i|^2), computed on the device."""
+        m, s2 = C.c_double(), C.c_double()
+        check(lib().qs_diff(self._h, other._h, C.byref(m), C.byref(s2)))
+        return m.value, s2.value
+
     def inner(self, other):
         re, im = C.c_double(), C.c_double()
         check(lib().qs_inner(self._h, other._h, C.byref(re), C.byref(im)))
         return complex(re.value, im.value)
+
+
+class FusionPlan:
+    """Gate list fused into dense 5-qubit blocks (qs_plan_*)."""
+
+    def __init__(self, n, gates, max_k=5):
+        g = np.ascontiguousarray(gates, dtype=GATE_DTYPE)
+        self._keep = g
+        h = C.c_void_p()
+        check(lib().qs_plan_create(int(n), g.ctypes.data, g.size, int(max_k), C.byref(h)))
+        self._h = h
+        self.n = int(n)
+
+    def close(self):
+        if self._h:
+            lib().qs_plan_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self):
+        return self._h
+
+    def num_blocks(self):
+        nb, ng = C.c_size_t(), C.c_size_t()
+        check(lib().qs_plan_info(self._h, C.byref(nb), C.byref(ng)))
+        return nb.value
+
+    def block(self, i):
+        k = C.c_int()
+        q = np.zeros(5, dtype=np.int32)
+        m = np.zeros(2 * 32 * 32)
+        check(lib().qs_plan_block(self._h, i, C.byref(k), _iptr(q), _dptr(m)))
+        return q.tolist(), m.view(np.complex128).reshape(32, 32)
+
+    def apply(self, sv):
+        check(lib().qs_plan_apply(sv.handle, self._h))
+
+    def apply_range(self, sv, first, count):
+        check(lib().qs_plan_apply_range(sv.handle, self._h, first, count))
+
+    def status(self, sv):
+        check(lib().qs_plan_status(sv.handle))

@@ -101,6 +101,7 @@ extern "C" int qs_destroy(qs_state *s)
     if (s->amp) cudaFree(s->amp);
     if (s->scratch) cudaFree(s->scratch);
     if (s->pinned) cudaFreeHost(s->pinned);
+    if (s->fused_norm) cudaFree(s->fused_norm);
     s->amp = nullptr;
     delete s;
     return QS_OK;

@@ -50,6 +50,8 @@ struct qs_state {
     size_t scratch_bytes = 0;
     // Small pinned host buffer for scalar results.
     void *pinned = nullptr;
+    // Norm partials of fused passes (3 x fused grid doubles), on first use.
+    double *fused_norm = nullptr;
     size_t amp_bytes() const { return N * (dtype == QS_C64 ? 8ull : 16ull); }
 };
 
@@ -66,7 +68,9 @@ struct Holes {
 
 __host__ __device__ inline uint64_t insert_holes(uint64_t x, const Holes &h)
 {
+#ifdef __CUDACC__
 #pragma unroll 4
+#endif
     for (int j = 0; j < h.k; ++j) {
         uint64_t lo = x & h.low[j];
         x = ((x & ~h.low[j]) << 1) | lo;

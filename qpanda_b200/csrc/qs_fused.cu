@@ -23,6 +23,12 @@
 //   mbarrier -> tcgen05.ld of the thread's 64 FP32 results -> HBM (same
 //   addresses, in place).  Four CTAs per SM overlap one another's loads,
 //   MMAs and stores.
+//
+// Norm: every pass accumulates sum |in|^2 and sum |out|^2 in FP64 (one
+// partial per CTA).  The truncating FP32 accumulation of the tensor cores
+// loses ~3e-7 of the norm per pass, always in the same direction; the next
+// pass rescales its input by sqrt(N0 / N_prev), N0 being the input norm of the
+// plan's first pass, so the drift does not build up over a circuit.
 #include <cuda_bf16.h>
 
 #include "qs_common.cuh"
@@ -52,6 +58,13 @@ struct FusedParams {
     int vec;                     // 1: qubit 0 is in Q, amplitude pairs (j, j+1) are adjacent
     const uint16_t *mat;         // [2][64][64] bf16 bits of R: hi then lo, row-major (n, k)
     int *err;
+    // Norm tracking (FP64, one partial per CTA, fixed grid): the pass scales
+    // its input by sqrt(sum(norm0) / sum(prev_out)) when both are given, and
+    // writes sum |input|^2 to in_parts (if given) and sum |output|^2 to out_parts.
+    const double *norm0;
+    const double *prev_out;
+    double *in_parts;
+    double *out_parts;
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p)
@@ -169,6 +182,24 @@ __global__ void __launch_bounds__(kThreads, 4) k_fused_tc(float *__restrict__ am
     uint32_t phase = 0;
     bool failed = false;
 
+    // Scale that undoes the systematic norm drift of the previous pass (the
+    // tensor cores' FP32 accumulation does not round to nearest).  Warp 1 sums
+    // the partials in a fixed order; every CTA computes the same value.
+    __shared__ float s_scale;
+    if (warp == 1) {
+        double n0 = 0, np = 0;
+        if (P.norm0 && P.prev_out)
+            for (int i = tid - 32; i < (int)gridDim.x; i += 32) { n0 += P.norm0[i]; np += P.prev_out[i]; }
+        for (int o = 16; o > 0; o >>= 1) {
+            n0 += __shfl_xor_sync(0xffffffffu, n0, o);
+            np += __shfl_xor_sync(0xffffffffu, np, o);
+        }
+        if (tid == 32) s_scale = (P.norm0 && P.prev_out && np > 0) ? (float)sqrt(n0 / np) : 1.0f;
+    }
+    __syncthreads();
+    const float scale = s_scale;
+    double acc_in = 0, acc_out = 0;
+
     for (uint64_t tile = blockIdx.x; tile < P.tiles; tile += gridDim.x) {
         const uint64_t base = insert_holes(tile, P.outer) | depC;
         // ---- load this row's 32 amplitudes
@@ -185,6 +216,12 @@ __global__ void __launch_bounds__(kThreads, 4) k_fused_tc(float *__restrict__ am
                 float2 v = *reinterpret_cast<const float2 *>(amp + 2 * (base | P.offQ[j]));
                 x[2 * j] = v.x; x[2 * j + 1] = v.y;
             }
+        }
+        {
+            float t = 0.f;
+#pragma unroll
+            for (int e = 0; e < 64; ++e) { x[e] *= scale; t = fmaf(x[e], x[e], t); }
+            acc_in += (double)t;
         }
         // ---- split into bf16 hi/lo and store the row (chunk c = reals 8c..8c+7)
 #pragma unroll
@@ -227,6 +264,14 @@ __global__ void __launch_bounds__(kThreads, 4) k_fused_tc(float *__restrict__ am
 #pragma unroll
         for (int q = 0; q < 4; ++q) tmem_ld16(taddr + 16 * q, y[q]);
         asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        {
+            float t = 0.f;
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+#pragma unroll
+                for (int e = 0; e < 16; ++e) t = fmaf(__uint_as_float(y[q][e]), __uint_as_float(y[q][e]), t);
+            acc_out += (double)t;
+        }
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
             if (P.vec) {
@@ -246,6 +291,22 @@ __global__ void __launch_bounds__(kThreads, 4) k_fused_tc(float *__restrict__ am
         }
         asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     }
+    // per-CTA norm partials (fixed order: warp shuffles, then warp 0)
+    {
+        __shared__ double red[2][kThreads / 32];
+        for (int o = 16; o > 0; o >>= 1) {
+            acc_in += __shfl_xor_sync(0xffffffffu, acc_in, o);
+            acc_out += __shfl_xor_sync(0xffffffffu, acc_out, o);
+        }
+        if ((tid & 31) == 0) { red[0][warp] = acc_in; red[1][warp] = acc_out; }
+        __syncthreads();
+        if (tid == 0) {
+            double a = 0, b = 0;
+            for (int w = 0; w < kThreads / 32; ++w) { a += red[0][w]; b += red[1][w]; }
+            if (P.in_parts) P.in_parts[blockIdx.x] = a;
+            if (P.out_parts) P.out_parts[blockIdx.x] = b;
+        }
+    }
     if (failed) {
         if (tid == 0) atomicExch(P.err, 1);
         // Let the MMA still in flight (the phase that timed out) finish
@@ -261,6 +322,12 @@ __global__ void __launch_bounds__(kThreads, 4) k_fused_tc(float *__restrict__ am
 }
 
 }  // namespace
+
+int qs_fused_grid(const qs_state *s)
+{
+    uint64_t tiles = s->N >> 12;
+    return (int)(tiles < (uint64_t)QS_SM_COUNT * 4 ? tiles : (uint64_t)QS_SM_COUNT * 4);
+}
 
 int qs_launch_fused(qs_state *s, const qs_fused_desc *d, int *err_dev)
 {
@@ -288,9 +355,13 @@ int qs_launch_fused(qs_state *s, const qs_fused_desc *d, int *err_dev)
     P.tiles = s->N >> 12;
     P.mat = static_cast<const uint16_t *>(d->mat_dev);
     P.err = err_dev;
+    P.norm0 = d->norm0;
+    P.prev_out = d->prev_out;
+    P.in_parts = d->in_parts;
+    P.out_parts = d->out_parts;
     QS_CUDA_TRY(cudaFuncSetAttribute(k_fused_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes));
-    uint64_t grid = P.tiles < (uint64_t)QS_SM_COUNT * 4 ? P.tiles : (uint64_t)QS_SM_COUNT * 4;
-    k_fused_tc<<<(unsigned)grid, kThreads, kSmemBytes, s->stream>>>(static_cast<float *>(s->amp), P);
+    const unsigned grid = (unsigned)qs_fused_grid(s);
+    k_fused_tc<<<grid, kThreads, kSmemBytes, s->stream>>>(static_cast<float *>(s->amp), P);
     QS_LAUNCH_CHECK("k_fused_tc");
     return QS_OK;
 }

@@ -9,7 +9,15 @@ struct qs_state;
 struct qs_fused_desc {
     int qpos[5];
     const void *mat_dev;
+    // norm tracking buffers (device, qs_fused_grid() doubles each; may be null)
+    const double *norm0;         // input-norm partials of the plan's first pass
+    const double *prev_out;      // output-norm partials of the previous pass
+    double *in_parts;            // this pass: input-norm partials
+    double *out_parts;           // this pass: output-norm partials
 };
+
+// CTAs of one fused pass on s (the number of norm partials per pass).
+int qs_fused_grid(const qs_state *s);
 
 // Launch one block on a complex64 state (n >= 12) on the state's stream.
 // err_dev: device int set to 1 if a bounded wait inside the kernel expired.

@@ -321,6 +321,47 @@ k_inner(const Ta *__restrict__ a, const Tb *__restrict__ b, uint64_t N, double *
     }
 }
 
+template <typename Ta, typename Tb>
+__global__ void __launch_bounds__(kThreads)
+k_diff(const Ta *__restrict__ a, const Tb *__restrict__ b, uint64_t N, double *partials)
+{
+    typedef typename vec2<Ta>::type VA;
+    typedef typename vec2<Tb>::type VB;
+    const VA *pa = reinterpret_cast<const VA *>(a);
+    const VB *pb = reinterpret_cast<const VB *>(b);
+    double mx = 0, ss = 0;
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < N; i += stride) {
+        VA x = pa[i];
+        VB y = pb[i];
+        double dr = (double)x.x - (double)y.x, di = (double)x.y - (double)y.y;
+        double d2 = dr * dr + di * di;
+        ss += d2;
+        mx = fmax(mx, d2);
+    }
+    // max via shuffles, sum via block_sum
+    for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    __shared__ double wmax[kThreads / 32];
+    if ((threadIdx.x & 31) == 0) wmax[threadIdx.x >> 5] = mx;
+    double s2 = block_sum(ss);
+    if (threadIdx.x == 0) {
+        double m = 0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) m = fmax(m, wmax[w]);
+        partials[2 * blockIdx.x] = m;
+        partials[2 * blockIdx.x + 1] = s2;
+    }
+}
+
+__global__ void k_finalize_diff(const double *partials, int count, double *res)
+{
+    if (threadIdx.x == 0) {
+        double m = 0, s = 0;
+        for (int i = 0; i < count; ++i) { m = fmax(m, partials[2 * i]); s += partials[2 * i + 1]; }
+        res[0] = sqrt(m);
+        res[1] = s;
+    }
+}
+
 __global__ void k_finalize2(const double *partials, int count, double *res)
 {
     double re = 0, im = 0;
@@ -625,6 +666,33 @@ extern "C" int qs_inner(qs_state *a, qs_state *b, double *re, double *im)
     if ((r = read_result(a, kResOff, 16))) return r;
     *re = static_cast<double *>(a->pinned)[0];
     *im = static_cast<double *>(a->pinned)[1];
+    return QS_OK;
+}
+
+extern "C" int qs_diff(qs_state *a, qs_state *b, double *max_abs, double *sum_sq)
+{
+    int r = qs_check_state(a);
+    if (r) return r;
+    if ((r = qs_check_state(b))) return r;
+    if (a->n != b->n) return qs_fail(QS_ERR_ARG, "qs_diff: qubit counts differ (%d vs %d)", a->n, b->n);
+    QS_CUDA_TRY(cudaStreamSynchronize(b->stream));
+    unsigned grid = grid_for(a->N, kThreads, 4);
+    double *part = reinterpret_cast<double *>(static_cast<char *>(a->scratch) + kPartOff);
+    if (a->dtype == QS_C64 && b->dtype == QS_C64)
+        k_diff<float, float><<<grid, kThreads, 0, a->stream>>>((const float *)a->amp, (const float *)b->amp, a->N, part);
+    else if (a->dtype == QS_C64)
+        k_diff<float, double><<<grid, kThreads, 0, a->stream>>>((const float *)a->amp, (const double *)b->amp, a->N, part);
+    else if (b->dtype == QS_C64)
+        k_diff<double, float><<<grid, kThreads, 0, a->stream>>>((const double *)a->amp, (const float *)b->amp, a->N, part);
+    else
+        k_diff<double, double><<<grid, kThreads, 0, a->stream>>>((const double *)a->amp, (const double *)b->amp, a->N, part);
+    QS_LAUNCH_CHECK("k_diff");
+    double *res = reinterpret_cast<double *>(static_cast<char *>(a->scratch) + kResOff);
+    k_finalize_diff<<<1, 32, 0, a->stream>>>(part, (int)grid, res);
+    QS_LAUNCH_CHECK("k_finalize_diff");
+    if ((r = read_result(a, kResOff, 16))) return r;
+    if (max_abs) *max_abs = static_cast<double *>(a->pinned)[0];
+    if (sum_sq) *sum_sq = static_cast<double *>(a->pinned)[1];
     return QS_OK;
 }
 

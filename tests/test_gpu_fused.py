@@ -1,0 +1,127 @@
+"""GPU parity of the fused tensor-core path (qs_plan_apply, complex64).
+
+Bar: max |amplitude error| <= 1e-5 against the FP64 oracle and state
+fidelity |<oracle|fused>|^2 >= 1 - 1e-6.
+"""
+import numpy as np
+import pytest
+
+from oracle.pyoracle import OracleState
+from qpanda_b200 import FusionPlan, StateVector, circuits
+
+pytestmark = pytest.mark.gpu
+AMP_TOL, FID_TOL = 1e-5, 1e-6
+
+
+def random_state(n, seed):
+    rng = np.random.default_rng(seed)
+    v = rng.normal(size=1 << n) + 1j * rng.normal(size=1 << n)
+    return v / np.linalg.norm(v)
+
+
+def check_fused(n, g, init=None):
+    sv = StateVector(n, "c64")
+    o = OracleState(n)
+    if init is not None:
+        sv.set_state(init.astype(np.complex64))
+        o.set_state(init.astype(np.complex64).astype(np.complex128))
+    p = FusionPlan(n, g)
+    p.apply(sv)
+    p.status(sv)
+    o.apply(g)
+    got, ref = sv.get_state(), o.state()
+    err = np.abs(got - ref).max()
+    fid = abs(np.vdot(ref, got)) ** 2 / (np.vdot(got, got).real * np.vdot(ref, ref).real)
+    assert err < AMP_TOL, err
+    assert fid > 1 - FID_TOL, fid
+    return p.num_blocks()
+
+
+@pytest.mark.parametrize("n", [12, 13, 17])
+def test_fused_random_layers(need_gpu, n):
+    nb = check_fused(n, circuits.random_layers(n, 8, 40 + n, iswap_frac=0.1))
+    assert nb > 0
+
+
+def test_fused_qft_gaussian(need_gpu):
+    check_fused(14, circuits.qft(14), init=random_state(14, 2))
+
+
+def test_fused_every_gate_kind(need_gpu):
+    from tests.golden.make_golden import every_gate_circuit
+    check_fused(12, every_gate_circuit(12, 9), init=random_state(12, 3))
+
+
+def test_fused_block_positions(need_gpu):
+    """Blocks on the lowest qubits (paired 16-byte loads), on the highest
+    qubits, and straddling: one dense random 2-qubit-gate layer per case."""
+    n = 15
+    rng = np.random.default_rng(0)
+    for qs in ([0, 1, 2, 3, 4], [10, 11, 12, 13, 14], [0, 5, 9, 13, 14], [1, 2, 3, 4, 5], [3, 7, 8, 11, 12]):
+        spec = []
+        for q in qs:
+            spec.append(("RY", (q,), float(rng.uniform(0, 6.28))))
+            spec.append(("RZ", (q,), float(rng.uniform(0, 6.28))))
+        for a, b in zip(qs[:-1], qs[1:]):
+            spec.append(("CNOT", (a, b)))
+            spec.append(("SQISWAP", (b, a)))
+        g = circuits.make_gates(spec)
+        p = FusionPlan(n, g)
+        assert p.num_blocks() == 1 and p.block(0)[0] == sorted(qs)
+        check_fused(n, g, init=random_state(n, qs[0] + 7))
+
+
+def test_fused_vqe_and_reuse(need_gpu):
+    n = 16
+    g = circuits.vqe_ansatz(n, 4, seed=5)
+    p = FusionPlan(n, g)
+    a = StateVector(n, "c64")
+    p.apply(a)
+    p.apply(a)               # a plan applies repeatedly
+    o = OracleState(n)
+    o.apply(g)
+    o.apply(g)
+    assert np.abs(a.get_state() - o.state()).max() < AMP_TOL
+
+
+def test_fused_fidelity_26q_vs_fp64_gpu(need_gpu):
+    """26 qubits, 12 layers: fused complex64 against the complex128 per-gate
+    path (itself pinned to the oracle by the other tests)."""
+    n = 26
+    g = circuits.random_layers(n, 12, 7, iswap_frac=0.1)
+    f = StateVector(n, "c64")
+    p = FusionPlan(n, g)
+    p.apply(f)
+    p.status(f)
+    d = StateVector(n, "c128")
+    d.apply(g)
+    ip = f.inner(d)
+    fid = abs(ip) ** 2 / f.norm2()
+    assert fid > 1 - FID_TOL, fid
+    # the per-pass rescale keeps the norm within one pass of drift
+    assert abs(f.norm2() - 1) < 2e-6, f.norm2()
+
+
+def test_fused_range_with_interleaved_probs(need_gpu):
+    """Blocks applied one at a time with a marginal computed in between give
+    the same state as the whole plan (norm partials survive other calls)."""
+    n = 20
+    g = circuits.random_layers(n, 6, 11, iswap_frac=0.1)
+    p = FusionPlan(n, g)
+    a, b = StateVector(n, "c64"), StateVector(n, "c64")
+    p.apply(a)
+    for i in range(p.num_blocks()):
+        p.apply_range(b, i, 1)
+        b.probs(list(range(n)))
+    mx, _ = a.diff(b)
+    assert mx == 0.0
+
+
+def test_small_state_plan_runs_per_gate(need_gpu):
+    n = 8
+    g = circuits.random_layers(n, 5, 2)
+    sv = StateVector(n, "c128")
+    FusionPlan(n, g).apply(sv)
+    o = OracleState(n)
+    o.apply(g)
+    assert np.abs(sv.get_state() - o.state()).max() < 1e-12
