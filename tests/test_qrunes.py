@@ -1,0 +1,97 @@
+"""QRunes programs through the reference's own parser and dispatcher.
+
+CPU part: the harness with the reference CPU backend reproduces the oracle and
+the reference's own fixture programs (read from the reference tree when it is
+present).  GPU part: the B200 backend (B200QuantumGates over the C ABI) gives
+the same PMEASURE probabilities and - with the same generator seed - the same
+MEASURE counts as the reference backend."""
+import os
+
+import numpy as np
+import pytest
+
+from oracle.pyoracle import OracleState
+from qpanda_b200 import circuits
+from qpanda_b200.qrunes import to_qrunes
+from tests import qrunes_harness as H
+
+needs_runner = pytest.mark.skipif(not H.available(), reason="tests/qrunes not built (needs the reference tree)")
+REF_SDK = os.path.join(os.environ.get("QPANDA_REF", "/root/reference"), "QPandaSDK")
+
+
+def programs(tmp_path):
+    progs = {}
+    n = 9
+    g = circuits.random_layers(n, 6, 77)
+    progs["layers_pmeasure"] = to_qrunes(n, g, pmeasure=[0, 3, 8, 5])
+    progs["layers_measure"] = to_qrunes(n, g, measure=[(q, q) for q in range(n)])
+    from tests.golden.make_golden import every_gate_circuit
+    eg = every_gate_circuit(7, 21)
+    # plain ISWAP lines are a no-op on the reference path (swapped dispatch
+    # branches, Instruction.cpp:558-577): keep them inside CONTROL blocks only
+    keep = [i for i in range(len(eg)) if not (eg[i]["op"] == 8 and eg[i]["nctrl"] == 0)]
+    eg = eg[keep]
+    # and controlled sqiSWAP / iSWAP / CR / CSWAP are no-ops or uncontrolled on
+    # the reference path: drop the controls from those
+    for i in range(len(eg)):
+        if int(eg[i]["op"]) in (7, 8, 9, 11):
+            eg[i]["nctrl"] = 0
+    progs["every_gate_pmeasure"] = to_qrunes(7, eg, pmeasure=[0, 1, 2, 3, 4, 5, 6])
+    qft = circuits.qft(8)
+    progs["qft_pmeasure"] = to_qrunes(8, np.concatenate([circuits.random_layers(8, 1, 5), qft]), pmeasure=[7, 6, 5])
+    paths = {}
+    for k, text in progs.items():
+        p = tmp_path / f"{k}.txt"
+        p.write_text(text)
+        paths[k] = str(p)
+    return paths
+
+
+@needs_runner
+def test_cpu_harness_matches_oracle(tmp_path):
+    n = 9
+    g = circuits.random_layers(n, 6, 77)
+    path = programs(tmp_path)["layers_pmeasure"]
+    kind, res, nq = H.run(path, H.CPU)
+    assert kind == "PMEASURE" and nq == n
+    o = OracleState(n)
+    o.apply(g)
+    p = o.probs([0, 3, 8, 5])
+    top = sorted(range(16), key=lambda i: (-p[i], i))[:10]
+    for i in top:
+        assert abs(res[format(i, "04b")] - p[i]) < 1e-12
+
+
+@needs_runner
+@pytest.mark.skipif(not os.path.isdir(REF_SDK), reason="reference fixture programs not present")
+def test_cpu_harness_reference_fixtures():
+    kind, res, _ = H.run(os.path.join(REF_SDK, "shor.txt"), H.CPU)
+    assert kind == "PMEASURE"
+    assert abs(res["100"] - 0.5) < 1e-12 and abs(res["101"] - 0.5) < 1e-12
+    kind, res, _ = H.run(os.path.join(REF_SDK, "testMain", "shor_15.txt"), H.CPU, seed=7, repeat=200)
+    assert kind == "MEASURE" and abs(sum(res.values()) - 1) < 1e-12
+
+
+@needs_runner
+@pytest.mark.gpu
+@pytest.mark.parametrize("backend,tol", [(H.B200_C128, 1e-12), (H.B200_C64, 1e-5)])
+def test_b200_backend_pmeasure(need_gpu, tmp_path, backend, tol):
+    for name, path in programs(tmp_path).items():
+        if "pmeasure" not in name:
+            continue
+        k0, r0, _ = H.run(path, H.CPU)
+        k1, r1, _ = H.run(path, backend)
+        assert k0 == k1 == "PMEASURE"
+        assert set(r0) == set(r1), name
+        for b in r0:
+            assert abs(r0[b] - r1[b]) < tol, (name, b)
+
+
+@needs_runner
+@pytest.mark.gpu
+def test_b200_backend_measure_counts_bit_exact(need_gpu, tmp_path):
+    path = programs(tmp_path)["layers_measure"]
+    k0, r0, _ = H.run(path, H.CPU, seed=4242, repeat=64)
+    k1, r1, _ = H.run(path, H.B200_C128, seed=4242, repeat=64)
+    assert k0 == k1 == "MEASURE"
+    assert r0 == r1
