@@ -171,6 +171,26 @@ int qs_inner(qs_state *a, qs_state *b, double *re, double *im);
 /* max_i |a_i - b_i| and sum_i |a_i - b_i|^2 on the device (dtypes may differ). */
 int qs_diff(qs_state *a, qs_state *b, double *max_abs, double *sum_sq);
 
+/* qubitMeasure for callers that cannot allocate memory when they measure.
+ * No counterpart in the reference.  qs_measure keeps its reduction partials in
+ * scratch that qs_create allocated; this entry point allocates nothing (no
+ * cudaMalloc, cudaFree or allocating library call) and needs no qs_state, for
+ * a serving loop that reserved all device memory up front, a framework whose
+ * own allocator owns the device memory, or a caller that holds the amplitudes
+ * in a buffer of its own.  amp: 2^n_qubits amplitudes of dtype on the current
+ * device, collapsed in place; u: the uniform of qubitMeasure's rule;
+ * outcome_dev / p0_dev: device words that receive the outcome (-1 if the
+ * selected outcome has probability 0, state left unchanged) and P(qubit q ==
+ * 0).  Asynchronous on `stream`.  Its partial sums live in a fixed 512 KB
+ * device array compiled into the library (held on every GPU that loads it
+ * until exit), which limits states to at most 32 qubits; larger ones are
+ * rejected with QS_ERR_ARG.  The first call on a device looks up that
+ * array's address (cudaGetSymbolAddress): make it before any stream capture
+ * on the device.  All calls share the array, so calls that overlap on the GPU
+ * (unordered streams) race; calls ordered on one stream do not. */
+int qs_measure_noalloc(void *amp, int n_qubits, int dtype, int q, double u,
+                       int *outcome_dev, double *p0_dev, void *stream);
+
 /* ---- fused path: gate runs -> dense 5-qubit blocks on the tensor cores ---- */
 /* The reference applies every gate as its own pass over the state
  * (QuantumInstructionGet.cpp:104-124 -> one CPUQuantumGates method each).  A

@@ -81,6 +81,7 @@ def lib():
         "qs_plan_apply": (i, [vp, vp]),
         "qs_plan_apply_range": (i, [vp, vp, sz, sz]),
         "qs_diff": (i, [vp, vp, dp, dp]),
+        "qs_measure_noalloc": (i, [vp, i, i, i, d, vp, vp, vp]),
         "qs_plan_status": (i, [vp]),
     }
     for name, (res, args) in sig.items():
