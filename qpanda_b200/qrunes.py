@@ -2,7 +2,7 @@
 parser, QPandaSDK/QRunesParser), for running the same circuit through the
 reference's own toolchain.
 
-Controls become CONTROL/ENDCONTROL blocks and dagger flags DAGGER/ENDDAGGER
+Controls become (nested, one qubit each) CONTROL/ENDCONTROL blocks and dagger flags DAGGER/ENDDAGGER
 blocks (the parser copies the control stack into each node and toggles the
 dagger flag, LinkedListController.cpp:289-398).  QRunes has no SWAP or
 controlSwap keyword: SWAP is written as three CNOTs and controlSwap as three
@@ -60,9 +60,10 @@ def to_qrunes(n, gates, measure=None, pmeasure=None):
         if int(g["dagger"]):
             lines = ["DAGGER"] + lines + ["ENDDAGGER"]
         nc = int(g["nctrl"])
-        if nc:
-            cs = ",".join(str(int(c)) for c in g["ctrl"][:nc])
-            lines = [f"CONTROL {cs}"] + lines + [f"ENDCONTROL {cs}"]
+        # one qubit per CONTROL line (the grammar takes a single qubit);
+        # several controls are nested blocks
+        for c in reversed([int(c) for c in g["ctrl"][:nc]]):
+            lines = [f"CONTROL {c}"] + lines + [f"ENDCONTROL {c}"]
         out.extend(lines)
     for q, c in (measure or []):
         out.append(f"MEASURE {q},${c}")

@@ -95,3 +95,24 @@ def test_b200_backend_measure_counts_bit_exact(need_gpu, tmp_path):
     k1, r1, _ = H.run(path, H.B200_C128, seed=4242, repeat=64)
     assert k0 == k1 == "MEASURE"
     assert r0 == r1
+
+
+@needs_runner
+def test_cpu_harness_every_gate_program_matches_oracle(tmp_path):
+    """The generated every-gate program (nested CONTROL and DAGGER blocks)
+    through the reference parser and CPU backend equals the oracle."""
+    from tests.golden.make_golden import every_gate_circuit
+    eg = every_gate_circuit(7, 21)
+    keep = [i for i in range(len(eg)) if not (eg[i]["op"] == 8 and eg[i]["nctrl"] == 0)]
+    eg = eg[keep]
+    for i in range(len(eg)):
+        if int(eg[i]["op"]) in (7, 8, 9, 11):
+            eg[i]["nctrl"] = 0
+    o = OracleState(7)
+    o.apply(eg)
+    p = o.probs(list(range(7)))
+    path = programs(tmp_path)["every_gate_pmeasure"]
+    kind, res, _ = H.run(path, H.CPU)
+    top = sorted(range(128), key=lambda i: (-p[i], i))[:10]
+    for i in top:
+        assert abs(res[format(i, "07b")] - p[i]) < 1e-12
