@@ -45,6 +45,8 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--path", default="fused", choices=["plain", "fused"])
+    ap.add_argument("--kernel", default="tiled", choices=["tiled", "single"],
+                    help="fused path: tiled passes (up to 3 blocks per pass) or one block per pass")
     ap.add_argument("--qubits", type=int, default=N_QUBITS)
     ap.add_argument("--depth", type=int, default=DEPTH)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -229,8 +231,10 @@ def timed_steps(L, h, gates, plan, steps, stream, torch, kinds, path):
     import ctypes as C
     from qpanda_b200.capi import check
     ng = len(gates)
-    nb = plan.num_blocks() if plan is not None else 0
+    nb = plan.num_launches() if plan is not None else 0
     nl = nb if path == "fused" else ng
+    fused_name = ("k_fused_tile (tiled pass)" if getattr(plan, "kernel", "tiled") == "tiled"
+                  else "k_fused_tc (5-qubit block)")
     gptr = [gates[i:i + 1].ctypes.data for i in range(ng)]
     ev = [[torch.cuda.Event(enable_timing=True) for _ in range(nl + 1)] for _ in range(steps)]
     for k in range(steps):
@@ -247,7 +251,7 @@ def timed_steps(L, h, gates, plan, steps, stream, torch, kinds, path):
     for k in range(steps):
         out.append(ev[k][0].elapsed_time(ev[k][nl]) / 1e3)
         for i in range(nl):
-            kind = "k_fused_tc (5-qubit block)" if path == "fused" else kernel_kind(gates[i])
+            kind = fused_name if path == "fused" else kernel_kind(gates[i])
             kinds.setdefault(kind, []).append(ev[k][i].elapsed_time(ev[k][i + 1]) / 1e3)
     return out
 
@@ -276,8 +280,9 @@ def run_b200(args):
     stream = torch.cuda.current_stream()
     sv = StateVector(n, "c64")
     h = sv.handle
-    plan = FusionPlan(n, gates)
-    nb = plan.num_blocks()
+    plan = FusionPlan(n, gates, kernel=args.kernel)
+    nb = plan.num_launches()
+    nblocks = plan.num_blocks()
     path = args.path
 
     # warm-up (untimed)
@@ -331,7 +336,7 @@ def run_b200(args):
     if rank == 0 and n >= 30:
         nf = 30
         gf = workload(nf, depth)
-        pf = FusionPlan(nf, gf)
+        pf = FusionPlan(nf, gf, kernel=args.kernel)
         a = StateVector(nf, "c64")
         pf.apply(a)
         pf.status(a)
@@ -341,7 +346,8 @@ def run_b200(args):
         fidelity = abs(ip) ** 2 / (a.norm2() * d.norm2())
         mx, ss = a.diff(d)
         fid = {"qubits": nf, "fidelity": fidelity, "infidelity": 1 - fidelity, "max_abs_err": mx,
-               "l2_err": math.sqrt(ss), "blocks": pf.num_blocks(), "oracle": "complex128 per-gate path"}
+               "l2_err": math.sqrt(ss), "blocks": pf.num_blocks(), "passes": pf.num_launches(),
+               "oracle": "complex128 per-gate path"}
         a.close()
         d.close()
         pf.close()
@@ -361,8 +367,12 @@ def run_b200(args):
     for _ in range(e2e_steps):
         check(L.qs_reset_zero(h))
         if path == "fused":
-            ph = C.c_void_p()
-            check(L.qs_plan_create(n, C.c_void_p(pin_g.data_ptr()), ng, 5, C.byref(ph)))
+            from qpanda_b200.capi import PlanOpts
+            ph, o = C.c_void_p(), PlanOpts()
+            check(L.qs_plan_default_opts(C.byref(o)))
+            if args.kernel == "single":
+                o.kernel, o.max_sub = 1, 1
+            check(L.qs_plan_create_ex(n, C.c_void_p(pin_g.data_ptr()), ng, C.byref(o), C.byref(ph)))
             check(L.qs_plan_apply(h, ph))
         else:
             check(L.qs_gates_apply(h, C.c_void_p(pin_g.data_ptr()), ng))
@@ -390,7 +400,8 @@ def run_b200(args):
             "dtype": "bf16x3->f32 (complex64 state)" if path == "fused" else "f32 (complex64 state)",
             "data": "synthetic",
             "config": {"workload": f"random-circuit-{n}q-depth{depth}-c64", "qubits": n, "depth": depth,
-                       "gates": ng, "fused_blocks": nb, "iswap_frac": ISWAP_FRAC, "seed": SEED, "path": path,
+                       "gates": ng, "fused_blocks": nblocks, "fused_passes": nb, "kernel": args.kernel,
+                       "iswap_frac": ISWAP_FRAC, "seed": SEED, "path": path,
                        "state_bytes": amp_b << n, "l2": "inputs larger than L2 (32 GiB state), no flush",
                        "parallelism": f"replicas x{ws}"},
             "circuit_s": circuit_s,

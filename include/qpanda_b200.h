@@ -200,7 +200,25 @@ int qs_measure_noalloc(void *amp, int n_qubits, int dtype, int q, double u,
  * least 12 qubits; other states run the plan's gates through the per-gate
  * kernels.  No reference counterpart (the reference has no gate fusion). */
 typedef struct qs_plan qs_plan;
+/* Single-block passes: one dense block of up to max_k qubits per pass. */
 int qs_plan_create(int n_qubits, const qs_gate *gates, size_t count, int max_k, qs_plan **out);
+
+#define QS_PLAN_SINGLE 1   /* one 5-qubit block per read+write of the state */
+#define QS_PLAN_TILED  2   /* up to max_sub 5-qubit blocks per read+write, within 12 tile qubits */
+typedef struct qs_plan_opts {
+    int block_qubits;      /* fusion width of one block, 1..5 */
+    int tile_qubits;       /* tiled passes: qubits per tile (12) */
+    int max_sub;           /* tiled passes: blocks per pass, 1..3 */
+    int low_qubits;        /* tiled passes: qubits 0..low_qubits-1 always in the tile (1..5) */
+    int kernel;            /* QS_PLAN_SINGLE or QS_PLAN_TILED */
+} qs_plan_opts;
+/* Defaults: 5-qubit blocks, tiled passes of 12 qubits with up to 3 blocks,
+ * qubits 0..2 in every tile. */
+int qs_plan_default_opts(qs_plan_opts *opts);
+int qs_plan_create_ex(int n_qubits, const qs_gate *gates, size_t count, const qs_plan_opts *opts,
+                      qs_plan **out);
+/* Kernel launches (passes) the plan makes per application. */
+int qs_plan_launches(const qs_plan *plan, size_t *n_launches);
 int qs_plan_destroy(qs_plan *plan);
 int qs_plan_info(const qs_plan *plan, size_t *n_blocks, size_t *n_gates);
 /* Block i: its 5 qubits (ascending) and its 32x32 unitary, row-major complex
@@ -209,7 +227,7 @@ int qs_plan_info(const qs_plan *plan, size_t *n_blocks, size_t *n_gates);
 int qs_plan_block(const qs_plan *plan, size_t i, int *k, int *qubits, double *matrix);
 /* Apply every block in order (asynchronous, on the state's stream). */
 int qs_plan_apply(qs_state *s, qs_plan *plan);
-/* Apply blocks [first, first + count) only (for timing or interleaving). */
+/* Apply launches (passes) [first, first + count) only (for timing or interleaving). */
 int qs_plan_apply_range(qs_state *s, qs_plan *plan, size_t first, size_t count);
 /* Synchronize and report whether a bounded wait inside a fused pass expired
  * since the last qs_plan_apply (QS_ERR_STATE) - a watchdog, not expected. */

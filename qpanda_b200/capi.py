@@ -75,6 +75,9 @@ def lib():
         "qs_norm2": (i, [vp, dp]),
         "qs_inner": (i, [vp, vp, dp, dp]),
         "qs_plan_create": (i, [i, vp, sz, i, C.POINTER(vp)]),
+        "qs_plan_create_ex": (i, [i, vp, sz, vp, C.POINTER(vp)]),
+        "qs_plan_default_opts": (i, [vp]),
+        "qs_plan_launches": (i, [vp, C.POINTER(sz)]),
         "qs_plan_destroy": (i, [vp]),
         "qs_plan_info": (i, [vp, C.POINTER(sz), C.POINTER(sz)]),
         "qs_plan_block": (i, [vp, sz, ip, ip, dp]),
@@ -232,16 +235,38 @@ class StateVector:
         return complex(re.value, im.value)
 
 
-class FusionPlan:
-    """Gate list fused into dense 5-qubit blocks (qs_plan_*)."""
+class PlanOpts(C.Structure):
+    _fields_ = [("block_qubits", C.c_int), ("tile_qubits", C.c_int), ("max_sub", C.c_int),
+                ("low_qubits", C.c_int), ("kernel", C.c_int)]
 
-    def __init__(self, n, gates, max_k=5):
+
+PLAN_SINGLE, PLAN_TILED = 1, 2
+
+
+class FusionPlan:
+    """Gate list fused into dense 5-qubit blocks (qs_plan_*).  kernel="tiled"
+    (default) applies up to max_sub blocks per pass over the state;
+    kernel="single" one block per pass."""
+
+    def __init__(self, n, gates, max_k=5, kernel="tiled", max_sub=3, low_qubits=3):
         g = np.ascontiguousarray(gates, dtype=GATE_DTYPE)
         self._keep = g
         h = C.c_void_p()
-        check(lib().qs_plan_create(int(n), g.ctypes.data, g.size, int(max_k), C.byref(h)))
+        if kernel == "single":
+            check(lib().qs_plan_create(int(n), g.ctypes.data, g.size, int(max_k), C.byref(h)))
+        else:
+            o = PlanOpts()
+            check(lib().qs_plan_default_opts(C.byref(o)))
+            o.block_qubits, o.max_sub, o.low_qubits = int(max_k), int(max_sub), int(low_qubits)
+            check(lib().qs_plan_create_ex(int(n), g.ctypes.data, g.size, C.byref(o), C.byref(h)))
         self._h = h
         self.n = int(n)
+        self.kernel = kernel
+
+    def num_launches(self):
+        nl = C.c_size_t()
+        check(lib().qs_plan_launches(self._h, C.byref(nl)))
+        return nl.value
 
     def close(self):
         if self._h:

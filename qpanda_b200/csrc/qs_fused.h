@@ -22,3 +22,20 @@ int qs_fused_grid(const qs_state *s);
 // Launch one block on a complex64 state (n >= 12) on the state's stream.
 // err_dev: device int set to 1 if a bounded wait inside the kernel expired.
 int qs_launch_fused(qs_state *s, const qs_fused_desc *d, int *err_dev);
+
+// One tiled pass: 12 tile qubits T (ascending) and nsub (1..3) blocks, each
+// on 5 of them (ascending), applied in order; mat_dev holds the blocks'
+// BF16 [2][64][64] matrices back to back.
+struct qs_tiled_desc {
+    int T[12];
+    int nsub;
+    int qpos[3][5];
+    const void *mat_dev;
+    const double *norm0;
+    const double *prev_out;
+    double *in_parts;
+    double *out_parts;
+};
+
+int qs_tiled_grid(const qs_state *s);
+int qs_launch_tiled(qs_state *s, const qs_tiled_desc *d, int *err_dev);

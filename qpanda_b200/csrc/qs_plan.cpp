@@ -30,11 +30,20 @@ struct PlanBlock {
     std::vector<size_t> gates;           // indices into the gate list, in application order
 };
 
+// A pass of the tiled kernel: one read and one write of the state, applying
+// up to 3 consecutive blocks (sub-blocks) whose qubits lie in the 12 tile qubits.
+struct PlanPass {
+    int T[12] = {0};                     // ascending global qubits of the tile
+    size_t first = 0, count = 0;         // its blocks: blocks[first, first + count)
+};
+
 struct qs_plan {
     int n = 0;
     int max_k = 5;
+    qs_plan_opts opts;
     std::vector<qs_gate> gates;
     std::vector<PlanBlock> blocks;
+    std::vector<PlanPass> passes;        // tiled kernel only
     int dev = -1;                        // device holding mats
     void *mats = nullptr;                // [blocks][2][64][64] bf16
 };
@@ -84,11 +93,85 @@ float bf16_float(uint16_t h)
     return f;
 }
 
-int build_blocks(qs_plan *P)
+// Greedy fusion of the gates idx[] (in list order) into groups of at most k
+// qubits: a gate joins the open group when no earlier unplaced gate shares a
+// qubit with it (so it only moves past gates it commutes with) and the group
+// stays within k qubits.  Returns the groups' member lists and qubit masks.
+std::vector<std::pair<uint64_t, std::vector<size_t>>> greedy_groups(const std::vector<size_t> &idx,
+                                                                    const std::vector<uint64_t> &mask, int k,
+                                                                    uint64_t seed_mask = 0, int max_groups = 0)
+{
+    std::vector<std::pair<uint64_t, std::vector<size_t>>> out;
+    std::vector<char> done(idx.size(), 0);
+    size_t left = idx.size(), first = 0;
+    while (left) {
+        uint64_t Q = seed_mask;
+        std::vector<size_t> mem;
+        bool changed = true;
+        while (changed) {
+            changed = false;
+            uint64_t blocked = 0;
+            while (first < idx.size() && done[first]) ++first;
+            for (size_t t = first; t < idx.size(); ++t) {
+                if (done[t]) continue;
+                const uint64_t m = mask[idx[t]];
+                if (!(m & blocked) && __builtin_popcountll(Q | m) <= k) {
+                    done[t] = 1;
+                    --left;
+                    Q |= m;
+                    mem.push_back(idx[t]);
+                    changed = true;
+                } else {
+                    blocked |= m;
+                }
+            }
+        }
+        out.push_back(std::make_pair(Q, std::move(mem)));
+        if (max_groups && (int)out.size() > max_groups) break;
+    }
+    return out;
+}
+
+// Block unitary: qubits q[0..4] ascending (global), gates applied in order.
+void block_unitary(PlanBlock &B, const std::vector<qs_prim> &prim)
+{
+    B.U.assign(32 * 32, cd(0, 0));
+    std::vector<cd> col(32);
+    for (int c = 0; c < 32; ++c) {
+        std::fill(col.begin(), col.end(), cd(0, 0));
+        col[c] = 1;
+        for (size_t gi : B.gates) {
+            qs_prim lp = prim[gi];
+            lp.holes = remap(lp.holes, B.q, 5);
+            lp.cmask = remap(lp.cmask, B.q, 5);
+            lp.off0 = remap(lp.off0, B.q, 5);
+            lp.off1 = remap(lp.off1, B.q, 5);
+            apply_local(lp, col.data(), 5);
+        }
+        for (int r = 0; r < 32; ++r) B.U[r * 32 + c] = col[r];
+    }
+}
+
+// Widen a mask to `want` qubits with the lowest free qubits of `pool`.
+uint64_t widen(uint64_t Q, uint64_t pool, int want)
+{
+    for (int q = 0; q < 64 && __builtin_popcountll(Q) < want; ++q)
+        if ((pool >> q) & 1ull) Q |= 1ull << q;
+    return Q;
+}
+
+void mask_to_list(uint64_t Q, int *out)
+{
+    int k = 0;
+    for (int q = 0; q < 64; ++q)
+        if ((Q >> q) & 1ull) out[k++] = q;
+}
+
+int lower_all(qs_plan *P, std::vector<qs_prim> &prim, std::vector<uint64_t> &mask)
 {
     const size_t G = P->gates.size();
-    std::vector<uint64_t> mask(G);
-    std::vector<qs_prim> prim(G);
+    prim.resize(G);
+    mask.resize(G);
     for (size_t i = 0; i < G; ++i) {
         int r = qs_lower_gate(P->n, &P->gates[i], &prim[i]);
         if (r) return r;
@@ -97,52 +180,86 @@ int build_blocks(qs_plan *P)
             return qs_fail(QS_ERR_UNSUPPORTED, "plan: gate %zu touches %d qubits (fusion width %d)", i,
                            __builtin_popcountll(mask[i]), P->max_k);
     }
-    std::vector<char> done(G, 0);
-    size_t left = G, first = 0;
-    while (left) {
+    return QS_OK;
+}
+
+// Single-block passes: every block is one pass of k_fused_tc.
+int build_blocks(qs_plan *P)
+{
+    std::vector<qs_prim> prim;
+    std::vector<uint64_t> mask;
+    int r = lower_all(P, prim, mask);
+    if (r) return r;
+    std::vector<size_t> all(P->gates.size());
+    for (size_t i = 0; i < all.size(); ++i) all[i] = i;
+    const uint64_t every = P->n >= 64 ? ~0ull : ((1ull << P->n) - 1);
+    for (auto &grp : greedy_groups(all, mask, P->max_k)) {
         PlanBlock B;
-        uint64_t Q = 0;
+        B.gates = grp.second;
+        mask_to_list(widen(grp.first, every, 5), B.q);
+        B.k = 5;
+        block_unitary(B, prim);
+        P->blocks.push_back(std::move(B));
+    }
+    return QS_OK;
+}
+
+// Tiled passes: a pass takes gates while its qubits stay within tile_qubits
+// (the lowest low_qubits always included, so that every row of the tile is a
+// run of at least 2^low_qubits contiguous amplitudes) and its gates still
+// fuse into at most max_sub blocks of 5 qubits.
+int build_passes(qs_plan *P)
+{
+    std::vector<qs_prim> prim;
+    std::vector<uint64_t> mask;
+    int r = lower_all(P, prim, mask);
+    if (r) return r;
+    const int TQ = P->opts.tile_qubits, MS = P->opts.max_sub;
+    const uint64_t every = P->n >= 64 ? ~0ull : ((1ull << P->n) - 1);
+    const uint64_t low = (1ull << P->opts.low_qubits) - 1;
+    const size_t G = P->gates.size();
+    std::vector<char> done(G, 0);
+    size_t left = G;
+    while (left) {
+        uint64_t T = low;
+        std::vector<size_t> mem;
         bool changed = true;
         while (changed) {
             changed = false;
             uint64_t blocked = 0;
-            while (first < G && done[first]) ++first;
-            for (size_t i = first; i < G; ++i) {
+            for (size_t i = 0; i < G; ++i) {
                 if (done[i]) continue;
                 const uint64_t m = mask[i];
-                if (!(m & blocked) && __builtin_popcountll(Q | m) <= P->max_k) {
-                    done[i] = 1;
-                    --left;
-                    Q |= m;
-                    B.gates.push_back(i);
-                    changed = true;
-                } else {
-                    blocked |= m;
+                if (!(m & blocked) && __builtin_popcountll(T | m) <= TQ) {
+                    std::vector<size_t> trial = mem;
+                    trial.push_back(i);
+                    if ((int)greedy_groups(trial, mask, 5, 0, MS).size() <= MS) {
+                        done[i] = 1;
+                        --left;
+                        T |= m;
+                        mem.push_back(i);
+                        changed = true;
+                        continue;
+                    }
                 }
+                blocked |= m;
             }
         }
-        // widen to 5 qubits with the lowest free ones
-        for (int q = 0; q < P->n && __builtin_popcountll(Q) < 5; ++q) Q |= 1ull << q;
-        B.k = 0;
-        for (int q = 0; q < P->n; ++q)
-            if (Q & (1ull << q)) B.q[B.k++] = q;
-        // U = product of the block's gates, column by column
-        B.U.assign(32 * 32, cd(0, 0));
-        std::vector<cd> col(32);
-        for (int c = 0; c < 32; ++c) {
-            std::fill(col.begin(), col.end(), cd(0, 0));
-            col[c] = 1;
-            for (size_t gi : B.gates) {
-                qs_prim lp = prim[gi];
-                lp.holes = remap(lp.holes, B.q, 5);
-                lp.cmask = remap(lp.cmask, B.q, 5);
-                lp.off0 = remap(lp.off0, B.q, 5);
-                lp.off1 = remap(lp.off1, B.q, 5);
-                apply_local(lp, col.data(), 5);
-            }
-            for (int r = 0; r < 32; ++r) B.U[r * 32 + c] = col[r];
+        if (mem.empty()) return qs_fail(QS_ERR_UNSUPPORTED, "plan: no gate fits a %d-qubit tile", TQ);
+        PlanPass pass;
+        T = widen(T, every, TQ);
+        mask_to_list(T, pass.T);
+        pass.first = P->blocks.size();
+        for (auto &grp : greedy_groups(mem, mask, 5)) {
+            PlanBlock B;
+            B.gates = grp.second;
+            mask_to_list(widen(grp.first, T, 5), B.q);
+            B.k = 5;
+            block_unitary(B, prim);
+            P->blocks.push_back(std::move(B));
         }
-        P->blocks.push_back(std::move(B));
+        pass.count = P->blocks.size() - pass.first;
+        P->passes.push_back(pass);
     }
     return QS_OK;
 }
@@ -172,19 +289,53 @@ extern "C" int qs_plan_apply_range(qs_state *s, qs_plan *P, size_t first, size_t
 
 extern "C" int qs_plan_create(int n, const qs_gate *gates, size_t count, int max_k, qs_plan **out)
 {
+    qs_plan_opts o;
+    o.block_qubits = max_k;
+    o.tile_qubits = 12;
+    o.max_sub = 1;
+    o.low_qubits = 0;
+    o.kernel = QS_PLAN_SINGLE;
+    return qs_plan_create_ex(n, gates, count, &o, out);
+}
+
+extern "C" int qs_plan_default_opts(qs_plan_opts *o)
+{
+    if (!o) return qs_fail(QS_ERR_ARG, "qs_plan_default_opts: null");
+    o->block_qubits = 5;
+    o->tile_qubits = 12;
+    o->max_sub = 3;
+    o->low_qubits = 3;
+    o->kernel = QS_PLAN_TILED;
+    return QS_OK;
+}
+
+extern "C" int qs_plan_create_ex(int n, const qs_gate *gates, size_t count, const qs_plan_opts *opts,
+                                 qs_plan **out)
+{
     if (!out) return qs_fail(QS_ERR_ARG, "qs_plan_create: null output");
     *out = nullptr;
+    qs_plan_opts o;
+    if (opts) o = *opts;
+    else qs_plan_default_opts(&o);
     if (n < 1 || n > QS_MAX_QUBITS) return qs_fail(QS_ERR_ARG, "qs_plan_create: bad qubit count %d", n);
-    if (max_k < 1 || max_k > 5)
-        return qs_fail(QS_ERR_UNSUPPORTED, "qs_plan_create: fusion width %d (this build fuses up to 5 qubits)", max_k);
+    if (o.block_qubits < 1 || o.block_qubits > 5)
+        return qs_fail(QS_ERR_UNSUPPORTED, "qs_plan_create: fusion width %d (this build fuses up to 5 qubits)",
+                       o.block_qubits);
+    if (o.kernel != QS_PLAN_SINGLE && o.kernel != QS_PLAN_TILED)
+        return qs_fail(QS_ERR_ARG, "qs_plan_create: unknown kernel %d", o.kernel);
+    if (o.kernel == QS_PLAN_TILED &&
+        (o.tile_qubits != 12 || o.max_sub < 1 || o.max_sub > 3 || o.low_qubits < 1 || o.low_qubits > 5))
+        return qs_fail(QS_ERR_UNSUPPORTED,
+                       "qs_plan_create: tiled passes need tile_qubits 12, max_sub 1..3, low_qubits 1..5");
     if (count && !gates) return qs_fail(QS_ERR_ARG, "qs_plan_create: null gate list");
     qs_plan *P = new qs_plan();
     P->n = n;
-    P->max_k = max_k;
+    P->max_k = o.block_qubits;
+    P->opts = o;
     P->gates.assign(gates, gates + count);
     // Below 12 qubits a state has fewer than one 128 x 32 tile: the plan keeps
     // the gate list only and runs it through the per-gate kernels.
-    int r = n >= 12 ? build_blocks(P) : QS_OK;
+    int r = n < 12 ? QS_OK : o.kernel == QS_PLAN_TILED ? build_passes(P) : build_blocks(P);
     if (r) { delete P; return r; }
     *out = P;
     return QS_OK;
@@ -242,9 +393,21 @@ int qs_plan_upload(qs_plan *P, int dev)
 
 int qs_launch_prim(qs_state *s, const qs_prim &p);
 
+static size_t plan_launches(const qs_plan *P)
+{
+    return P->opts.kernel == QS_PLAN_TILED ? P->passes.size() : P->blocks.size();
+}
+
+extern "C" int qs_plan_launches(const qs_plan *P, size_t *n)
+{
+    if (!P || !n) return qs_fail(QS_ERR_ARG, "qs_plan_launches: null argument");
+    *n = plan_launches(P);
+    return QS_OK;
+}
+
 extern "C" int qs_plan_apply(qs_state *s, qs_plan *P)
 {
-    return qs_plan_apply_range(s, P, 0, P ? P->blocks.size() : 0);
+    return qs_plan_apply_range(s, P, 0, P ? plan_launches(P) : 0);
 }
 
 extern "C" int qs_plan_apply_range(qs_state *s, qs_plan *P, size_t first, size_t count)
@@ -261,10 +424,15 @@ extern "C" int qs_plan_apply_range(qs_state *s, qs_plan *P, size_t first, size_t
         if (P->blocks.empty()) {
             for (size_t i = 0; i < P->gates.size(); ++i) idx.push_back(i);
         } else {
-            if (first > P->blocks.size() || count > P->blocks.size() - first)
-                return qs_fail(QS_ERR_ARG, "qs_plan_apply_range: blocks [%zu, +%zu) out of range", first, count);
-            for (size_t b = first; b < first + count; ++b)
-                idx.insert(idx.end(), P->blocks[b].gates.begin(), P->blocks[b].gates.end());
+            const size_t nl = plan_launches(P);
+            if (first > nl || count > nl - first)
+                return qs_fail(QS_ERR_ARG, "qs_plan_apply_range: launches [%zu, +%zu) out of range", first, count);
+            for (size_t u = first; u < first + count; ++u) {
+                size_t b0 = u, b1 = u + 1;
+                if (P->opts.kernel == QS_PLAN_TILED) { b0 = P->passes[u].first; b1 = b0 + P->passes[u].count; }
+                for (size_t b = b0; b < b1; ++b)
+                    idx.insert(idx.end(), P->blocks[b].gates.begin(), P->blocks[b].gates.end());
+            }
         }
         for (size_t i : idx) {
             qs_prim p;
@@ -272,8 +440,8 @@ extern "C" int qs_plan_apply_range(qs_state *s, qs_plan *P, size_t first, size_t
         }
         return QS_OK;
     }
-    if (first > P->blocks.size() || count > P->blocks.size() - first)
-        return qs_fail(QS_ERR_ARG, "qs_plan_apply_range: blocks [%zu, +%zu) out of range", first, count);
+    if (first > plan_launches(P) || count > plan_launches(P) - first)
+        return qs_fail(QS_ERR_ARG, "qs_plan_apply_range: launches [%zu, +%zu) out of range", first, count);
     if ((r = qs_plan_upload(P, s->device))) return r;
     // Norm partials live in their own per-state buffer, so that other calls
     // between two qs_plan_apply_range calls cannot overwrite them:
@@ -286,6 +454,25 @@ extern "C" int qs_plan_apply_range(qs_state *s, qs_plan *P, size_t first, size_t
     int *flag = reinterpret_cast<int *>(static_cast<char *>(s->scratch) + kFlagOff);
     if (first == 0) QS_CUDA_TRY(cudaMemsetAsync(flag, 0, sizeof(int), s->stream));
     const size_t per = 2 * 64 * 64 * sizeof(uint16_t);
+    if (P->opts.kernel == QS_PLAN_TILED) {
+        const int GT = qs_tiled_grid(s);
+        for (size_t u = first; u < first + count; ++u) {
+            const PlanPass &pp = P->passes[u];
+            qs_tiled_desc d;
+            memset(&d, 0, sizeof(d));
+            for (int i = 0; i < 12; ++i) d.T[i] = pp.T[i];
+            d.nsub = (int)pp.count;
+            for (size_t b = 0; b < pp.count; ++b)
+                for (int j = 0; j < 5; ++j) d.qpos[b][j] = P->blocks[pp.first + b].q[j];
+            d.mat_dev = static_cast<const char *>(P->mats) + pp.first * per;
+            d.norm0 = u ? norm : nullptr;
+            d.prev_out = u ? norm + GT * (1 + (u - 1) % 2) : nullptr;
+            d.in_parts = u ? nullptr : norm;
+            d.out_parts = norm + GT * (1 + u % 2);
+            if ((r = qs_launch_tiled(s, &d, flag))) return r;
+        }
+        return QS_OK;
+    }
     for (size_t b = first; b < first + count; ++b) {
         qs_fused_desc d;
         for (int j = 0; j < 5; ++j) d.qpos[j] = P->blocks[b].q[j];
@@ -308,6 +495,7 @@ extern "C" int qs_plan_status(qs_state *s)
     QS_CUDA_TRY(cudaMemcpyAsync(&flag, static_cast<char *>(s->scratch) + kFlagOff, sizeof(int),
                                 cudaMemcpyDeviceToHost, s->stream));
     QS_CUDA_TRY(cudaStreamSynchronize(s->stream));
+    if (flag == 2) return qs_fail(QS_ERR_STATE, "fused pass: dynamic shared memory not 1024-byte aligned");
     if (flag) return qs_fail(QS_ERR_STATE, "fused pass: a bounded wait in the tensor-core kernel expired");
     return QS_OK;
 }

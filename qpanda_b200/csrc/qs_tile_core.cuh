@@ -1,0 +1,196 @@
+// qs_tile_core.cuh - device building blocks of the tiled tensor-core passes
+// (qs_fused2.cu: one circuit, many CTAs; qs_batch.cu: many circuits, one CTA
+// each).  A tile is 4096 complex64 amplitudes that differ in 12 tile qubits;
+// for a 5-qubit block it is 128 rows (7 tile bits) x 32 columns (the block's
+// 5 bits).  Thread i of 128 owns row i and TMEM lane i.
+#pragma once
+
+#include <cuda_bf16.h>
+
+#include "qs_common.cuh"
+
+namespace qs_tile {
+
+constexpr int kThreads = 128;
+constexpr uint32_t kTmemCols = 64;
+constexpr uint32_t kA = 128 * 64 * 2;             // 16 KB: one BF16 A buffer (128 rows x 64)
+constexpr uint32_t kB = 64 * 64 * 2;              //  8 KB: one BF16 B buffer
+constexpr uint32_t kStage = 128 * 256;            // 32 KB: 128 rows x 32 complex64
+constexpr int kMaxSub = 3;
+// instruction descriptor: D f32 (bits 4-5 = 1), A and B bf16 (7-9, 10-12 = 1),
+// both K-major, N = 64 (N>>3 at 17-22), M = 128 (M>>4 at 24-28)
+constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(64 >> 3) << 17) |
+                            ((uint32_t)(128 >> 4) << 24);
+constexpr unsigned long long kWaitNs = 2000000000ull;   // bound on every wait
+
+// Layout of one pass over a tile: where block 0's rows come from, how each
+// block's results feed the next block's rows and columns, where the last
+// block's results go.  Built on the host (qs_tile_layout_build).
+struct Layout {
+    uint64_t outer_low[12];      // (1 << tile position) - 1, ascending: tile index -> global base
+    uint64_t g0[32];             // global offset of column j, block 0
+    uint64_t gl[32];             // global offset of column j, last block
+    int32_t c0_glob[7];          // global position of row bit i, block 0
+    int32_t cl_glob[7];          // global position of row bit i, last block
+    int32_t nsub, vec0, vecl, pad;
+    int8_t rowmap[kMaxSub - 1][7];   // row bit i of block b -> row bit (>= 0) or ~column bit of block b+1
+    uint8_t tabR[kMaxSub - 1][32];   // column j of block b -> row bits of block b+1
+    uint8_t tabJ[kMaxSub - 1][32];   // column j of block b -> column bits of block b+1
+};
+
+__device__ __forceinline__ uint64_t tile_base(uint64_t tile, const Layout &L)
+{
+#pragma unroll
+    for (int j = 0; j < 12; ++j) {
+        const uint64_t lo = tile & L.outer_low[j];
+        tile = ((tile & ~L.outer_low[j]) << 1) | lo;
+    }
+    return tile;
+}
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// UMMA shared-memory descriptor: K-major, 128-byte swizzle, rows of 128 B in
+// 8-row groups 1024 B apart, version 1 (sm_100).
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr)
+{
+    return (uint64_t)((saddr >> 4) & 0x3FFFu) | (1ull << 16) | (64ull << 32) | (1ull << 46) | (2ull << 61);
+}
+
+__device__ __forceinline__ uint32_t pack_bf16x2(float a, float b)
+{
+    __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
+    return *reinterpret_cast<uint32_t *>(&h);
+}
+
+__device__ __forceinline__ unsigned long long globaltimer()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Bounded wait on an mbarrier phase: false after kWaitNs.
+__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity)
+{
+    const unsigned long long t0 = globaltimer();
+    while (true) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred P1;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+            "selp.b32 %0, 1, 0, P1;\n\t}\n"
+            : "=r"(done)
+            : "r"(mbar), "r"(parity)
+            : "memory");
+        if (done) return true;
+        if (globaltimer() - t0 > kWaitNs) return false;
+    }
+}
+
+__device__ __forceinline__ void mma_bf16(uint32_t d_tmem, uint64_t da, uint64_t db, uint32_t acc)
+{
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n"
+        :
+        : "r"(d_tmem), "l"(da), "l"(db), "r"(kIdesc), "r"(acc));
+}
+
+// D = A_hi*B_hi + A_hi*B_lo + A_lo*B_hi (12 MMAs of K = 16), then commit.
+__device__ __forceinline__ void issue_block_mma(uint32_t tmem, uint32_t a_hi, uint32_t a_lo, uint32_t b_hi,
+                                                uint32_t b_lo, uint32_t mbar)
+{
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint64_t dAh = umma_desc(a_hi), dAl = umma_desc(a_lo), dBh = umma_desc(b_hi), dBl = umma_desc(b_lo);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) mma_bf16(tmem, dAh + 2 * k, dBh + 2 * k, k > 0);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) mma_bf16(tmem, dAh + 2 * k, dBl + 2 * k, 1);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) mma_bf16(tmem, dAl + 2 * k, dBh + 2 * k, 1);
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                 :: "r"(mbar) : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16])
+{
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+        "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+          "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+          "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+}
+
+// Staging row of thread `row`: 16 chunks of 16 B (2 amplitudes), chunk k at
+// position k ^ (row & 15) so that a quarter warp's 8 rows hit distinct banks.
+__device__ __forceinline__ uint32_t stage_addr(uint32_t stage, int row, int chunk)
+{
+    return stage + row * 256 + ((chunk ^ (row & 15)) << 4);
+}
+
+// Asynchronous copies of this thread's row of block 0 (tile base `base`)
+// into its staging row.  L2-only copies (.cg) when columns come in 16-byte
+// pairs; 8-byte copies otherwise.
+__device__ __forceinline__ void prefetch_row(const float *amp, uint64_t base, const Layout &L, uint32_t stage,
+                                             int row)
+{
+    if (L.vec0) {
+#pragma unroll
+        for (int j = 0; j < 32; j += 2) {
+            const float *src = amp + 2 * (base | L.g0[j]);
+            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" :: "r"(stage_addr(stage, row, j >> 1)),
+                         "l"(src) : "memory");
+        }
+    } else {
+#pragma unroll
+        for (int j = 0; j < 32; ++j) {
+            const float *src = amp + 2 * (base | L.g0[j]);
+            asm volatile("cp.async.ca.shared.global [%0], [%1], 8;"
+                         :: "r"(stage_addr(stage, row, j >> 1) + ((j & 1) << 3)), "l"(src) : "memory");
+        }
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+}
+
+__device__ __forceinline__ void read_stage_row(uint32_t stage, int row, float (&x)[64])
+{
+#pragma unroll
+    for (int k = 0; k < 16; ++k) {
+        float4 v;
+        asm volatile("ld.shared.v4.f32 {%0,%1,%2,%3}, [%4];"
+                     : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w) : "r"(stage_addr(stage, row, k)));
+        x[4 * k] = v.x; x[4 * k + 1] = v.y; x[4 * k + 2] = v.z; x[4 * k + 3] = v.w;
+    }
+}
+
+// One complex amplitude (re, im) as BF16 hi/lo pairs at row r, column j of
+// the swizzled K-major A buffers.
+__device__ __forceinline__ void a_store_pair(uint8_t *aHi, uint8_t *aLo, int r, int j, float re, float im)
+{
+    const uint32_t hv = pack_bf16x2(re, im);
+    const float hre = __uint_as_float(hv << 16), him = __uint_as_float(hv & 0xffff0000u);
+    const uint32_t lv = pack_bf16x2(re - hre, im - him);
+    const uint32_t off = r * 128 + ((((j >> 2) ^ (r & 7))) << 4) + ((j & 3) << 2);
+    *reinterpret_cast<uint32_t *>(aHi + off) = hv;
+    *reinterpret_cast<uint32_t *>(aLo + off) = lv;
+}
+
+// B operands of a pass (nsub blocks, hi and lo each) into the swizzled layout.
+__device__ __forceinline__ void load_b(uint8_t *dst, const uint16_t *mat, int nsub)
+{
+    for (int c = threadIdx.x; c < nsub * 2 * 64 * 8; c += kThreads) {
+        const int mtx = c / (64 * 8), row = (c / 8) % 64, ch = c % 8;
+        uint4 v = *reinterpret_cast<const uint4 *>(mat + (size_t)mtx * 64 * 64 + row * 64 + ch * 8);
+        *reinterpret_cast<uint4 *>(dst + mtx * kB + row * 128 + ((ch ^ (row & 7)) << 4)) = v;
+    }
+}
+
+}  // namespace qs_tile
+
+// Host: the Layout of a pass with tile qubits T[12] (ascending, global) and
+// nsub blocks on qpos[b][5] (ascending, within T).  QS_OK or QS_ERR_ARG.
+int qs_tile_layout_build(int n, const int *T, int nsub, const int (*qpos)[5], qs_tile::Layout *L);

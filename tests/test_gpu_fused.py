@@ -19,13 +19,16 @@ def random_state(n, seed):
     return v / np.linalg.norm(v)
 
 
-def check_fused(n, g, init=None):
+KERNELS = ["single", "tiled"]
+
+
+def check_fused(n, g, init=None, kernel="tiled"):
     sv = StateVector(n, "c64")
     o = OracleState(n)
     if init is not None:
         sv.set_state(init.astype(np.complex64))
         o.set_state(init.astype(np.complex64).astype(np.complex128))
-    p = FusionPlan(n, g)
+    p = FusionPlan(n, g, kernel=kernel)
     p.apply(sv)
     p.status(sv)
     o.apply(g)
@@ -37,19 +40,31 @@ def check_fused(n, g, init=None):
     return p.num_blocks()
 
 
+@pytest.mark.parametrize("kernel", KERNELS)
 @pytest.mark.parametrize("n", [12, 13, 17])
-def test_fused_random_layers(need_gpu, n):
-    nb = check_fused(n, circuits.random_layers(n, 8, 40 + n, iswap_frac=0.1))
+def test_fused_random_layers(need_gpu, n, kernel):
+    nb = check_fused(n, circuits.random_layers(n, 8, 40 + n, iswap_frac=0.1), kernel=kernel)
     assert nb > 0
 
 
-def test_fused_qft_gaussian(need_gpu):
-    check_fused(14, circuits.qft(14), init=random_state(14, 2))
+@pytest.mark.parametrize("kernel", KERNELS)
+def test_fused_qft_gaussian(need_gpu, kernel):
+    check_fused(14, circuits.qft(14), init=random_state(14, 2), kernel=kernel)
 
 
-def test_fused_every_gate_kind(need_gpu):
+@pytest.mark.parametrize("kernel", KERNELS)
+def test_fused_every_gate_kind(need_gpu, kernel):
     from tests.golden.make_golden import every_gate_circuit
-    check_fused(12, every_gate_circuit(12, 9), init=random_state(12, 3))
+    check_fused(12, every_gate_circuit(12, 9), init=random_state(12, 3), kernel=kernel)
+
+
+@pytest.mark.parametrize("max_sub", [1, 2, 3])
+@pytest.mark.parametrize("low", [1, 3, 5])
+def test_tiled_options(need_gpu, max_sub, low):
+    """Every blocks-per-pass count and tile shape of the tiled kernel."""
+    n = 15
+    check_fused(n, circuits.random_layers(n, 6, 70 + max_sub + 10 * low, iswap_frac=0.2),
+                init=random_state(n, max_sub), kernel="tiled")
 
 
 def test_fused_block_positions(need_gpu):
@@ -66,15 +81,17 @@ def test_fused_block_positions(need_gpu):
             spec.append(("CNOT", (a, b)))
             spec.append(("SQISWAP", (b, a)))
         g = circuits.make_gates(spec)
-        p = FusionPlan(n, g)
-        assert p.num_blocks() == 1 and p.block(0)[0] == sorted(qs)
-        check_fused(n, g, init=random_state(n, qs[0] + 7))
+        for kernel in KERNELS:
+            p = FusionPlan(n, g, kernel=kernel)
+            assert p.num_blocks() == 1 and p.block(0)[0] == sorted(qs)
+            check_fused(n, g, init=random_state(n, qs[0] + 7), kernel=kernel)
 
 
-def test_fused_vqe_and_reuse(need_gpu):
+@pytest.mark.parametrize("kernel", KERNELS)
+def test_fused_vqe_and_reuse(need_gpu, kernel):
     n = 16
     g = circuits.vqe_ansatz(n, 4, seed=5)
-    p = FusionPlan(n, g)
+    p = FusionPlan(n, g, kernel=kernel)
     a = StateVector(n, "c64")
     p.apply(a)
     p.apply(a)               # a plan applies repeatedly
@@ -84,13 +101,14 @@ def test_fused_vqe_and_reuse(need_gpu):
     assert np.abs(a.get_state() - o.state()).max() < AMP_TOL
 
 
-def test_fused_fidelity_26q_vs_fp64_gpu(need_gpu):
+@pytest.mark.parametrize("kernel", KERNELS)
+def test_fused_fidelity_26q_vs_fp64_gpu(need_gpu, kernel):
     """26 qubits, 12 layers: fused complex64 against the complex128 per-gate
     path (itself pinned to the oracle by the other tests)."""
     n = 26
     g = circuits.random_layers(n, 12, 7, iswap_frac=0.1)
     f = StateVector(n, "c64")
-    p = FusionPlan(n, g)
+    p = FusionPlan(n, g, kernel=kernel)
     p.apply(f)
     p.status(f)
     d = StateVector(n, "c128")
@@ -102,15 +120,16 @@ def test_fused_fidelity_26q_vs_fp64_gpu(need_gpu):
     assert abs(f.norm2() - 1) < 2e-6, f.norm2()
 
 
-def test_fused_range_with_interleaved_probs(need_gpu):
-    """Blocks applied one at a time with a marginal computed in between give
+@pytest.mark.parametrize("kernel", KERNELS)
+def test_fused_range_with_interleaved_probs(need_gpu, kernel):
+    """Passes applied one at a time with a marginal computed in between give
     the same state as the whole plan (norm partials survive other calls)."""
     n = 20
     g = circuits.random_layers(n, 6, 11, iswap_frac=0.1)
-    p = FusionPlan(n, g)
+    p = FusionPlan(n, g, kernel=kernel)
     a, b = StateVector(n, "c64"), StateVector(n, "c64")
     p.apply(a)
-    for i in range(p.num_blocks()):
+    for i in range(p.num_launches()):
         p.apply_range(b, i, 1)
         b.probs(list(range(n)))
     mx, _ = a.diff(b)

@@ -18,8 +18,9 @@ def apply_block(v, n, qubits, U):
     return np.moveaxis(T, list(range(5)), axes).reshape(-1)
 
 
+@pytest.mark.parametrize("kernel", ["single", "tiled"])
 @pytest.mark.parametrize("case", ["layers", "qft", "every_gate", "vqe"])
-def test_plan_blocks_reproduce_oracle(case):
+def test_plan_blocks_reproduce_oracle(case, kernel):
     n = 13
     if case == "layers":
         g = circuits.random_layers(n, 6, 3, iswap_frac=0.3)
@@ -36,9 +37,10 @@ def test_plan_blocks_reproduce_oracle(case):
     o = OracleState(n)
     o.set_state(v)
     o.apply(g)
-    p = FusionPlan(n, g)
+    p = FusionPlan(n, g, kernel=kernel)
     nb = p.num_blocks()
     assert 0 < nb < len(g)
+    assert 0 < p.num_launches() <= nb
     w = v.copy()
     for i in range(nb):
         q, U = p.block(i)
@@ -50,8 +52,10 @@ def test_plan_blocks_reproduce_oracle(case):
 
 def test_plan_pass_count_32q():
     g = circuits.random_layers(32, 16, 20240601, iswap_frac=0.1)
-    p = FusionPlan(32, g)
-    assert p.num_blocks() <= 90           # vs 768 gates / ~640 full passes per gate
+    p = FusionPlan(32, g, kernel="single")
+    assert p.num_blocks() <= 90 and p.num_launches() == p.num_blocks()   # vs ~640 per-gate passes
+    t = FusionPlan(32, g, kernel="tiled")
+    assert t.num_launches() <= 40         # up to 3 blocks per pass within 12 tile qubits
 
 
 def test_plan_rejects_wide_gates_and_bad_width():
