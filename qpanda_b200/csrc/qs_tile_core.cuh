@@ -34,9 +34,28 @@ struct Layout {
     int32_t cl_glob[7];          // global position of row bit i, last block
     int32_t nsub, vec0, vecl, pad;
     int8_t rowmap[kMaxSub - 1][7];   // row bit i of block b -> row bit (>= 0) or ~column bit of block b+1
+    // Byte offset, within block b+1's swizzled A buffer, of the result in
+    // column j of block b is  thread_part ^ scat[b][j]: the row/column bits a
+    // result gets in block b+1 come either from the thread's row or from j,
+    // never both, so the swizzled offset splits into two XOR-able halves.
+    uint16_t scat[kMaxSub - 1][32];
     uint8_t tabR[kMaxSub - 1][32];   // column j of block b -> row bits of block b+1
     uint8_t tabJ[kMaxSub - 1][32];   // column j of block b -> column bits of block b+1
 };
+
+// Thread part of the scatter offset (see Layout::scat).
+__device__ __forceinline__ uint32_t scatter_thread_part(const Layout &L, int t, int row)
+{
+    uint32_t r2 = 0, j2 = 0;
+#pragma unroll
+    for (int b = 0; b < 7; ++b) {
+        const uint32_t bit = (row >> b) & 1;
+        const int m = L.rowmap[t][b];
+        if (m >= 0) r2 |= bit << m;
+        else j2 |= bit << (~m);
+    }
+    return (r2 << 7) | ((((j2 >> 2) ^ (r2 & 7)) & 7) << 4) | ((j2 & 3) << 2);
+}
 
 __device__ __forceinline__ uint64_t tile_base(uint64_t tile, const Layout &L)
 {
@@ -167,16 +186,49 @@ __device__ __forceinline__ void read_stage_row(uint32_t stage, int row, float (&
     }
 }
 
-// One complex amplitude (re, im) as BF16 hi/lo pairs at row r, column j of
-// the swizzled K-major A buffers.
+// BF16 hi/lo split of a complex pair: hi = bf16(x), lo = bf16(x - hi).
+__device__ __forceinline__ void split_pair(float re, float im, uint32_t &hv, uint32_t &lv)
+{
+    hv = pack_bf16x2(re, im);
+    lv = pack_bf16x2(re - __uint_as_float(hv << 16), im - __uint_as_float(hv & 0xffff0000u));
+}
+
+// One complex amplitude as BF16 hi/lo pairs at row r, column j of the
+// swizzled K-major A buffers.
 __device__ __forceinline__ void a_store_pair(uint8_t *aHi, uint8_t *aLo, int r, int j, float re, float im)
 {
-    const uint32_t hv = pack_bf16x2(re, im);
-    const float hre = __uint_as_float(hv << 16), him = __uint_as_float(hv & 0xffff0000u);
-    const uint32_t lv = pack_bf16x2(re - hre, im - him);
+    uint32_t hv, lv;
+    split_pair(re, im, hv, lv);
     const uint32_t off = r * 128 + ((((j >> 2) ^ (r & 7))) << 4) + ((j & 3) << 2);
     *reinterpret_cast<uint32_t *>(aHi + off) = hv;
     *reinterpret_cast<uint32_t *>(aLo + off) = lv;
+}
+
+// One complex amplitude as BF16 hi/lo pairs at byte offset `off` of the A buffers.
+__device__ __forceinline__ void a_store_at(uint8_t *aHi, uint8_t *aLo, uint32_t off, float re, float im)
+{
+    uint32_t hv, lv;
+    split_pair(re, im, hv, lv);
+    *reinterpret_cast<uint32_t *>(aHi + off) = hv;
+    *reinterpret_cast<uint32_t *>(aLo + off) = lv;
+}
+
+// A whole row (32 complex = 64 floats) as 16-byte chunks: chunk c (columns
+// 4c..4c+3) at position c ^ (row & 7) of the row's 128 bytes.
+__device__ __forceinline__ void a_store_row(uint8_t *aHi, uint8_t *aLo, int row, const float (&x)[64])
+{
+    uint8_t *rh = aHi + row * 128, *rl = aLo + row * 128;
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+        uint4 h, l;
+        split_pair(x[8 * c + 0], x[8 * c + 1], h.x, l.x);
+        split_pair(x[8 * c + 2], x[8 * c + 3], h.y, l.y);
+        split_pair(x[8 * c + 4], x[8 * c + 5], h.z, l.z);
+        split_pair(x[8 * c + 6], x[8 * c + 7], h.w, l.w);
+        const uint32_t pos = (uint32_t)(c ^ (row & 7)) << 4;
+        *reinterpret_cast<uint4 *>(rh + pos) = h;
+        *reinterpret_cast<uint4 *>(rl + pos) = l;
+    }
 }
 
 // B operands of a pass (nsub blocks, hi and lo each) into the swizzled layout.

@@ -67,6 +67,8 @@ int qs_tile_layout_build(int n, const int *T, int nsub, const int (*qpos)[5], qs
             }
             L->tabR[t][j] = (uint8_t)rr;
             L->tabJ[t][j] = (uint8_t)jj;
+            // swizzled offset bits contributed by column j (qs_tile::Layout::scat)
+            L->scat[t][j] = (uint16_t)((rr << 7) | ((((jj >> 2) ^ (rr & 7)) & 7) << 4) | ((jj & 3) << 2));
         }
     }
     return QS_OK;
