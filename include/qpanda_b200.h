@@ -233,6 +233,47 @@ int qs_plan_apply_range(qs_state *s, qs_plan *plan, size_t first, size_t count);
  * since the last qs_plan_apply (QS_ERR_STATE) - a watchdog, not expected. */
 int qs_plan_status(qs_state *s);
 
+/* ---- batched circuits: many circuits in one persistent launch ---------- */
+/* The reference runs one program per QPandaSDK::run (QPandaAPI.cpp:131-211); a
+ * parameter sweep is a host loop over runs.  A batch holds many independent
+ * circuits (up to 24 qubits each; narrower than 12 are padded with idle
+ * qubits), each with its own state in HBM and its own fused plan, and runs
+ * them all from |0...0> in one persistent kernel launch (captured in a CUDA
+ * graph when use_graph is set): the CTAs take whole circuits from a queue.
+ * After a run, qs_batch_zz gives every circuit's nearest-neighbour
+ * <Z_i Z_{i+1}> (i = 0..n-2), i.e. P00 + P11 - P01 - P10 of the pMeasure
+ * marginal on (i, i+1) (CPUQuantumGates.cpp:159-190).  No reference
+ * counterpart beyond that loop. */
+typedef struct qs_batch qs_batch;
+#define QS_BATCH_LONGEST_FIRST 0
+#define QS_BATCH_INPUT_ORDER   1
+typedef struct qs_batch_opts {
+    int max_sub;           /* fused blocks per pass, 1..3 */
+    int low_qubits;        /* qubits 0..low_qubits-1 in every tile, 1..5 */
+    int order;             /* QS_BATCH_LONGEST_FIRST or QS_BATCH_INPUT_ORDER */
+    int use_graph;         /* capture the launch in a CUDA graph and replay it */
+} qs_batch_opts;
+int qs_batch_default_opts(qs_batch_opts *opts);
+/* Circuit c has n_qubits[c] qubits and gates[offsets[c] .. offsets[c+1]). */
+int qs_batch_create(int n_circuits, const int *n_qubits, const qs_gate *gates, const size_t *offsets,
+                    const qs_batch_opts *opts, qs_batch **out);
+/* Run every circuit from |0...0> (asynchronous on `stream`). */
+int qs_batch_run(qs_batch *b, void *stream);
+/* Synchronize; copy the <Z_i Z_{i+1}> of all circuits, concatenated in
+ * circuit order (out may be NULL to query *count). */
+int qs_batch_zz(qs_batch *b, double *out, size_t *count);
+/* offsets[c] = first output of circuit c in qs_batch_zz's array; n+1 entries. */
+int qs_batch_zz_offsets(const qs_batch *b, size_t *offsets);
+/* Final state of circuit c (2^n_qubits[c] amplitudes) to the host. */
+int qs_batch_state(qs_batch *b, int circuit, void *host_out, int host_dtype);
+int qs_batch_info(const qs_batch *b, size_t *state_bytes, size_t *passes_total);
+int qs_batch_destroy(qs_batch *b);
+/* Autotuner: build and time candidate options (blocks per pass 1..3, lowest
+ * tile qubits 3 or 5, queue order) on every stride-th circuit and write the
+ * fastest to *best (with use_graph set) and its time per run to *best_ms. */
+int qs_batch_autotune(int n_circuits, const int *n_qubits, const qs_gate *gates, const size_t *offsets,
+                      int stride, qs_batch_opts *best, double *best_ms);
+
 #ifdef __cplusplus
 }
 #endif

@@ -75,6 +75,15 @@ def lib():
         "qs_norm2": (i, [vp, dp]),
         "qs_inner": (i, [vp, vp, dp, dp]),
         "qs_plan_create": (i, [i, vp, sz, i, C.POINTER(vp)]),
+        "qs_batch_default_opts": (i, [vp]),
+        "qs_batch_create": (i, [i, ip, vp, C.POINTER(sz), vp, C.POINTER(vp)]),
+        "qs_batch_run": (i, [vp, vp]),
+        "qs_batch_zz": (i, [vp, dp, C.POINTER(sz)]),
+        "qs_batch_zz_offsets": (i, [vp, C.POINTER(sz)]),
+        "qs_batch_state": (i, [vp, i, vp, i]),
+        "qs_batch_info": (i, [vp, C.POINTER(sz), C.POINTER(sz)]),
+        "qs_batch_destroy": (i, [vp]),
+        "qs_batch_autotune": (i, [i, ip, vp, C.POINTER(sz), i, vp, dp]),
         "qs_plan_create_ex": (i, [i, vp, sz, vp, C.POINTER(vp)]),
         "qs_plan_default_opts": (i, [vp]),
         "qs_plan_launches": (i, [vp, C.POINTER(sz)]),
@@ -303,3 +312,77 @@ class FusionPlan:
 
     def status(self, sv):
         check(lib().qs_plan_status(sv.handle))
+
+
+class BatchOpts(C.Structure):
+    _fields_ = [("max_sub", C.c_int), ("low_qubits", C.c_int), ("order", C.c_int), ("use_graph", C.c_int)]
+
+
+def _concat(circuits_list):
+    nq = np.array([n for n, _ in circuits_list], dtype=np.int32)
+    offs = np.zeros(len(circuits_list) + 1, dtype=np.uint64)
+    for k, (_, g) in enumerate(circuits_list):
+        offs[k + 1] = offs[k] + len(g)
+    gates = np.ascontiguousarray(np.concatenate([np.asarray(g, dtype=GATE_DTYPE) for _, g in circuits_list]),
+                                 dtype=GATE_DTYPE)
+    return nq, gates, offs
+
+
+def autotune_batch(circuits_list, stride=8):
+    """Fastest BatchOpts for these circuits (timed on every stride-th one) and
+    its time per run in ms."""
+    nq, gates, offs = _concat(circuits_list)
+    best, ms = BatchOpts(), C.c_double()
+    check(lib().qs_batch_autotune(len(nq), _iptr(nq), gates.ctypes.data,
+                                  offs.ctypes.data_as(C.POINTER(C.c_size_t)), int(stride), C.byref(best),
+                                  C.byref(ms)))
+    return best, ms.value
+
+
+class Batch:
+    """Many circuits run from |0...0> in one persistent launch (qs_batch_*).
+    circuits_list: [(n_qubits, gate records), ...]."""
+
+    def __init__(self, circuits_list, opts=None, **kw):
+        nq, gates, offs = _concat(circuits_list)
+        self.nq = nq
+        o = BatchOpts()
+        if opts is not None:
+            o = opts
+        else:
+            check(lib().qs_batch_default_opts(C.byref(o)))
+        for k, v in kw.items():
+            setattr(o, k, int(v))
+        h = C.c_void_p()
+        check(lib().qs_batch_create(len(nq), _iptr(nq), gates.ctypes.data,
+                                    offs.ctypes.data_as(C.POINTER(C.c_size_t)), C.byref(o), C.byref(h)))
+        self._h = h
+
+    def close(self):
+        if self._h:
+            lib().qs_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def run(self, stream=None):
+        check(lib().qs_batch_run(self._h, stream))
+
+    def zz(self):
+        """List of arrays: <Z_i Z_{i+1}> for each circuit."""
+        cnt = C.c_size_t()
+        check(lib().qs_batch_zz(self._h, None, C.byref(cnt)))
+        out = np.empty(cnt.value)
+        check(lib().qs_batch_zz(self._h, _dptr(out), C.byref(cnt)))
+        offs = np.empty(len(self.nq) + 1, dtype=np.uint64)
+        check(lib().qs_batch_zz_offsets(self._h, offs.ctypes.data_as(C.POINTER(C.c_size_t))))
+        return [out[int(offs[k]):int(offs[k + 1])] for k in range(len(self.nq))]
+
+    def state(self, c, dtype=np.complex128):
+        out = np.empty(1 << int(self.nq[c]), dtype=dtype)
+        check(lib().qs_batch_state(self._h, int(c), out.ctypes.data, QS_C64 if dtype == np.complex64 else QS_C128))
+        return out

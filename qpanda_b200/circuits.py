@@ -102,3 +102,16 @@ def gate_bytes(gates, n, amp_bytes):
             amps = N
         tot += 2 * amp_bytes * (amps >> c)
     return tot
+
+
+def vqe_sweep(n_circuits, seed, qmin=10, qmax=22, lmin=4, lmax=12):
+    """Batched variational sweep: circuit k has q ~ U{qmin..qmax} qubits and
+    L ~ U{lmin..lmax} layers of the hardware-efficient ansatz (vqe_ansatz),
+    angles uniform in [0, 2pi).  Returns [(q, gates), ...]."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n_circuits):
+        q = int(rng.integers(qmin, qmax + 1))
+        L = int(rng.integers(lmin, lmax + 1))
+        out.append((q, vqe_ansatz(q, L, angles=rng.uniform(0.0, 2 * math.pi, size=(L, 2, q)))))
+    return out

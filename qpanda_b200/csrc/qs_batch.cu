@@ -1,0 +1,614 @@
+// qs_batch.cu - many independent circuits in one persistent launch.
+//
+// The reference runs one program at a time (QPandaSDK::run, QPandaAPI.cpp:131-211);
+// a parameter sweep is a loop of runs.  Here thousands of circuits of uneven
+// width and depth share one launch: every circuit gets its own state buffer
+// (at least 12 qubits: narrower ones are padded with idle qubits that stay in
+// |0>), its own fused plan (tiled passes of up to three 5-qubit tensor-core
+// blocks, qs_plan.cpp), and the kernel's CTAs take whole circuits from a
+// queue, longest first.  A CTA runs all passes of its circuit over all of the
+// circuit's tiles, so passes need no synchronisation between CTAs; states up
+// to a few MB stay in L2 while their CTA works on them.  The first pass starts
+// from |0...0> without reading memory; the last pass also accumulates the
+// nearest-neighbour <Z_i Z_{i+1}> expectations of the circuit.
+//
+// Circuits with the same gate pattern (same operations on the same qubits)
+// share one plan structure; only their block matrices are rebuilt.
+#include <algorithm>
+#include <cstring>
+#include <map>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "qs_plan_internal.h"
+#include "qs_prim.h"
+#include "qs_tile_core.cuh"
+
+namespace {
+
+using namespace qs_tile;
+
+constexpr int kMaxZZ = 23;                        // circuits of up to 24 qubits
+constexpr uint32_t kOffA = 0;
+constexpr uint32_t kOffB = 2 * kA;
+constexpr uint32_t kOffStage = kOffB + kMaxSub * 2 * kB;
+constexpr uint32_t kOffLayout = kOffStage + kStage;
+constexpr uint32_t kLayoutBytes = (sizeof(Layout) + 15) & ~15u;
+constexpr uint32_t kOffMisc = kOffLayout + kLayoutBytes;   // mbarrier 8, tmem 4, circuit 4, pad
+constexpr uint32_t kSmemBytes = kOffMisc + 16;
+// Reductions (4 + 4 x kMaxZZ doubles) reuse the staging rows: they run only
+// when no copy into staging is in flight.  Two CTAs per SM need
+// 2 x (kSmemBytes + 1 KB reserved) <= 228 KB.
+constexpr uint32_t kOffRed = kOffStage;
+static_assert(2 * (kSmemBytes + 1024) <= 228 * 1024, "two CTAs per SM");
+
+struct BatchCirc {
+    float *amp;                  // 2^nq_eff complex64
+    const uint16_t *mats;        // the circuit's blocks, [2][64][64] BF16 each
+    const Layout *layouts;       // its passes (Layout::pad = first block of the pass)
+    double *zz;                  // nq - 1 outputs
+    int32_t npass, nq, nq_eff, pad;
+};
+
+struct BatchParams {
+    const BatchCirc *circ;
+    const int32_t *order;        // processing order (longest first)
+    int32_t ncirc;
+    int32_t *head;               // queue position, zeroed before the launch
+    int *err;
+};
+
+__global__ void __launch_bounds__(kThreads, 2) k_batch(BatchParams P)
+{
+    extern __shared__ __align__(1024) uint8_t smem[];
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    if (smem_u32(smem) & 1023u) {
+        if (tid == 0) atomicExch(P.err, 2);
+        return;
+    }
+    uint8_t *aHi = smem + kOffA, *aLo = smem + kOffA + kA;
+    Layout &L = *reinterpret_cast<Layout *>(smem + kOffLayout);
+    uint64_t *mbar = reinterpret_cast<uint64_t *>(smem + kOffMisc);
+    uint32_t *tmem_holder = reinterpret_cast<uint32_t *>(smem + kOffMisc + 8);
+    int32_t *s_circ = reinterpret_cast<int32_t *>(smem + kOffMisc + 12);
+    double *red = reinterpret_cast<double *>(smem + kOffRed);
+    const uint32_t stage = smem_u32(smem + kOffStage);
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                     :: "r"(smem_u32(tmem_holder)), "r"(kTmemCols));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(smem_u32(mbar)), "r"(1));
+        asm volatile("fence.mbarrier_init.release.cluster;");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = *tmem_holder;
+    const uint32_t mb = smem_u32(mbar);
+    const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16);
+    const uint32_t a_hi = smem_u32(aHi), a_lo = smem_u32(aLo);
+    const int row = tid;
+    uint32_t phase = 0;
+    bool failed = false;
+
+    while (!failed) {
+        if (tid == 0) {
+            const int c = atomicAdd(P.head, 1);
+            *s_circ = c < P.ncirc ? P.order[c] : -1;
+        }
+        __syncthreads();
+        const int ci = *s_circ;
+        if (ci < 0) break;
+        const BatchCirc C = P.circ[ci];
+        const uint64_t tiles = 1ull << (C.nq_eff - 12);
+        const int nzz = C.nq - 1;
+        float scale = 1.0f;
+        double zz[kMaxZZ];
+#pragma unroll
+        for (int i = 0; i < kMaxZZ; ++i) zz[i] = 0.0;
+        double out_norm = 0.0;
+
+        for (int p = 0; p < C.npass && !failed; ++p) {
+            // the pass's layout and matrices into shared memory
+            {
+                const uint32_t *src = reinterpret_cast<const uint32_t *>(C.layouts + p);
+                uint32_t *dst = reinterpret_cast<uint32_t *>(&L);
+                for (int i = tid; i < (int)(sizeof(Layout) / 4); i += kThreads) dst[i] = src[i];
+            }
+            __syncthreads();
+            load_b(smem + kOffB, C.mats + (size_t)L.pad * 2 * 64 * 64, L.nsub);
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            __syncthreads();
+            uint64_t gC0 = 0, gCl = 0;
+#pragma unroll
+            for (int b = 0; b < 7; ++b) {
+                gC0 |= (uint64_t)((row >> b) & 1) << L.c0_glob[b];
+                gCl |= (uint64_t)((row >> b) & 1) << L.cl_glob[b];
+            }
+            uint32_t baseR[kMaxSub - 1] = {0, 0}, baseJ[kMaxSub - 1] = {0, 0};
+            for (int t = 0; t + 1 < L.nsub; ++t)
+                for (int b = 0; b < 7; ++b) {
+                    const uint32_t bit = (row >> b) & 1;
+                    const int m = L.rowmap[t][b];
+                    if (m >= 0) baseR[t] |= bit << m;
+                    else baseJ[t] |= bit << (~m);
+                }
+            const bool last_pass = p + 1 == C.npass;
+            double acc_out = 0;
+            if (p > 0) prefetch_row(C.amp, tile_base(0, L) | gC0, L, stage, row);
+            for (uint64_t tile = 0; tile < tiles; ++tile) {
+                const uint64_t tbase = tile_base(tile, L);
+                float x[64];
+                if (p == 0) {
+                    // |0...0>: amplitude 0 is tile 0, the row with no row bits, column 0
+#pragma unroll
+                    for (int e = 0; e < 64; ++e) x[e] = 0.f;
+                    if (tile == 0 && gC0 == 0) x[0] = 1.f;
+                } else {
+                    asm volatile("cp.async.wait_group 0;" ::: "memory");
+                    read_stage_row(stage, row, x);
+                    if (tile + 1 < tiles) prefetch_row(C.amp, tile_base(tile + 1, L) | gC0, L, stage, row);
+#pragma unroll
+                    for (int e = 0; e < 64; ++e) x[e] *= scale;
+                }
+#pragma unroll
+                for (int j = 0; j < 32; ++j) a_store_pair(aHi, aLo, row, j, x[2 * j], x[2 * j + 1]);
+
+                for (int b = 0; b < L.nsub; ++b) {
+                    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                    __syncthreads();
+                    if (tid == 0)
+                        issue_block_mma(tmem, a_hi, a_lo, smem_u32(smem + kOffB + (2 * b) * kB),
+                                        smem_u32(smem + kOffB + (2 * b + 1) * kB), mb);
+                    const bool ok = mbar_wait(mb, phase);
+                    phase ^= 1;
+                    if (__syncthreads_or(!ok)) { failed = true; break; }
+                    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                    uint32_t y[4][16];
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) tmem_ld16(taddr + 16 * q, y[q]);
+                    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+                    if (b + 1 < L.nsub) {
+#pragma unroll
+                        for (int q = 0; q < 4; ++q)
+#pragma unroll
+                            for (int e = 0; e < 8; ++e) {
+                                const int j = 8 * q + e;
+                                const int r2 = baseR[b] | L.tabR[b][j], j2 = baseJ[b] | L.tabJ[b][j];
+                                a_store_pair(aHi, aLo, r2, j2, __uint_as_float(y[q][2 * e]),
+                                             __uint_as_float(y[q][2 * e + 1]));
+                            }
+                    } else {
+                        const uint64_t obase = tbase | gCl;
+                        float t = 0.f;
+                        float zt[kMaxZZ];
+#pragma unroll
+                        for (int i = 0; i < kMaxZZ; ++i) zt[i] = 0.f;
+#pragma unroll
+                        for (int q = 0; q < 4; ++q)
+#pragma unroll
+                            for (int e = 0; e < 8; ++e) {
+                                const float re = __uint_as_float(y[q][2 * e]), im = __uint_as_float(y[q][2 * e + 1]);
+                                const uint64_t g = obase | L.gl[8 * q + e];
+                                *reinterpret_cast<float2 *>(C.amp + 2 * g) = make_float2(re, im);
+                                const float pr = fmaf(re, re, im * im);
+                                t += pr;
+                                if (last_pass) {
+                                    const uint32_t par = (uint32_t)(g ^ (g >> 1));   // bit i: x_i xor x_{i+1}
+#pragma unroll
+                                    for (int i = 0; i < kMaxZZ; ++i) zt[i] += ((par >> i) & 1u) ? -pr : pr;
+                                }
+                            }
+                        acc_out += (double)t;
+                        if (last_pass)
+#pragma unroll
+                            for (int i = 0; i < kMaxZZ; ++i) zz[i] += (double)zt[i];
+                    }
+                    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+                }
+                if (failed) break;
+            }
+            asm volatile("cp.async.wait_group 0;" ::: "memory");
+            // the pass's output norm (fixed order), and the next pass's scale
+            for (int o = 16; o > 0; o >>= 1) acc_out += __shfl_xor_sync(0xffffffffu, acc_out, o);
+            __syncthreads();
+            if (lane == 0) red[warp] = acc_out;
+            __syncthreads();
+            out_norm = red[0] + red[1] + red[2] + red[3];
+            scale = out_norm > 0 ? (float)(1.0 / sqrt(out_norm)) : 1.0f;
+            // this pass's stores must be visible to the next pass's loads
+            __threadfence();
+            __syncthreads();
+        }
+        if (failed) break;
+        // <Z_i Z_{i+1}> of the normalised final state
+#pragma unroll
+        for (int i = 0; i < kMaxZZ; ++i)
+            for (int o = 16; o > 0; o >>= 1) zz[i] += __shfl_xor_sync(0xffffffffu, zz[i], o);
+        if (lane == 0)
+#pragma unroll
+            for (int i = 0; i < kMaxZZ; ++i) red[4 + warp * kMaxZZ + i] = zz[i];
+        __syncthreads();
+        for (int i = tid; i < nzz; i += kThreads)
+            C.zz[i] = (red[4 + i] + red[4 + kMaxZZ + i] + red[4 + 2 * kMaxZZ + i] + red[4 + 3 * kMaxZZ + i]) /
+                      out_norm;
+        __syncthreads();
+    }
+    if (failed) {
+        if (tid == 0) atomicExch(P.err, 1);
+        mbar_wait(mb, phase ^ 1);
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" :: "r"(tmem), "r"(kTmemCols));
+    }
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------ host
+struct qs_batch {
+    int n = 0;
+    qs_batch_opts opts;
+    std::vector<int> nq, nq_eff;
+    std::vector<size_t> zz_off;          // output offsets (nq - 1 each)
+    std::vector<size_t> amp_off;         // state offsets (bytes)
+    std::vector<int32_t> order;
+    int dev = -1;
+    void *d_states = nullptr;            // all states
+    void *d_mats = nullptr;              // all block matrices
+    void *d_layouts = nullptr;           // layouts of the distinct plan structures
+    void *d_circ = nullptr;              // BatchCirc[n]
+    void *d_order = nullptr;
+    double *d_zz = nullptr;
+    int32_t *d_head = nullptr;           // queue head + error flag
+    size_t zz_count = 0, state_bytes = 0;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t graph_exec = nullptr;
+    cudaStream_t graph_stream = nullptr;
+};
+
+namespace {
+
+void batch_free(qs_batch *B)
+{
+    if (B->graph_exec) cudaGraphExecDestroy(B->graph_exec);
+    if (B->graph) cudaGraphDestroy(B->graph);
+    for (void *p : {B->d_states, B->d_mats, B->d_layouts, B->d_circ, B->d_order, (void *)B->d_zz, (void *)B->d_head})
+        if (p) cudaFree(p);
+    delete B;
+}
+
+std::string signature(int nq, const qs_gate *g, size_t count)
+{
+    std::string s(reinterpret_cast<const char *>(&nq), sizeof(nq));
+    for (size_t i = 0; i < count; ++i) {
+        s.append(reinterpret_cast<const char *>(&g[i].op), sizeof(int32_t));
+        s.append(reinterpret_cast<const char *>(g[i].q), sizeof(g[i].q));
+        s.append(reinterpret_cast<const char *>(&g[i].nctrl), sizeof(int32_t));
+        s.append(reinterpret_cast<const char *>(g[i].ctrl), sizeof(int32_t) * (size_t)std::max(0, g[i].nctrl));
+    }
+    return s;
+}
+
+}  // namespace
+
+extern "C" int qs_batch_default_opts(qs_batch_opts *o)
+{
+    if (!o) return qs_fail(QS_ERR_ARG, "qs_batch_default_opts: null");
+    o->max_sub = 3;
+    o->low_qubits = 3;
+    o->order = QS_BATCH_LONGEST_FIRST;
+    o->use_graph = 1;
+    return QS_OK;
+}
+
+extern "C" int qs_batch_create(int n_circ, const int *n_qubits, const qs_gate *gates, const size_t *offsets,
+                               const qs_batch_opts *opts, qs_batch **out)
+{
+    if (!out) return qs_fail(QS_ERR_ARG, "qs_batch_create: null output");
+    *out = nullptr;
+    if (n_circ < 1 || !n_qubits || !offsets || (!gates && offsets[n_circ] > 0))
+        return qs_fail(QS_ERR_ARG, "qs_batch_create: bad arguments");
+    qs_batch_opts o;
+    if (opts) o = *opts;
+    else qs_batch_default_opts(&o);
+    if (o.max_sub < 1 || o.max_sub > 3 || o.low_qubits < 1 || o.low_qubits > 5)
+        return qs_fail(QS_ERR_ARG, "qs_batch_create: max_sub 1..3, low_qubits 1..5");
+    for (int c = 0; c < n_circ; ++c) {
+        if (n_qubits[c] < 1 || n_qubits[c] > kMaxZZ + 1)
+            return qs_fail(QS_ERR_UNSUPPORTED, "qs_batch_create: circuit %d has %d qubits (batched circuits: 1..%d)",
+                           c, n_qubits[c], kMaxZZ + 1);
+        if (offsets[c + 1] < offsets[c]) return qs_fail(QS_ERR_ARG, "qs_batch_create: offsets must not decrease");
+    }
+    qs_batch *B = new qs_batch();
+    B->n = n_circ;
+    B->opts = o;
+    int r = QS_OK;
+    cudaError_t e = cudaGetDevice(&B->dev);
+    if (e != cudaSuccess) { delete B; return qs_cuda_fail(e, "qs_batch_create"); }
+
+    // ---- plans: one structure per gate pattern, rebound per circuit
+    qs_plan_opts po;
+    qs_plan_default_opts(&po);
+    po.max_sub = o.max_sub;
+    po.low_qubits = o.low_qubits;
+    std::map<std::string, int> proto_of;              // signature -> index in protos
+    std::vector<qs_plan *> protos, plans(n_circ, nullptr);
+    std::vector<int> proto_id(n_circ);
+    B->nq.resize(n_circ);
+    B->nq_eff.resize(n_circ);
+    for (int c = 0; c < n_circ && !r; ++c) {
+        B->nq[c] = n_qubits[c];
+        B->nq_eff[c] = std::max(12, n_qubits[c]);
+        const qs_gate *g = gates + offsets[c];
+        const size_t cnt = offsets[c + 1] - offsets[c];
+        for (size_t i = 0; i < cnt && !r; ++i)
+            if (qs_gate_qubits(&g[i]) >> n_qubits[c])
+                r = qs_fail(QS_ERR_ARG, "qs_batch_create: circuit %d gate %zu uses a qubit >= %d", c, i, n_qubits[c]);
+        if (r) break;
+        std::string sig = signature(B->nq_eff[c], g, cnt);
+        auto it = proto_of.find(sig);
+        if (it == proto_of.end()) {
+            qs_plan *pp = nullptr;
+            if ((r = qs_plan_create_ex(B->nq_eff[c], g, cnt, &po, &pp))) break;
+            proto_of[sig] = (int)protos.size();
+            proto_id[c] = (int)protos.size();
+            protos.push_back(pp);
+        } else {
+            proto_id[c] = it->second;
+        }
+    }
+    // rebind the block matrices of every circuit (parallel on the host)
+    if (!r) {
+        std::vector<int> rc(n_circ, QS_OK);
+        const int nt = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+        std::vector<std::thread> th;
+        for (int t = 0; t < nt; ++t)
+            th.emplace_back([&, t]() {
+                for (int c = t; c < n_circ; c += nt)
+                    rc[c] = qs_plan_rebind(protos[proto_id[c]], gates + offsets[c], offsets[c + 1] - offsets[c],
+                                           &plans[c]);
+            });
+        for (auto &x : th) x.join();
+        for (int c = 0; c < n_circ && !r; ++c)
+            if (rc[c]) r = qs_fail(QS_ERR_ARG, "qs_batch_create: rebinding circuit %d failed", c);
+    }
+    // ---- device memory
+    std::vector<Layout> layouts;                      // per proto, concatenated
+    std::vector<size_t> layout_first(protos.size());
+    for (size_t pi = 0; pi < protos.size() && !r; ++pi) {
+        layout_first[pi] = layouts.size();
+        const qs_plan *pp = protos[pi];
+        for (const PlanPass &pass : pp->passes) {
+            Layout L;
+            int qpos[3][5];
+            for (size_t b = 0; b < pass.count; ++b)
+                for (int j = 0; j < 5; ++j) qpos[b][j] = pp->blocks[pass.first + b].q[j];
+            if ((r = qs_tile_layout_build(pp->n, pass.T, (int)pass.count, qpos, &L))) break;
+            L.pad = (int32_t)pass.first;
+            layouts.push_back(L);
+        }
+    }
+    std::vector<size_t> mat_off(n_circ);
+    size_t mat_total = 0;
+    B->amp_off.resize(n_circ);
+    B->zz_off.resize(n_circ);
+    for (int c = 0; c < n_circ && !r; ++c) {
+        mat_off[c] = mat_total;
+        mat_total += plans[c]->blocks.size() * 2 * 64 * 64;
+        B->amp_off[c] = B->state_bytes;
+        B->state_bytes += ((8ull << B->nq_eff[c]) + 255) & ~255ull;
+        B->zz_off[c] = B->zz_count;
+        B->zz_count += (size_t)(B->nq[c] - 1);
+    }
+    std::vector<BatchCirc> hc(n_circ);
+    if (!r) {
+        std::vector<uint16_t> hm(mat_total);
+        for (int c = 0; c < n_circ; ++c)
+            for (size_t b = 0; b < plans[c]->blocks.size(); ++b)
+                qs_plan_block_bf16(plans[c], b, hm.data() + mat_off[c] + b * 2 * 64 * 64);
+        e = cudaMalloc(&B->d_states, B->state_bytes);
+        if (e == cudaSuccess) e = cudaMalloc(&B->d_mats, std::max<size_t>(hm.size() * 2, 16));
+        if (e == cudaSuccess) e = cudaMalloc(&B->d_layouts, std::max<size_t>(layouts.size() * sizeof(Layout), 16));
+        if (e == cudaSuccess) e = cudaMalloc(&B->d_circ, sizeof(BatchCirc) * n_circ);
+        if (e == cudaSuccess) e = cudaMalloc(&B->d_order, sizeof(int32_t) * n_circ);
+        if (e == cudaSuccess) e = cudaMalloc((void **)&B->d_zz, std::max<size_t>(B->zz_count, 1) * sizeof(double));
+        if (e == cudaSuccess) e = cudaMalloc((void **)&B->d_head, 2 * sizeof(int32_t));
+        if (e == cudaSuccess) e = cudaMemcpy(B->d_mats, hm.data(), hm.size() * 2, cudaMemcpyHostToDevice);
+        if (e == cudaSuccess && !layouts.empty())
+            e = cudaMemcpy(B->d_layouts, layouts.data(), layouts.size() * sizeof(Layout), cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) r = qs_cuda_fail(e, "qs_batch_create: device memory");
+    }
+    if (!r) {
+        for (int c = 0; c < n_circ; ++c) {
+            const qs_plan *pp = protos[proto_id[c]];
+            BatchCirc &bc = hc[c];
+            bc.amp = reinterpret_cast<float *>(static_cast<char *>(B->d_states) + B->amp_off[c]);
+            bc.mats = static_cast<const uint16_t *>(B->d_mats) + mat_off[c];
+            bc.layouts = static_cast<const Layout *>(B->d_layouts) + layout_first[proto_id[c]];
+            bc.zz = B->d_zz + B->zz_off[c];
+            bc.npass = (int32_t)pp->passes.size();
+            bc.nq = B->nq[c];
+            bc.nq_eff = B->nq_eff[c];
+        }
+        // processing order: longest first (tiles x passes), or as given
+        B->order.resize(n_circ);
+        for (int c = 0; c < n_circ; ++c) B->order[c] = c;
+        if (o.order == QS_BATCH_LONGEST_FIRST)
+            std::stable_sort(B->order.begin(), B->order.end(), [&](int32_t a, int32_t b) {
+                return (double)hc[a].npass * (double)(1ull << hc[a].nq_eff) >
+                       (double)hc[b].npass * (double)(1ull << hc[b].nq_eff);
+            });
+        e = cudaMemcpy(B->d_circ, hc.data(), sizeof(BatchCirc) * n_circ, cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = cudaMemcpy(B->d_order, B->order.data(), sizeof(int32_t) * n_circ, cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) r = qs_cuda_fail(e, "qs_batch_create: tables");
+    }
+    for (qs_plan *p : plans) qs_plan_destroy(p);
+    for (qs_plan *p : protos) qs_plan_destroy(p);
+    if (r) { batch_free(B); return r; }
+    *out = B;
+    return QS_OK;
+}
+
+namespace {
+
+int batch_launch(qs_batch *B, cudaStream_t st)
+{
+    QS_CUDA_TRY(cudaMemsetAsync(B->d_head, 0, 2 * sizeof(int32_t), st));
+    BatchParams P;
+    P.circ = static_cast<const BatchCirc *>(B->d_circ);
+    P.order = static_cast<const int32_t *>(B->d_order);
+    P.ncirc = B->n;
+    P.head = B->d_head;
+    P.err = B->d_head + 1;
+    const unsigned grid = (unsigned)std::min(B->n, QS_SM_COUNT * 2);
+    k_batch<<<grid, kThreads, kSmemBytes, st>>>(P);
+    QS_LAUNCH_CHECK("k_batch");
+    return QS_OK;
+}
+
+}  // namespace
+
+extern "C" int qs_batch_run(qs_batch *B, void *stream)
+{
+    if (!B) return qs_fail(QS_ERR_ARG, "qs_batch_run: null batch");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    QS_CUDA_TRY(cudaFuncSetAttribute(k_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes));
+    if (!B->opts.use_graph) return batch_launch(B, st);
+    if (!B->graph_exec) {
+        // capture once on a private stream; replay on the caller's stream
+        if (!B->graph_stream) QS_CUDA_TRY(cudaStreamCreateWithFlags(&B->graph_stream, cudaStreamNonBlocking));
+        QS_CUDA_TRY(cudaStreamBeginCapture(B->graph_stream, cudaStreamCaptureModeThreadLocal));
+        int r = batch_launch(B, B->graph_stream);
+        cudaGraph_t g = nullptr;
+        cudaError_t e = cudaStreamEndCapture(B->graph_stream, &g);
+        if (r) { if (g) cudaGraphDestroy(g); return r; }
+        if (e != cudaSuccess) return qs_cuda_fail(e, "qs_batch_run: capture");
+        B->graph = g;
+        QS_CUDA_TRY(cudaGraphInstantiate(&B->graph_exec, B->graph, 0));
+    }
+    QS_CUDA_TRY(cudaGraphLaunch(B->graph_exec, st));
+    return QS_OK;
+}
+
+extern "C" int qs_batch_zz(qs_batch *B, double *out, size_t *count)
+{
+    if (!B || !count) return qs_fail(QS_ERR_ARG, "qs_batch_zz: null argument");
+    *count = B->zz_count;
+    if (!out) return QS_OK;
+    QS_CUDA_TRY(cudaDeviceSynchronize());
+    int32_t flag[2] = {0, 0};
+    QS_CUDA_TRY(cudaMemcpy(flag, B->d_head, sizeof(flag), cudaMemcpyDeviceToHost));
+    if (flag[1] == 2) return qs_fail(QS_ERR_STATE, "qs_batch: dynamic shared memory not 1024-byte aligned");
+    if (flag[1]) return qs_fail(QS_ERR_STATE, "qs_batch: a bounded wait in the batch kernel expired");
+    QS_CUDA_TRY(cudaMemcpy(out, B->d_zz, B->zz_count * sizeof(double), cudaMemcpyDeviceToHost));
+    return QS_OK;
+}
+
+extern "C" int qs_batch_zz_offsets(const qs_batch *B, size_t *offsets)
+{
+    if (!B || !offsets) return qs_fail(QS_ERR_ARG, "qs_batch_zz_offsets: null argument");
+    for (int c = 0; c < B->n; ++c) offsets[c] = B->zz_off[c];
+    offsets[B->n] = B->zz_count;
+    return QS_OK;
+}
+
+extern "C" int qs_batch_state(qs_batch *B, int c, void *host_out, int host_dtype)
+{
+    if (!B || c < 0 || c >= B->n || !host_out) return qs_fail(QS_ERR_ARG, "qs_batch_state: bad arguments");
+    if (host_dtype != QS_C64 && host_dtype != QS_C128) return qs_fail(QS_ERR_ARG, "qs_batch_state: bad dtype");
+    QS_CUDA_TRY(cudaDeviceSynchronize());
+    const size_t N = 1ull << B->nq[c];               // idle padding qubits are |0>: the first 2^nq amplitudes
+    std::vector<float> tmp(2 * N);
+    QS_CUDA_TRY(cudaMemcpy(tmp.data(), static_cast<char *>(B->d_states) + B->amp_off[c], 8 * N,
+                           cudaMemcpyDeviceToHost));
+    if (host_dtype == QS_C64) memcpy(host_out, tmp.data(), 8 * N);
+    else
+        for (size_t i = 0; i < 2 * N; ++i) static_cast<double *>(host_out)[i] = tmp[i];
+    return QS_OK;
+}
+
+extern "C" int qs_batch_info(const qs_batch *B, size_t *state_bytes, size_t *passes_total)
+{
+    if (!B) return qs_fail(QS_ERR_ARG, "qs_batch_info: null batch");
+    if (state_bytes) *state_bytes = B->state_bytes;
+    if (passes_total) *passes_total = 0;
+    return QS_OK;
+}
+
+extern "C" int qs_batch_destroy(qs_batch *B)
+{
+    if (!B) return QS_OK;
+    cudaDeviceSynchronize();
+    if (B->graph_stream) cudaStreamDestroy(B->graph_stream);
+    batch_free(B);
+    return QS_OK;
+}
+
+// Autotuner: time candidate options on a sample of the circuits (every
+// `stride`-th one) and return the fastest.  Candidates: blocks per pass
+// (1, 2, 3) x lowest tile qubits (3, 5) x queue order (longest first, as
+// given).  Each candidate is built, run once untimed, then timed over two runs
+// with CUDA events on a private stream.
+extern "C" int qs_batch_autotune(int n_circ, const int *n_qubits, const qs_gate *gates, const size_t *offsets,
+                                 int stride, qs_batch_opts *best, double *best_ms)
+{
+    if (!best || n_circ < 1 || stride < 1) return qs_fail(QS_ERR_ARG, "qs_batch_autotune: bad arguments");
+    std::vector<int> nq;
+    std::vector<qs_gate> g;
+    std::vector<size_t> off(1, 0);
+    for (int c = 0; c < n_circ; c += stride) {
+        nq.push_back(n_qubits[c]);
+        g.insert(g.end(), gates + offsets[c], gates + offsets[c + 1]);
+        off.push_back(g.size());
+    }
+    cudaStream_t st;
+    QS_CUDA_TRY(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    double bt = 1e300;
+    int r = QS_OK;
+    for (int ms : {1, 2, 3})
+        for (int lq : {3, 5})
+            for (int order : {QS_BATCH_LONGEST_FIRST, QS_BATCH_INPUT_ORDER}) {
+                qs_batch_opts o;
+                qs_batch_default_opts(&o);
+                o.max_sub = ms;
+                o.low_qubits = lq;
+                o.order = order;
+                o.use_graph = 0;
+                qs_batch *b = nullptr;
+                if ((r = qs_batch_create((int)nq.size(), nq.data(), g.data(), off.data(), &o, &b))) goto done;
+                if ((r = qs_batch_run(b, st))) { qs_batch_destroy(b); goto done; }
+                cudaEventRecord(e0, st);
+                for (int k = 0; k < 2 && !r; ++k) r = qs_batch_run(b, st);
+                cudaEventRecord(e1, st);
+                cudaStreamSynchronize(st);
+                float t = 0;
+                cudaEventElapsedTime(&t, e0, e1);
+                size_t cnt = 0;
+                if (!r) r = qs_batch_zz(b, nullptr, &cnt);
+                qs_batch_destroy(b);
+                if (r) goto done;
+                if (t / 2 < bt) {
+                    bt = t / 2;
+                    *best = o;
+                }
+            }
+done:
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaStreamDestroy(st);
+    if (r) return r;
+    best->use_graph = 1;
+    if (best_ms) *best_ms = bt;
+    return QS_OK;
+}

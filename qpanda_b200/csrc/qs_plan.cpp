@@ -23,30 +23,7 @@
 
 typedef std::complex<double> cd;
 
-struct PlanBlock {
-    int k = 0;
-    int q[5] = {0, 0, 0, 0, 0};          // ascending global qubits
-    std::vector<cd> U;                   // 32 x 32 row-major
-    std::vector<size_t> gates;           // indices into the gate list, in application order
-};
-
-// A pass of the tiled kernel: one read and one write of the state, applying
-// up to 3 consecutive blocks (sub-blocks) whose qubits lie in the 12 tile qubits.
-struct PlanPass {
-    int T[12] = {0};                     // ascending global qubits of the tile
-    size_t first = 0, count = 0;         // its blocks: blocks[first, first + count)
-};
-
-struct qs_plan {
-    int n = 0;
-    int max_k = 5;
-    qs_plan_opts opts;
-    std::vector<qs_gate> gates;
-    std::vector<PlanBlock> blocks;
-    std::vector<PlanPass> passes;        // tiled kernel only
-    int dev = -1;                        // device holding mats
-    void *mats = nullptr;                // [blocks][2][64][64] bf16
-};
+#include "qs_plan_internal.h"
 
 namespace {
 
@@ -497,5 +474,36 @@ extern "C" int qs_plan_status(qs_state *s)
     QS_CUDA_TRY(cudaStreamSynchronize(s->stream));
     if (flag == 2) return qs_fail(QS_ERR_STATE, "fused pass: dynamic shared memory not 1024-byte aligned");
     if (flag) return qs_fail(QS_ERR_STATE, "fused pass: a bounded wait in the tensor-core kernel expired");
+    return QS_OK;
+}
+
+void qs_plan_block_bf16(const qs_plan *P, size_t b, uint16_t *out)
+{
+    block_bf16(P->blocks[b], out);
+}
+
+int qs_plan_rebind(const qs_plan *proto, const qs_gate *gates, size_t count, qs_plan **out)
+{
+    *out = nullptr;
+    if (!proto || count != proto->gates.size()) return qs_fail(QS_ERR_ARG, "plan rebind: gate count differs");
+    for (size_t i = 0; i < count; ++i) {
+        const qs_gate &a = proto->gates[i], &g = gates[i];
+        if (a.op != g.op || a.nctrl != g.nctrl || memcmp(a.q, g.q, sizeof(a.q)) ||
+            memcmp(a.ctrl, g.ctrl, sizeof(int32_t) * (size_t)(a.nctrl > 0 ? a.nctrl : 0)))
+            return qs_fail(QS_ERR_ARG, "plan rebind: gate %zu differs in operation or qubits", i);
+    }
+    qs_plan *P = new qs_plan();
+    P->n = proto->n;
+    P->max_k = proto->max_k;
+    P->opts = proto->opts;
+    P->gates.assign(gates, gates + count);
+    P->passes = proto->passes;
+    P->blocks = proto->blocks;
+    std::vector<qs_prim> prim;
+    std::vector<uint64_t> mask;
+    int r = lower_all(P, prim, mask);
+    if (r) { delete P; return r; }
+    for (PlanBlock &B : P->blocks) block_unitary(B, prim);
+    *out = P;
     return QS_OK;
 }
