@@ -93,6 +93,10 @@ const char *qs_version(void);
  * Replaces QuantumGates::initState (QuantumGates.h:376;
  * CPUQuantumGates.cpp:1136-1157; GPU: GPUEmulator/GPUGates.cu:1208-1299). */
 int qs_create(int n_qubits, int dtype, void *stream, qs_state **out);
+/* As qs_create, with stream-ordered memory: the state's buffers come from
+ * cudaMallocAsync on `stream` and go back with cudaFreeAsync in qs_destroy, so
+ * creating and destroying states never synchronizes the device (serving). */
+int qs_create_async(int n_qubits, int dtype, void *stream, qs_state **out);
 /* Free the state.  Replaces QuantumGates::destroyState (QuantumGates.h:438). */
 int qs_destroy(qs_state *s);
 int qs_num_qubits(const qs_state *s, int *n_qubits);
@@ -152,6 +156,8 @@ int qs_measure(qs_state *s, int q, double u, int *outcome);
  * idx bit j = qubit qubits[j].  This is the un-truncated vector that
  * pMeasure builds (QuantumGates.h:75; CPUQuantumGates.cpp:159-190). */
 int qs_probs(qs_state *s, const int *qubits, int m, double *out);
+/* qs_probs into a device buffer of 2^m doubles, asynchronous on the state's stream. */
+int qs_probs_device(qs_state *s, const int *qubits, int m, double *dev_out);
 /* pMeasure as the reference returns it: the marginal sorted by descending
  * probability and cut to the first 10 entries (CPUQuantumGates.cpp:178-189).
  * idx_out/p_out hold up to 10 entries; *count receives how many. */
@@ -273,6 +279,45 @@ int qs_batch_destroy(qs_batch *b);
  * fastest to *best (with use_graph set) and its time per run to *best_ms. */
 int qs_batch_autotune(int n_circuits, const int *n_qubits, const qs_gate *gates, const size_t *offsets,
                       int stride, qs_batch_opts *best, double *best_ms);
+
+/* ---- request loop: continuous batching on one GPU ----------------------- */
+/* Requests (a circuit, plus 1024-style shots or the full probability vector)
+ * are submitted at any time; `slots` worker threads with their own streams
+ * take them in arrival order (or up to `bypass` places past a head that does
+ * not fit yet) when their HBM footprint - state, scratch and, for
+ * probabilities, the output vector - fits `hbm_budget_bytes` beside the
+ * requests already on the device.  Requests overlap on the GPU; states use
+ * stream-ordered memory.  A request's result does not depend on what else
+ * runs.  The reference's counterpart is one QPandaSDK::run per program
+ * (QPandaAPI.cpp:131-211) and its remote cloud mode
+ * (QuantumCloudHTTP.cpp:117-191). */
+typedef struct qs_server qs_server;
+#define QS_REQ_SHOTS 1     /* sample shots of all qubits (qs_sample semantics) into out_host */
+#define QS_REQ_PROBS 2     /* full 2^n probability vector, held on the device */
+#define QS_MAX_QUBITS_SERVED 32
+typedef struct qs_server_opts {
+    size_t hbm_budget_bytes;
+    int slots;             /* concurrent requests (worker threads / streams), 1..64 */
+    int bypass;            /* admission may skip this many non-fitting requests */
+} qs_server_opts;
+int qs_server_default_opts(qs_server_opts *opts);
+int qs_server_create(const qs_server_opts *opts, qs_server **out);
+/* Queue a request; returns at once with its id.  For QS_REQ_SHOTS, uniforms
+ * holds shots x n_qubits values (u[s*n + k] for qubit k of shot s) and
+ * out_host receives the shots; out_host must stay valid until the request is
+ * done.  QS_ERR_OOM if the request alone exceeds the budget. */
+int qs_server_submit(qs_server *srv, int n_qubits, const qs_gate *gates, size_t count, int kind,
+                     const double *uniforms, size_t shots, uint64_t *out_host, uint64_t *id);
+/* Block until the request is done; latency = submit -> result ready, service =
+ * admitted -> result ready.  Returns the request's status. */
+int qs_server_wait(qs_server *srv, uint64_t id, double *latency_s, double *service_s);
+/* Copy a QS_REQ_PROBS result (2^n doubles) to the host. */
+int qs_server_fetch_probs(qs_server *srv, uint64_t id, double *host_out);
+/* Forget a finished request and free its held result. */
+int qs_server_release(qs_server *srv, uint64_t id);
+int qs_server_stats(qs_server *srv, size_t *served, size_t *max_concurrent, size_t *hbm_in_use);
+/* Stop: queued requests end with QS_ERR_STATE, running ones finish. */
+int qs_server_destroy(qs_server *srv);
 
 #ifdef __cplusplus
 }

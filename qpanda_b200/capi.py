@@ -75,6 +75,16 @@ def lib():
         "qs_norm2": (i, [vp, dp]),
         "qs_inner": (i, [vp, vp, dp, dp]),
         "qs_plan_create": (i, [i, vp, sz, i, C.POINTER(vp)]),
+        "qs_create_async": (i, [i, i, vp, C.POINTER(vp)]),
+        "qs_probs_device": (i, [vp, ip, i, vp]),
+        "qs_server_default_opts": (i, [vp]),
+        "qs_server_create": (i, [vp, C.POINTER(vp)]),
+        "qs_server_submit": (i, [vp, i, vp, sz, i, dp, sz, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
+        "qs_server_wait": (i, [vp, C.c_uint64, dp, dp]),
+        "qs_server_fetch_probs": (i, [vp, C.c_uint64, dp]),
+        "qs_server_release": (i, [vp, C.c_uint64]),
+        "qs_server_stats": (i, [vp, C.POINTER(sz), C.POINTER(sz), C.POINTER(sz)]),
+        "qs_server_destroy": (i, [vp]),
         "qs_batch_default_opts": (i, [vp]),
         "qs_batch_create": (i, [i, ip, vp, C.POINTER(sz), vp, C.POINTER(vp)]),
         "qs_batch_run": (i, [vp, vp]),
@@ -386,3 +396,77 @@ class Batch:
         out = np.empty(1 << int(self.nq[c]), dtype=dtype)
         check(lib().qs_batch_state(self._h, int(c), out.ctypes.data, QS_C64 if dtype == np.complex64 else QS_C128))
         return out
+
+
+class ServerOpts(C.Structure):
+    _fields_ = [("hbm_budget_bytes", C.c_size_t), ("slots", C.c_int), ("bypass", C.c_int)]
+
+
+REQ_SHOTS, REQ_PROBS = 1, 2
+
+
+class Server:
+    """Request loop with continuous batching (qs_server_*)."""
+
+    def __init__(self, budget_bytes=None, slots=None, bypass=None):
+        o = ServerOpts()
+        check(lib().qs_server_default_opts(C.byref(o)))
+        if budget_bytes is not None:
+            o.hbm_budget_bytes = int(budget_bytes)
+        if slots is not None:
+            o.slots = int(slots)
+        if bypass is not None:
+            o.bypass = int(bypass)
+        h = C.c_void_p()
+        check(lib().qs_server_create(C.byref(o), C.byref(h)))
+        self._h = h
+        self._keep = {}
+
+    def submit(self, n, gates, kind="shots", uniforms=None):
+        g = np.ascontiguousarray(gates, dtype=GATE_DTYPE)
+        rid = C.c_uint64()
+        if kind == "shots":
+            u = np.ascontiguousarray(uniforms, dtype=np.float64)
+            shots = u.size // n
+            out = np.zeros(shots, dtype=np.uint64)
+            check(lib().qs_server_submit(self._h, int(n), g.ctypes.data, g.size, REQ_SHOTS, _dptr(u), shots,
+                                         out.ctypes.data_as(C.POINTER(C.c_uint64)), C.byref(rid)))
+            self._keep[rid.value] = (u, out, n)
+        else:
+            check(lib().qs_server_submit(self._h, int(n), g.ctypes.data, g.size, REQ_PROBS, None, 0, None,
+                                         C.byref(rid)))
+            self._keep[rid.value] = (None, None, n)
+        return rid.value
+
+    def wait(self, rid):
+        lat, svc = C.c_double(), C.c_double()
+        check(lib().qs_server_wait(self._h, C.c_uint64(rid), C.byref(lat), C.byref(svc)))
+        return lat.value, svc.value
+
+    def shots(self, rid):
+        return self._keep[rid][1]
+
+    def fetch_probs(self, rid):
+        out = np.empty(1 << self._keep[rid][2])
+        check(lib().qs_server_fetch_probs(self._h, C.c_uint64(rid), _dptr(out)))
+        return out
+
+    def release(self, rid):
+        check(lib().qs_server_release(self._h, C.c_uint64(rid)))
+        self._keep.pop(rid, None)
+
+    def stats(self):
+        a, b, c = C.c_size_t(), C.c_size_t(), C.c_size_t()
+        check(lib().qs_server_stats(self._h, C.byref(a), C.byref(b), C.byref(c)))
+        return {"served": a.value, "max_concurrent": b.value, "hbm_in_use": c.value}
+
+    def close(self):
+        if self._h:
+            lib().qs_server_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -115,3 +115,18 @@ def vqe_sweep(n_circuits, seed, qmin=10, qmax=22, lmin=4, lmax=12):
         L = int(rng.integers(lmin, lmax + 1))
         out.append((q, vqe_ansatz(q, L, angles=rng.uniform(0.0, 2 * math.pi, size=(L, 2, q)))))
     return out
+
+
+def request_trace(n_requests, seed, rate=2000.0, qmin=8, qmax=30, dmin=4, dmax=32):
+    """Request-loop workload: arrivals of a Poisson process with `rate` per
+    second; each request has q ~ U{qmin..qmax} qubits, a random_layers circuit
+    of depth ~ U{dmin..dmax} (its own seed) and asks for shots or the full
+    probability vector with equal odds.  Returns a list of dicts."""
+    rng = np.random.default_rng(seed)
+    t = np.cumsum(rng.exponential(1.0 / rate, size=n_requests))
+    out = []
+    for k in range(n_requests):
+        out.append({"arrival": float(t[k]), "qubits": int(rng.integers(qmin, qmax + 1)),
+                    "depth": int(rng.integers(dmin, dmax + 1)), "kind": "shots" if rng.uniform() < 0.5 else "probs",
+                    "seed": int(rng.integers(1 << 31))})
+    return out

@@ -50,22 +50,51 @@ int qs_check_state(const qs_state *s)
     return QS_OK;
 }
 
+int qs_dev_alloc(qs_state *s, size_t bytes, void **p)
+{
+    *p = nullptr;
+    if (s->stream_alloc) QS_CUDA_TRY(cudaMallocAsync(p, bytes, s->stream));
+    else QS_CUDA_TRY(cudaMalloc(p, bytes));
+    return QS_OK;
+}
+
+void qs_dev_free(qs_state *s, void *p)
+{
+    if (!p) return;
+    if (s->stream_alloc) cudaFreeAsync(p, s->stream);
+    else cudaFree(p);
+}
+
 int qs_ensure_scratch(qs_state *s, size_t bytes)
 {
     if (bytes <= s->scratch_bytes) return QS_OK;
     size_t nb = 1 << 20;
     while (nb < bytes) nb <<= 1;
     void *p = nullptr;
-    // The stream may still be using the old buffer.
-    QS_CUDA_TRY(cudaStreamSynchronize(s->stream));
-    QS_CUDA_TRY(cudaMalloc(&p, nb));
-    if (s->scratch) cudaFree(s->scratch);
+    // The stream may still be using the old buffer (stream-ordered frees wait
+    // for it by construction).
+    if (!s->stream_alloc) QS_CUDA_TRY(cudaStreamSynchronize(s->stream));
+    int r = qs_dev_alloc(s, nb, &p);
+    if (r) return r;
+    qs_dev_free(s, s->scratch);
     s->scratch = p;
     s->scratch_bytes = nb;
     return QS_OK;
 }
 
+static int create_impl(int n_qubits, int dtype, void *stream, bool stream_alloc, qs_state **out);
+
 extern "C" int qs_create(int n_qubits, int dtype, void *stream, qs_state **out)
+{
+    return create_impl(n_qubits, dtype, stream, false, out);
+}
+
+extern "C" int qs_create_async(int n_qubits, int dtype, void *stream, qs_state **out)
+{
+    return create_impl(n_qubits, dtype, stream, true, out);
+}
+
+static int create_impl(int n_qubits, int dtype, void *stream, bool stream_alloc, qs_state **out)
 {
     if (!out) return qs_fail(QS_ERR_ARG, "qs_create: null output");
     *out = nullptr;
@@ -77,12 +106,18 @@ extern "C" int qs_create(int n_qubits, int dtype, void *stream, qs_state **out)
     s->dtype = dtype;
     s->N = 1ull << n_qubits;
     s->stream = static_cast<cudaStream_t>(stream);
+    s->stream_alloc = stream_alloc;
+    const size_t ab = s->amp_bytes() < 16 ? 16 : s->amp_bytes();
     cudaError_t e = cudaGetDevice(&s->device);
-    if (e == cudaSuccess) e = cudaMalloc(&s->amp, s->amp_bytes() < 16 ? 16 : s->amp_bytes());
-    if (e == cudaSuccess) e = cudaMallocHost(&s->pinned, 4096);
+    if (e == cudaSuccess) e = stream_alloc ? cudaMallocAsync(&s->amp, ab, s->stream) : cudaMalloc(&s->amp, ab);
+    if (e == cudaSuccess) {
+        if (stream_alloc) s->pinned = malloc(4096);
+        else e = cudaMallocHost(&s->pinned, 4096);
+    }
     if (e != cudaSuccess) {
         int r = qs_cuda_fail(e, "qs_create");
-        if (s->amp) cudaFree(s->amp);
+        if (s->amp) qs_dev_free(s, s->amp);
+        if (stream_alloc) free(s->pinned);
         delete s;
         cudaGetLastError();
         return r;
@@ -97,11 +132,19 @@ extern "C" int qs_create(int n_qubits, int dtype, void *stream, qs_state **out)
 extern "C" int qs_destroy(qs_state *s)
 {
     if (!s) return QS_OK;
-    if (s->stream || s->amp) cudaStreamSynchronize(s->stream);
-    if (s->amp) cudaFree(s->amp);
-    if (s->scratch) cudaFree(s->scratch);
-    if (s->pinned) cudaFreeHost(s->pinned);
-    if (s->fused_norm) cudaFree(s->fused_norm);
+    if (s->stream_alloc) {
+        // stream-ordered: the frees run after the work queued on the stream
+        qs_dev_free(s, s->amp);
+        qs_dev_free(s, s->scratch);
+        qs_dev_free(s, s->fused_norm);
+        free(s->pinned);
+    } else {
+        cudaStreamSynchronize(s->stream);
+        if (s->amp) cudaFree(s->amp);
+        if (s->scratch) cudaFree(s->scratch);
+        if (s->pinned) cudaFreeHost(s->pinned);
+        if (s->fused_norm) cudaFree(s->fused_norm);
+    }
     s->amp = nullptr;
     delete s;
     return QS_OK;

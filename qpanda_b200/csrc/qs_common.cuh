@@ -52,10 +52,15 @@ struct qs_state {
     void *pinned = nullptr;
     // Norm partials of fused passes (3 x fused grid doubles), on first use.
     double *fused_norm = nullptr;
+    // Stream-ordered memory (qs_create_async): cudaMallocAsync / cudaFreeAsync
+    // on `stream`, and an ordinary host buffer instead of pinned memory.
+    bool stream_alloc = false;
     size_t amp_bytes() const { return N * (dtype == QS_C64 ? 8ull : 16ull); }
 };
 
 int qs_ensure_scratch(qs_state *s, size_t bytes);
+int qs_dev_alloc(qs_state *s, size_t bytes, void **p);
+void qs_dev_free(qs_state *s, void *p);
 int qs_check_state(const qs_state *s);
 
 // ------------------------------------------------------------------ index math

@@ -612,6 +612,21 @@ extern "C" int qs_probs(qs_state *s, const int *qubits, int m, double *out)
     return s->dtype == QS_C64 ? probs_t<float>(s, qubits, m, out) : probs_t<double>(s, qubits, m, out);
 }
 
+// Marginal into a caller-provided device buffer (2^m doubles); asynchronous.
+extern "C" int qs_probs_device(qs_state *s, const int *qubits, int m, double *dev_out)
+{
+    int r = qs_check_state(s);
+    if (r) return r;
+    if ((r = check_qubit_list(s, qubits, m, "qs_probs_device"))) return r;
+    if (!dev_out) return qs_fail(QS_ERR_ARG, "qs_probs_device: null output");
+    size_t part_b = 0;
+    MargParams P = marginal_plan(s, qubits, m, &part_b);
+    if ((r = qs_ensure_scratch(s, kBufOff + part_b))) return r;
+    double *part = reinterpret_cast<double *>(static_cast<char *>(s->scratch) + kBufOff);
+    return s->dtype == QS_C64 ? marginal_launch<float>(s, P, dev_out, part)
+                              : marginal_launch<double>(s, P, dev_out, part);
+}
+
 extern "C" int qs_sample(qs_state *s, const int *qubits, int m, const double *u, size_t shots,
                          uint64_t *out)
 {

@@ -325,7 +325,8 @@ extern "C" int qs_plan_destroy(qs_plan *P)
         int cur = 0;
         cudaGetDevice(&cur);
         cudaSetDevice(P->dev);
-        cudaFree(P->mats);
+        if (P->mats_async) cudaFreeAsync(P->mats, P->mats_stream);
+        else cudaFree(P->mats);
         cudaSetDevice(cur);
     }
     delete P;
@@ -352,19 +353,33 @@ extern "C" int qs_plan_block(const qs_plan *P, size_t i, int *k, int *qubits, do
     return QS_OK;
 }
 
-int qs_plan_upload(qs_plan *P, int dev)
+// Block matrices to the state's device.  For a state with stream-ordered
+// memory the matrices are too (allocated, copied and later freed in the
+// state's stream order), so serving never synchronizes the device.
+int qs_plan_upload(qs_plan *P, qs_state *s)
 {
-    if (P->mats && P->dev == dev) return QS_OK;
+    if (P->mats && P->dev == s->device) return QS_OK;
     if (P->mats) {
-        cudaFree(P->mats);
+        if (P->mats_async) cudaFreeAsync(P->mats, P->mats_stream);
+        else cudaFree(P->mats);
         P->mats = nullptr;
     }
     const size_t per = 2 * 64 * 64;
     std::vector<uint16_t> host(per * (P->blocks.size() ? P->blocks.size() : 1));
     for (size_t b = 0; b < P->blocks.size(); ++b) block_bf16(P->blocks[b], host.data() + b * per);
-    QS_CUDA_TRY(cudaMalloc(&P->mats, host.size() * sizeof(uint16_t)));
-    QS_CUDA_TRY(cudaMemcpy(P->mats, host.data(), host.size() * sizeof(uint16_t), cudaMemcpyHostToDevice));
-    P->dev = dev;
+    const size_t bytes = host.size() * sizeof(uint16_t);
+    if (s->stream_alloc) {
+        QS_CUDA_TRY(cudaMallocAsync(&P->mats, bytes, s->stream));
+        QS_CUDA_TRY(cudaMemcpyAsync(P->mats, host.data(), bytes, cudaMemcpyHostToDevice, s->stream));
+        QS_CUDA_TRY(cudaStreamSynchronize(s->stream));      // host buffer lifetime
+        P->mats_async = true;
+        P->mats_stream = s->stream;
+    } else {
+        QS_CUDA_TRY(cudaMalloc(&P->mats, bytes));
+        QS_CUDA_TRY(cudaMemcpy(P->mats, host.data(), bytes, cudaMemcpyHostToDevice));
+        P->mats_async = false;
+    }
+    P->dev = s->device;
     return QS_OK;
 }
 
@@ -419,12 +434,16 @@ extern "C" int qs_plan_apply_range(qs_state *s, qs_plan *P, size_t first, size_t
     }
     if (first > plan_launches(P) || count > plan_launches(P) - first)
         return qs_fail(QS_ERR_ARG, "qs_plan_apply_range: launches [%zu, +%zu) out of range", first, count);
-    if ((r = qs_plan_upload(P, s->device))) return r;
+    if ((r = qs_plan_upload(P, s))) return r;
     // Norm partials live in their own per-state buffer, so that other calls
     // between two qs_plan_apply_range calls cannot overwrite them:
     // [0] input norm of block 0, [1]/[2] output norms of even/odd blocks.
     const int G = qs_fused_grid(s);
-    if (!s->fused_norm) QS_CUDA_TRY(cudaMalloc(&s->fused_norm, 3 * (size_t)QS_SM_COUNT * 4 * sizeof(double)));
+    if (!s->fused_norm) {
+        void *p = nullptr;
+        if ((r = qs_dev_alloc(s, 3 * (size_t)QS_SM_COUNT * 4 * sizeof(double), &p))) return r;
+        s->fused_norm = static_cast<double *>(p);
+    }
     double *norm = s->fused_norm;
     // watchdog flag (result area of scratch), cleared before the first block
     const size_t kFlagOff = 64 * 1024 + 192;

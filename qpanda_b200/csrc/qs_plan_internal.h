@@ -1,6 +1,8 @@
 // qs_plan_internal.h - the fusion plan's structure, shared by the planner
 // (qs_plan.cpp) and the batched executor (qs_batch.cu).
 #pragma once
+#include <cuda_runtime.h>
+
 #include <complex>
 #include <vector>
 
@@ -31,6 +33,8 @@ struct qs_plan {
     std::vector<PlanPass> passes;        // tiled kernel only
     int dev = -1;                        // device holding mats
     void *mats = nullptr;                // [blocks][2][64][64] bf16
+    cudaStream_t mats_stream = nullptr;  // stream-ordered mats: freed with cudaFreeAsync on it
+    bool mats_async = false;
 };
 
 
