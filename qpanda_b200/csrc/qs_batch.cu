@@ -139,9 +139,11 @@ __global__ void __launch_bounds__(kThreads, 2) k_batch(BatchParams P)
                 }
             const bool last_pass = p + 1 == C.npass;
             double acc_out = 0;
-            if (p > 0) prefetch_row(C.amp, tile_base(0, L) | gC0, L, stage, row);
+            const uint64_t step = tile_base(1, L);
+            uint64_t tbase = 0;                       // tile_base(0)
+            if (p > 0) prefetch_row(C.amp, tbase | gC0, L, stage, row);
             for (uint64_t tile = 0; tile < tiles; ++tile) {
-                const uint64_t tbase = tile_base(tile, L);
+                const uint64_t tnext = tile_base_advance(tbase, step, L.tmask);
                 float x[64];
                 if (p == 0) {
                     // |0...0>: amplitude 0 is tile 0, the row with no row bits, column 0
@@ -151,7 +153,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_batch(BatchParams P)
                 } else {
                     asm volatile("cp.async.wait_group 0;" ::: "memory");
                     read_stage_row(stage, row, x);
-                    if (tile + 1 < tiles) prefetch_row(C.amp, tile_base(tile + 1, L) | gC0, L, stage, row);
+                    if (tile + 1 < tiles) prefetch_row(C.amp, tnext | gC0, L, stage, row);
 #pragma unroll
                     for (int e = 0; e < 64; ++e) x[e] *= scale;
                 }
@@ -211,6 +213,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_batch(BatchParams P)
                     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
                 }
                 if (failed) break;
+                tbase = tnext;
             }
             asm volatile("cp.async.wait_group 0;" ::: "memory");
             // the pass's output norm (fixed order), and the next pass's scale

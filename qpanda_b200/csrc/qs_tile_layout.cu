@@ -19,6 +19,7 @@ int qs_tile_layout_build(int n, const int *T, int nsub, const int (*qpos)[5], qs
             return qs_fail(QS_ERR_ARG, "tiled pass: tile qubits must be ascending and in range");
         local[q] = i;
         L->outer_low[i] = (1ull << q) - 1;
+        L->tmask |= 1ull << q;
     }
     int Q[kMaxSub][5], Cp[kMaxSub][7];
     for (int b = 0; b < nsub; ++b) {
