@@ -218,8 +218,9 @@ typedef struct qs_plan_opts {
     int low_qubits;        /* tiled passes: qubits 0..low_qubits-1 always in the tile (1..5) */
     int kernel;            /* QS_PLAN_SINGLE or QS_PLAN_TILED */
 } qs_plan_opts;
-/* Defaults: 5-qubit blocks, tiled passes of 12 qubits with up to 3 blocks,
- * qubits 0..2 in every tile. */
+/* Defaults: 5-qubit blocks, tiled passes of 12 qubits with up to 2 blocks
+ * (a pass of 3 blocks saves a pass but runs on a kernel with fewer resident
+ * CTAs, and measured slower overall), qubits 0..2 in every tile. */
 int qs_plan_default_opts(qs_plan_opts *opts);
 int qs_plan_create_ex(int n_qubits, const qs_gate *gates, size_t count, const qs_plan_opts *opts,
                       qs_plan **out);
@@ -231,6 +232,12 @@ int qs_plan_info(const qs_plan *plan, size_t *n_blocks, size_t *n_gates);
  * as 2048 doubles (either output may be NULL).  Row/column index bit b is
  * qubit qubits[b]. */
 int qs_plan_block(const qs_plan *plan, size_t i, int *k, int *qubits, double *matrix);
+/* Pass i of a tiled plan: its number of blocks (1..3), its 12 tile qubits
+ * (ascending) and each block's 5 qubits, row-major [3][5] (rows past
+ * *n_blocks untouched).  Any output may be NULL.  QS_ERR_ARG for a plan
+ * without tiled passes or i out of range.  No reference counterpart:
+ * introspection of this backend's fusion plan. */
+int qs_plan_pass(const qs_plan *plan, size_t i, int *n_blocks, int *tile_qubits, int *block_qubits);
 /* Apply every block in order (asynchronous, on the state's stream). */
 int qs_plan_apply(qs_state *s, qs_plan *plan);
 /* Apply launches (passes) [first, first + count) only (for timing or interleaving). */

@@ -100,6 +100,7 @@ def lib():
         "qs_plan_destroy": (i, [vp]),
         "qs_plan_info": (i, [vp, C.POINTER(sz), C.POINTER(sz)]),
         "qs_plan_block": (i, [vp, sz, ip, ip, dp]),
+        "qs_plan_pass": (i, [vp, sz, ip, ip, ip]),
         "qs_plan_apply": (i, [vp, vp]),
         "qs_plan_apply_range": (i, [vp, vp, sz, sz]),
         "qs_diff": (i, [vp, vp, dp, dp]),
@@ -267,7 +268,7 @@ class FusionPlan:
     (default) applies up to max_sub blocks per pass over the state;
     kernel="single" one block per pass."""
 
-    def __init__(self, n, gates, max_k=5, kernel="tiled", max_sub=3, low_qubits=3):
+    def __init__(self, n, gates, max_k=5, kernel="tiled", max_sub=2, low_qubits=3):
         g = np.ascontiguousarray(gates, dtype=GATE_DTYPE)
         self._keep = g
         h = C.c_void_p()
@@ -313,6 +314,17 @@ class FusionPlan:
         m = np.zeros(2 * 32 * 32)
         check(lib().qs_plan_block(self._h, i, C.byref(k), _iptr(q), _dptr(m)))
         return q.tolist(), m.view(np.complex128).reshape(32, 32)
+
+    def passes(self):
+        """Tiled plans: [(tile_qubits, [block qubits, ...]), ...] per pass."""
+        out = []
+        for i in range(self.num_launches()):
+            nb = C.c_int()
+            T = np.zeros(12, dtype=np.int32)
+            Q = np.zeros(15, dtype=np.int32)
+            check(lib().qs_plan_pass(self._h, i, C.byref(nb), _iptr(T), _iptr(Q)))
+            out.append((T.tolist(), [Q[5 * b:5 * b + 5].tolist() for b in range(nb.value)]))
+        return out
 
     def apply(self, sv):
         check(lib().qs_plan_apply(sv.handle, self._h))

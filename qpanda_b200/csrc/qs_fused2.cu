@@ -10,10 +10,9 @@
 // and block (split-BF16 x3, FP32 accumulation in TMEM, as in qs_fused.cu).
 //
 // Per tile, thread i of 128 owns row i and TMEM lane i (qs_tile_core.cuh):
-//   1. its row of block 0 arrives by cp.async (issued one tile ahead) in a
-//      staging row of its own; it reads it to registers, immediately issues
-//      the copies of the next tile into the same staging row, and writes the
-//      BF16 hi/lo split into the swizzled K-major A buffer (16-byte chunks);
+//   1. its row of block 0 arrives by cp.async in a staging row of its own; it
+//      reads it to registers and writes the BF16 hi/lo split into the
+//      swizzled K-major A buffer (16-byte chunks);
 //   2. for each block: one thread issues the 12 MMAs and commits to an
 //      mbarrier; every thread waits, loads its 64 FP32 results from TMEM, and
 //      either scatters them as BF16 hi/lo into the next block's A layout (one
@@ -21,8 +20,17 @@
 //      stores them to HBM in place.
 // A CTA walks tiles blockIdx.x, blockIdx.x + gridDim.x, ...; the global base
 // of the next tile is one masked add away from the current one.
-// Two CTAs per SM (112 KB of shared memory each).  Norm tracking and bounded
-// waits as in qs_fused.cu.
+//
+// Two shapes, chosen per pass by its number of blocks:
+//   * up to 2 blocks: 64 KB of shared memory, three CTAs per SM.  The staging
+//     rows live in the A region: the next tile's copies are issued as soon as
+//     the last block's MMAs have finished reading A, and land while the
+//     results go out to HBM;
+//   * 3 blocks: 112 KB, two CTAs per SM, a separate staging area filled one
+//     whole tile ahead.
+// The extra resident CTA is what pays: each tile is a serial chain (copy,
+// split, MMA, wait, scatter, MMA, wait, store) that one CTA cannot overlap.
+// Norm tracking and bounded waits as in qs_fused.cu.
 #include "qs_fused.h"
 #include "qs_tile_core.cuh"
 
@@ -30,25 +38,35 @@ namespace {
 
 using namespace qs_tile;
 
-constexpr uint32_t kOffA = 0;                     // A hi, A lo
-constexpr uint32_t kOffB = 2 * kA;                // B hi/lo per block
-constexpr uint32_t kOffStage = kOffB + kMaxSub * 2 * kB;
-constexpr uint32_t kOffMisc = kOffStage + kStage; // mbarrier (8), tmem address (4), scale (4)
-constexpr uint32_t kSmemBytes = kOffMisc + 16;
+template <int SUB>
+struct Shape {
+    static constexpr bool kStageInA = SUB <= 2;
+    static constexpr int kCtasPerSm = kStageInA ? 3 : 2;
+    static constexpr uint32_t kOffA = 0;                          // A hi, A lo
+    static constexpr uint32_t kOffB = 2 * kA;                     // B hi/lo per block
+    static constexpr uint32_t kOffStage = kStageInA ? kOffA : kOffB + SUB * 2 * kB;
+    static constexpr uint32_t kOffMisc = kOffB + SUB * 2 * kB + (kStageInA ? 0 : kStage);
+    static constexpr uint32_t kSmemBytes = kOffMisc + 16;         // mbarrier (8), tmem address (4), scale (4)
+    static_assert(kCtasPerSm * (kSmemBytes + 1024) <= 228 * 1024, "resident CTAs per SM");
+    static_assert(!kStageInA || 2 * kA == kStage, "the A region holds one tile of staging rows");
+};
 
 struct TileParams {
     Layout L;
     uint64_t tiles;
     const uint16_t *mat;         // nsub x [2][64][64] BF16 bits (hi, lo) of R
     int *err;
+    int nparts;                  // norm partials per pass (>= gridDim.x; the tail is written as zeros)
     const double *norm0;
     const double *prev_out;
     double *in_parts;
     double *out_parts;
 };
 
-__global__ void __launch_bounds__(kThreads, 2) k_fused_tile(float *__restrict__ amp, TileParams P)
+template <int SUB>
+__global__ void __launch_bounds__(kThreads, Shape<SUB>::kCtasPerSm) k_fused_tile(float *__restrict__ amp, TileParams P)
 {
+    using S = Shape<SUB>;
     extern __shared__ __align__(1024) uint8_t smem[];
     const int tid = threadIdx.x, warp = tid >> 5;
     if (smem_u32(smem) & 1023u) {             // swizzled operands need 1024-byte alignment
@@ -56,11 +74,11 @@ __global__ void __launch_bounds__(kThreads, 2) k_fused_tile(float *__restrict__ 
         return;
     }
     const Layout &L = P.L;
-    uint8_t *aHi = smem + kOffA, *aLo = smem + kOffA + kA;
-    uint64_t *mbar = reinterpret_cast<uint64_t *>(smem + kOffMisc);
-    uint32_t *tmem_holder = reinterpret_cast<uint32_t *>(smem + kOffMisc + 8);
-    float *s_scale = reinterpret_cast<float *>(smem + kOffMisc + 12);
-    const uint32_t stage = smem_u32(smem + kOffStage);
+    uint8_t *aHi = smem + S::kOffA, *aLo = smem + S::kOffA + kA;
+    uint64_t *mbar = reinterpret_cast<uint64_t *>(smem + S::kOffMisc);
+    uint32_t *tmem_holder = reinterpret_cast<uint32_t *>(smem + S::kOffMisc + 8);
+    float *s_scale = reinterpret_cast<float *>(smem + S::kOffMisc + 12);
+    const uint32_t stage = smem_u32(smem + S::kOffStage);
 
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
@@ -71,12 +89,12 @@ __global__ void __launch_bounds__(kThreads, 2) k_fused_tile(float *__restrict__ 
         asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(smem_u32(mbar)), "r"(1));
         asm volatile("fence.mbarrier_init.release.cluster;");
     }
-    load_b(smem + kOffB, P.mat, L.nsub);
+    load_b(smem + S::kOffB, P.mat, L.nsub);
     // scale undoing the previous pass's norm drift (fixed-order sums)
     if (warp == 1) {
         double n0 = 0, np = 0;
         if (P.norm0 && P.prev_out)
-            for (int i = tid - 32; i < (int)gridDim.x; i += 32) { n0 += P.norm0[i]; np += P.prev_out[i]; }
+            for (int i = tid - 32; i < P.nparts; i += 32) { n0 += P.norm0[i]; np += P.prev_out[i]; }
         for (int o = 16; o > 0; o >>= 1) {
             n0 += __shfl_xor_sync(0xffffffffu, n0, o);
             np += __shfl_xor_sync(0xffffffffu, np, o);
@@ -112,11 +130,15 @@ __global__ void __launch_bounds__(kThreads, 2) k_fused_tile(float *__restrict__ 
     if (tile < P.tiles) prefetch_row(amp, tbase | gC0, L, stage, row);
     for (; tile < P.tiles; tile += gridDim.x) {
         const uint64_t tnext = tile_base_advance(tbase, step, L.tmask);
+        const bool more = tile + gridDim.x < P.tiles;
         // ---- block 0 input: this thread's staging row -> registers -> A
         asm volatile("cp.async.wait_group 0;" ::: "memory");
         float x[64];
         read_stage_row(stage, row, x);
-        if (tile + gridDim.x < P.tiles) prefetch_row(amp, tnext | gC0, L, stage, row);
+        if constexpr (S::kStageInA)
+            __syncthreads();                  // every staging row is read before A overwrites them
+        else if (more)
+            prefetch_row(amp, tnext | gC0, L, stage, row);
         {
             float t = 0.f;
 #pragma unroll
@@ -129,12 +151,14 @@ __global__ void __launch_bounds__(kThreads, 2) k_fused_tile(float *__restrict__ 
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             __syncthreads();
             if (tid == 0)
-                issue_block_mma(tmem, a_hi, a_lo, smem_u32(smem + kOffB + (2 * b) * kB),
-                                smem_u32(smem + kOffB + (2 * b + 1) * kB), mb);
+                issue_block_mma(tmem, a_hi, a_lo, smem_u32(smem + S::kOffB + (2 * b) * kB),
+                                smem_u32(smem + S::kOffB + (2 * b + 1) * kB), mb);
             const bool ok = mbar_wait(mb, phase);
             phase ^= 1;
             if (__syncthreads_or(!ok)) { failed = true; break; }
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            if (S::kStageInA && b + 1 == L.nsub && more)
+                prefetch_row(amp, tnext | gC0, L, stage, row);   // the MMAs are done with A
             uint32_t y[4][16];
 #pragma unroll
             for (int q = 0; q < 4; ++q) tmem_ld16(taddr + 16 * q, y[q]);
@@ -184,7 +208,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_fused_tile(float *__restrict__ 
             ai += __shfl_xor_sync(0xffffffffu, ai, o);
             ao += __shfl_xor_sync(0xffffffffu, ao, o);
         }
-        double *red = reinterpret_cast<double *>(smem + kOffStage);     // staging is free now
+        double *red = reinterpret_cast<double *>(smem + S::kOffStage);   // staging is free now
         __syncthreads();
         if ((tid & 31) == 0) { red[warp] = ai; red[4 + warp] = ao; }
         __syncthreads();
@@ -194,6 +218,11 @@ __global__ void __launch_bounds__(kThreads, 2) k_fused_tile(float *__restrict__ 
             if (P.in_parts) P.in_parts[blockIdx.x] = a;
             if (P.out_parts) P.out_parts[blockIdx.x] = b;
         }
+        if (blockIdx.x == 0)                 // partials past this grid read as zero
+            for (int i = (int)gridDim.x + tid; i < P.nparts; i += kThreads) {
+                if (P.in_parts) P.in_parts[i] = 0.0;
+                if (P.out_parts) P.out_parts[i] = 0.0;
+            }
     }
     if (failed) {
         if (tid == 0) atomicExch(P.err, 1);
@@ -207,12 +236,28 @@ __global__ void __launch_bounds__(kThreads, 2) k_fused_tile(float *__restrict__ 
     }
 }
 
+uint64_t grid_for(const qs_state *s, int ctas_per_sm)
+{
+    const uint64_t tiles = s->N >> 12, cap = (uint64_t)QS_SM_COUNT * ctas_per_sm;
+    return tiles < cap ? tiles : cap;
+}
+
+template <int SUB>
+int launch(qs_state *s, TileParams &P)
+{
+    using S = Shape<SUB>;
+    QS_CUDA_TRY(cudaFuncSetAttribute(k_fused_tile<SUB>, cudaFuncAttributeMaxDynamicSharedMemorySize, S::kSmemBytes));
+    const unsigned grid = (unsigned)grid_for(s, S::kCtasPerSm);
+    k_fused_tile<SUB><<<grid, kThreads, S::kSmemBytes, s->stream>>>(static_cast<float *>(s->amp), P);
+    QS_LAUNCH_CHECK("k_fused_tile");
+    return QS_OK;
+}
+
 }  // namespace
 
 int qs_tiled_grid(const qs_state *s)
 {
-    uint64_t tiles = s->N >> 12;
-    return (int)(tiles < (uint64_t)QS_SM_COUNT * 2 ? tiles : (uint64_t)QS_SM_COUNT * 2);
+    return (int)grid_for(s, Shape<2>::kCtasPerSm);    // the larger of the two grids
 }
 
 int qs_launch_tiled(qs_state *s, const qs_tiled_desc *d, int *err_dev)
@@ -226,13 +271,10 @@ int qs_launch_tiled(qs_state *s, const qs_tiled_desc *d, int *err_dev)
     P.tiles = s->N >> 12;
     P.mat = static_cast<const uint16_t *>(d->mat_dev);
     P.err = err_dev;
+    P.nparts = qs_tiled_grid(s);
     P.norm0 = d->norm0;
     P.prev_out = d->prev_out;
     P.in_parts = d->in_parts;
     P.out_parts = d->out_parts;
-    QS_CUDA_TRY(cudaFuncSetAttribute(k_fused_tile, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes));
-    const unsigned grid = (unsigned)qs_tiled_grid(s);
-    k_fused_tile<<<grid, kThreads, kSmemBytes, s->stream>>>(static_cast<float *>(s->amp), P);
-    QS_LAUNCH_CHECK("k_fused_tile");
-    return QS_OK;
+    return d->nsub <= 2 ? launch<2>(s, P) : launch<3>(s, P);
 }

@@ -280,7 +280,7 @@ extern "C" int qs_plan_default_opts(qs_plan_opts *o)
     if (!o) return qs_fail(QS_ERR_ARG, "qs_plan_default_opts: null");
     o->block_qubits = 5;
     o->tile_qubits = 12;
-    o->max_sub = 3;
+    o->max_sub = 2;              // passes of <= 2 blocks run three CTAs per SM (qs_fused2.cu)
     o->low_qubits = 3;
     o->kernel = QS_PLAN_TILED;
     return QS_OK;
@@ -350,6 +350,19 @@ extern "C" int qs_plan_block(const qs_plan *P, size_t i, int *k, int *qubits, do
         for (int b = 0; b < 5; ++b) qubits[b] = B.q[b];
     if (matrix)
         for (int j = 0; j < 32 * 32; ++j) { matrix[2 * j] = B.U[j].real(); matrix[2 * j + 1] = B.U[j].imag(); }
+    return QS_OK;
+}
+
+extern "C" int qs_plan_pass(const qs_plan *P, size_t i, int *n_blocks, int *tile_qubits, int *block_qubits)
+{
+    if (!P || i >= P->passes.size()) return qs_fail(QS_ERR_ARG, "qs_plan_pass: no tiled pass %zu", i);
+    const PlanPass &S = P->passes[i];
+    if (n_blocks) *n_blocks = (int)S.count;
+    if (tile_qubits)
+        for (int j = 0; j < 12; ++j) tile_qubits[j] = S.T[j];
+    if (block_qubits)
+        for (size_t b = 0; b < S.count; ++b)
+            for (int j = 0; j < 5; ++j) block_qubits[5 * b + j] = P->blocks[S.first + b].q[j];
     return QS_OK;
 }
 

@@ -27,13 +27,16 @@ constexpr unsigned long long kWaitNs = 2000000000ull;   // bound on every wait
 // block's results feed the next block's rows and columns, where the last
 // block's results go.  Built on the host (qs_tile_layout_build).
 struct Layout {
-    uint64_t outer_low[12];      // (1 << tile position) - 1, ascending: tile index -> global base
     uint64_t tmask;              // the 12 tile positions as a bit mask
     uint64_t g0[32];             // global offset of column j, block 0
     uint64_t gl[32];             // global offset of column j, last block
     int32_t c0_glob[7];          // global position of row bit i, block 0
     int32_t cl_glob[7];          // global position of row bit i, last block
     int32_t nsub, vec0, vecl, pad;
+    int8_t tpos[12];             // global position of tile bit i (= T[i], ascending)
+    int8_t cl_loc[7];            // tile bit of row bit i, last block
+    int8_t pad2;
+    uint16_t lout[32];           // tile bits of column j, last block (a 12-bit tile index)
     int8_t rowmap[kMaxSub - 1][7];   // row bit i of block b -> row bit (>= 0) or ~column bit of block b+1
     // Byte offset, within block b+1's swizzled A buffer, of the result in
     // column j of block b is  thread_part ^ scat[b][j]: the row/column bits a
@@ -66,8 +69,8 @@ __device__ __forceinline__ uint64_t tile_base(uint64_t tile, const Layout &L)
 {
 #pragma unroll 4
     for (int j = 0; j < 12; ++j) {
-        const uint64_t lo = tile & L.outer_low[j];
-        tile = ((tile & ~L.outer_low[j]) << 1) | lo;
+        const uint64_t low = (1ull << L.tpos[j]) - 1;
+        tile = ((tile & ~low) << 1) | (tile & low);
     }
     return tile;
 }

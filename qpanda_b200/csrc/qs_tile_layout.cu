@@ -18,7 +18,6 @@ int qs_tile_layout_build(int n, const int *T, int nsub, const int (*qpos)[5], qs
         if (q < 0 || q >= n || (i && q <= T[i - 1]))
             return qs_fail(QS_ERR_ARG, "tiled pass: tile qubits must be ascending and in range");
         local[q] = i;
-        L->outer_low[i] = (1ull << q) - 1;
         L->tmask |= 1ull << q;
     }
     int Q[kMaxSub][5], Cp[kMaxSub][7];
@@ -36,9 +35,17 @@ int qs_tile_layout_build(int n, const int *T, int nsub, const int (*qpos)[5], qs
     }
     L->nsub = nsub;
     const int last = nsub - 1;
+    for (int i = 0; i < 12; ++i) L->tpos[i] = (int8_t)T[i];
     for (int i = 0; i < 7; ++i) {
         L->c0_glob[i] = T[Cp[0][i]];
         L->cl_glob[i] = T[Cp[last][i]];
+        L->cl_loc[i] = (int8_t)Cp[last][i];
+    }
+    for (int j = 0; j < 32; ++j) {
+        uint32_t t = 0;
+        for (int i = 0; i < 5; ++i)
+            if (j & (1 << i)) t |= 1u << Q[last][i];
+        L->lout[j] = (uint16_t)t;
     }
     for (int j = 0; j < 32; ++j) {
         uint64_t a = 0, b = 0;

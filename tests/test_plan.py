@@ -54,8 +54,13 @@ def test_plan_pass_count_32q():
     g = circuits.random_layers(32, 16, 20240601, iswap_frac=0.1)
     p = FusionPlan(32, g, kernel="single")
     assert p.num_blocks() <= 90 and p.num_launches() == p.num_blocks()   # vs ~640 per-gate passes
-    t = FusionPlan(32, g, kernel="tiled")
-    assert t.num_launches() <= 40         # up to 3 blocks per pass within 12 tile qubits
+    t3 = FusionPlan(32, g, kernel="tiled", max_sub=3)
+    assert t3.num_launches() <= 40        # up to 3 blocks per pass within 12 tile qubits
+    t2 = FusionPlan(32, g, kernel="tiled")  # default: up to 2 blocks per pass
+    assert t3.num_launches() <= t2.num_launches() <= 48
+    for T, blocks in t2.passes():
+        assert 1 <= len(blocks) <= 2 and T[:3] == [0, 1, 2] and T == sorted(T)
+        assert all(set(q) <= set(T) for q in blocks)
 
 
 def test_plan_rejects_wide_gates_and_bad_width():
