@@ -21,6 +21,7 @@
 #include <thread>
 #include <vector>
 
+#include "qs_fused.h"
 #include "qs_plan_internal.h"
 #include "qs_prim.h"
 #include "qs_tile_core.cuh"
@@ -394,7 +395,9 @@ extern "C" int qs_batch_create(int n_circ, const int *n_qubits, const qs_gate *g
             int qpos[3][5];
             for (size_t b = 0; b < pass.count; ++b)
                 for (int j = 0; j < 5; ++j) qpos[b][j] = pp->blocks[pass.first + b].q[j];
-            if ((r = qs_tile_layout_build(pp->n, pass.T, (int)pass.count, qpos, &L))) break;
+            int rows[3][7];
+            if ((r = qs_tile_row_orders(pp->n, pass.T, (int)pass.count, qpos, rows))) break;
+            if ((r = qs_tile_layout_build(pp->n, pass.T, (int)pass.count, qpos, rows, &L))) break;
             L.pad = (int32_t)pass.first;
             layouts.push_back(L);
         }

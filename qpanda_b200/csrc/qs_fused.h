@@ -30,6 +30,8 @@ struct qs_tiled_desc {
     int T[12];
     int nsub;
     int qpos[3][5];
+    int has_rows;                // rows[b] = block b's other tile qubits in row-bit order (else ascending)
+    int rows[3][7];
     const void *mat_dev;
     const double *norm0;
     const double *prev_out;
@@ -38,4 +40,8 @@ struct qs_tiled_desc {
 };
 
 int qs_tiled_grid(const qs_state *s);
+// Row-bit orders for a pass's blocks that keep warp-wide accesses coalesced
+// and the scatter between blocks free of shared-memory bank conflicts as far
+// as possible (qs_tile_layout.cu).  rows[b][i] = global qubit of row bit i.
+int qs_tile_row_orders(int n, const int *T, int nsub, const int (*qpos)[5], int (*rows)[7]);
 int qs_launch_tiled(qs_state *s, const qs_tiled_desc *d, int *err_dev);

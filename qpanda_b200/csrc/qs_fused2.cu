@@ -266,7 +266,7 @@ int qs_launch_tiled(qs_state *s, const qs_tiled_desc *d, int *err_dev)
     if (s->n < 12) return qs_fail(QS_ERR_UNSUPPORTED, "tiled passes: need at least 12 qubits");
     TileParams P;
     memset(&P, 0, sizeof(P));
-    int r = qs_tile_layout_build(s->n, d->T, d->nsub, d->qpos, &P.L);
+    int r = qs_tile_layout_build(s->n, d->T, d->nsub, d->qpos, d->has_rows ? d->rows : nullptr, &P.L);
     if (r) return r;
     P.tiles = s->N >> 12;
     P.mat = static_cast<const uint16_t *>(d->mat_dev);

@@ -236,6 +236,11 @@ int build_passes(qs_plan *P)
             P->blocks.push_back(std::move(B));
         }
         pass.count = P->blocks.size() - pass.first;
+        int qpos[3][5];
+        for (size_t b = 0; b < pass.count && b < 3; ++b)
+            for (int j = 0; j < 5; ++j) qpos[b][j] = P->blocks[pass.first + b].q[j];
+        if (P->n >= TQ && (r = qs_tile_row_orders(P->n, pass.T, (int)pass.count, qpos, pass.rows)))
+            return r;                        // narrower states run the gates per gate
         P->passes.push_back(pass);
     }
     return QS_OK;
@@ -473,6 +478,8 @@ extern "C" int qs_plan_apply_range(qs_state *s, qs_plan *P, size_t first, size_t
             d.nsub = (int)pp.count;
             for (size_t b = 0; b < pp.count; ++b)
                 for (int j = 0; j < 5; ++j) d.qpos[b][j] = P->blocks[pp.first + b].q[j];
+            d.has_rows = 1;
+            memcpy(d.rows, pp.rows, sizeof(d.rows));
             d.mat_dev = static_cast<const char *>(P->mats) + pp.first * per;
             d.norm0 = u ? norm : nullptr;
             d.prev_out = u ? norm + GT * (1 + (u - 1) % 2) : nullptr;

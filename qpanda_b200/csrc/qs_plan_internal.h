@@ -22,6 +22,7 @@ struct PlanBlock {
 struct PlanPass {
     int T[12] = {0};                     // ascending global qubits of the tile
     size_t first = 0, count = 0;         // its blocks: blocks[first, first + count)
+    int rows[3][7] = {};                 // each block's other tile qubits in row-bit order (qs_tile_row_orders)
 };
 
 struct qs_plan {

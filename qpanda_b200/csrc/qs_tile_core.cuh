@@ -260,4 +260,5 @@ __device__ __forceinline__ void load_b(uint8_t *dst, const uint16_t *mat, int ns
 
 // Host: the Layout of a pass with tile qubits T[12] (ascending, global) and
 // nsub blocks on qpos[b][5] (ascending, within T).  QS_OK or QS_ERR_ARG.
-int qs_tile_layout_build(int n, const int *T, int nsub, const int (*qpos)[5], qs_tile::Layout *L);
+int qs_tile_layout_build(int n, const int *T, int nsub, const int (*qpos)[5], const int (*rows)[7],
+                         qs_tile::Layout *L);

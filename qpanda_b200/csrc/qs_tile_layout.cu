@@ -3,10 +3,144 @@
 // columns and which 7 its rows, and the tables that route block b's results
 // into block b+1's rows and columns.
 #include <cstring>
+#include <utility>
+#include <vector>
 
 #include "qs_tile_core.cuh"
 
-int qs_tile_layout_build(int n, const int *T, int nsub, const int (*qpos)[5], qs_tile::Layout *L)
+namespace {
+
+using qs_tile::kMaxSub;
+
+// A block's 7 row bits may be listed in any order: rows are independent
+// columns of the contraction.  The order decides which tile bits a warp's 32
+// lanes (row bits 0..4) run over, and with it
+//   * how many 32-byte sectors one warp-wide global load (block 0) or store
+//     (last block) touches: lanes on qubits 0 and 1 share sectors;
+//   * how many shared-memory wavefronts one warp-wide 4-byte scatter store
+//     into the next block's swizzled A buffer takes: the bank of a store is
+//     offset bits 2..6 = the next block's column bits 0..1 and (column bits
+//     2..4 XOR row bits 0..2); a lane bit that lands on none of them, or on
+//     one another lane bit already took, doubles the wavefronts.
+// Costs are warp-level transactions per tile, up to a common factor.
+struct RowCfg {
+    int t[3];                    // tile bits of row bits 0..2
+    unsigned lanes;              // tile bits of row bits 0..4, as a mask
+};
+
+int glob_cost(unsigned lanes, int loc0, int loc1, bool vec)
+{
+    int k = 0;
+    if (loc1 >= 0) k += (lanes >> loc1) & 1;
+    if (!vec && loc0 >= 0) k += (lanes >> loc0) & 1;
+    return (vec ? 16 : 32) * (32 >> k);
+}
+
+int scatter_cost(unsigned lanes, const int *Qn, const int *t)
+{
+    unsigned hit = 0;
+    for (int c = 0; c < 5; ++c) hit |= ((lanes >> Qn[c]) & 1u) << (2 + c);
+    for (int r = 0; r < 3; ++r) hit |= ((lanes >> t[r]) & 1u) << (4 + r);
+    return 64 << (5 - __builtin_popcount(hit));
+}
+
+// Row orders (tile bits) for each block minimising the costs above, by
+// dynamic programming over the blocks; ascending order unless another order
+// is strictly cheaper.
+void choose_row_orders(const int *T, int nsub, const int (*Q)[5], int (*Cp)[7])
+{
+    int loc0 = -1, loc1 = -1;
+    for (int i = 0; i < 12; ++i) {
+        if (T[i] == 0) loc0 = i;
+        if (T[i] == 1) loc1 = i;
+    }
+    const bool vec0 = T[Q[0][0]] == 0, vecl = T[Q[nsub - 1][0]] == 0;
+    std::vector<RowCfg> cfg[kMaxSub];
+    for (int b = 0; b < nsub; ++b) {
+        const int *C = Cp[b];
+        // configuration 0 is the ascending order
+        for (int i = 0; i < 7; ++i)
+            for (int j = 0; j < 7; ++j)
+                for (int k = 0; k < 7; ++k) {
+                    if (i == j || i == k || j == k) continue;
+                    int rest[4], nr = 0;
+                    for (int m = 0; m < 7; ++m)
+                        if (m != i && m != j && m != k) rest[nr++] = C[m];
+                    const unsigned m3 = (1u << C[i]) | (1u << C[j]) | (1u << C[k]);
+                    for (int u = 0; u < 4; ++u)
+                        for (int v = u + 1; v < 4; ++v)
+                            cfg[b].push_back(RowCfg{{C[i], C[j], C[k]}, m3 | (1u << rest[u]) | (1u << rest[v])});
+                }
+    }
+    std::vector<int> best[kMaxSub], from[kMaxSub];
+    best[0].resize(cfg[0].size());
+    for (size_t i = 0; i < cfg[0].size(); ++i) best[0][i] = glob_cost(cfg[0][i].lanes, loc0, loc1, vec0);
+    for (int b = 1; b < nsub; ++b) {
+        // the previous block enters only through its lane set: keep its cheapest configuration per set
+        std::vector<std::pair<unsigned, int>> sets;     // (lanes, configuration)
+        for (size_t p = 0; p < cfg[b - 1].size(); ++p) {
+            size_t s = 0;
+            while (s < sets.size() && sets[s].first != cfg[b - 1][p].lanes) ++s;
+            if (s == sets.size()) sets.push_back({cfg[b - 1][p].lanes, (int)p});
+            else if (best[b - 1][p] < best[b - 1][sets[s].second]) sets[s].second = (int)p;
+        }
+        best[b].assign(cfg[b].size(), 1 << 30);
+        from[b].assign(cfg[b].size(), -1);
+        for (size_t i = 0; i < cfg[b].size(); ++i)
+            for (const auto &s : sets) {
+                const int c = best[b - 1][s.second] + scatter_cost(s.first, Q[b], cfg[b][i].t);
+                if (c < best[b][i]) { best[b][i] = c; from[b][i] = s.second; }
+            }
+    }
+    const int last = nsub - 1;
+    int sel[kMaxSub] = {0, 0, 0}, bestc = 1 << 30;
+    for (size_t i = 0; i < cfg[last].size(); ++i) {
+        const int c = best[last][i] + glob_cost(cfg[last][i].lanes, loc0, loc1, vecl);
+        if (c < bestc) { bestc = c; sel[last] = (int)i; }
+    }
+    // cost of the ascending orders (configuration 0 everywhere)
+    int base = glob_cost(cfg[0][0].lanes, loc0, loc1, vec0) + glob_cost(cfg[last][0].lanes, loc0, loc1, vecl);
+    for (int b = 1; b < nsub; ++b) base += scatter_cost(cfg[b - 1][0].lanes, Q[b], cfg[b][0].t);
+    if (bestc >= base) return;
+    for (int b = last; b > 0; --b) sel[b - 1] = from[b][sel[b]];
+    for (int b = 0; b < nsub; ++b) {
+        const RowCfg &c = cfg[b][sel[b]];
+        int order[7], n = 0;
+        for (int r = 0; r < 3; ++r) order[n++] = c.t[r];
+        for (int m = 0; m < 7; ++m)          // row bits 3, 4: the other lanes, ascending
+            if (((c.lanes >> Cp[b][m]) & 1) && Cp[b][m] != c.t[0] && Cp[b][m] != c.t[1] && Cp[b][m] != c.t[2])
+                order[n++] = Cp[b][m];
+        for (int m = 0; m < 7; ++m)          // row bits 5, 6
+            if (!((c.lanes >> Cp[b][m]) & 1)) order[n++] = Cp[b][m];
+        for (int m = 0; m < 7; ++m) Cp[b][m] = order[m];
+    }
+}
+
+}  // namespace
+
+int qs_tile_row_orders(int n, const int *T, int nsub, const int (*qpos)[5], int (*rows)[7])
+{
+    qs_tile::Layout L;
+    int r = qs_tile_layout_build(n, T, nsub, qpos, nullptr, &L);   // validates the pass
+    if (r) return r;
+    int local[64];
+    for (int i = 0; i < 64; ++i) local[i] = -1;
+    for (int i = 0; i < 12; ++i) local[T[i]] = i;
+    int Q[kMaxSub][5], Cp[kMaxSub][7];
+    for (int b = 0; b < nsub; ++b) {
+        uint32_t qm = 0;
+        for (int i = 0; i < 5; ++i) { Q[b][i] = local[qpos[b][i]]; qm |= 1u << Q[b][i]; }
+        for (int p = 0, c = 0; p < 12; ++p)
+            if (!(qm & (1u << p))) Cp[b][c++] = p;
+    }
+    choose_row_orders(T, nsub, Q, Cp);
+    for (int b = 0; b < nsub; ++b)
+        for (int i = 0; i < 7; ++i) rows[b][i] = T[Cp[b][i]];
+    return QS_OK;
+}
+
+int qs_tile_layout_build(int n, const int *T, int nsub, const int (*qpos)[5], const int (*rows)[7],
+                         qs_tile::Layout *L)
 {
     using qs_tile::kMaxSub;
     if (nsub < 1 || nsub > kMaxSub) return qs_fail(QS_ERR_ARG, "tiled pass: %d blocks", nsub);
@@ -32,6 +166,16 @@ int qs_tile_layout_build(int n, const int *T, int nsub, const int (*qpos)[5], qs
         }
         for (int p = 0, c = 0; p < 12; ++p)
             if (!(qm & (1u << p))) Cp[b][c++] = p;
+        if (rows) {                              // a given order of the same row bits
+            uint32_t rm = 0;
+            for (int i = 0; i < 7; ++i) {
+                const int q = rows[b][i];
+                if (q < 0 || q >= n || local[q] < 0 || (qm & (1u << local[q])) || (rm & (1u << local[q])))
+                    return qs_fail(QS_ERR_ARG, "tiled pass: row order must list the block's other tile qubits");
+                rm |= 1u << local[q];
+                Cp[b][i] = local[q];
+            }
+        }
     }
     L->nsub = nsub;
     const int last = nsub - 1;
