@@ -261,7 +261,7 @@ typedef struct qs_batch qs_batch;
 #define QS_BATCH_LONGEST_FIRST 0
 #define QS_BATCH_INPUT_ORDER   1
 typedef struct qs_batch_opts {
-    int max_sub;           /* fused blocks per pass, 1..3 */
+    int max_sub;           /* fused blocks per pass, 1..3 (default 2: three CTAs per SM) */
     int low_qubits;        /* qubits 0..low_qubits-1 in every tile, 1..5 */
     int order;             /* QS_BATCH_LONGEST_FIRST or QS_BATCH_INPUT_ORDER */
     int use_graph;         /* capture the launch in a CUDA graph and replay it */

@@ -31,18 +31,28 @@ namespace {
 using namespace qs_tile;
 
 constexpr int kMaxZZ = 23;                        // circuits of up to 24 qubits
-constexpr uint32_t kOffA = 0;
-constexpr uint32_t kOffB = 2 * kA;
-constexpr uint32_t kOffStage = kOffB + kMaxSub * 2 * kB;
-constexpr uint32_t kOffLayout = kOffStage + kStage;
 constexpr uint32_t kLayoutBytes = (sizeof(Layout) + 15) & ~15u;
-constexpr uint32_t kOffMisc = kOffLayout + kLayoutBytes;   // mbarrier 8, tmem 4, circuit 4, pad
-constexpr uint32_t kSmemBytes = kOffMisc + 16;
+
+// Shared memory of the two shapes (as in qs_fused2.cu): with up to 2 blocks
+// per pass the staging rows live in the A region and three CTAs fit per SM;
+// with 3 blocks there is a separate staging area and two CTAs per SM.
 // Reductions (4 + 4 x kMaxZZ doubles) reuse the staging rows: they run only
-// when no copy into staging is in flight.  Two CTAs per SM need
-// 2 x (kSmemBytes + 1 KB reserved) <= 228 KB.
-constexpr uint32_t kOffRed = kOffStage;
-static_assert(2 * (kSmemBytes + 1024) <= 228 * 1024, "two CTAs per SM");
+// when no copy into staging is in flight and no MMA reads A.
+template <int SUB>
+struct BShape {
+    static constexpr bool kStageInA = SUB <= 2;
+    static constexpr int kCtasPerSm = kStageInA ? 3 : 2;
+    static constexpr uint32_t kOffA = 0;
+    static constexpr uint32_t kOffB = 2 * kA;
+    static constexpr uint32_t kOffStage = kStageInA ? kOffA : kOffB + SUB * 2 * kB;
+    static constexpr uint32_t kOffLayout = kOffB + SUB * 2 * kB + (kStageInA ? 0 : kStage);
+    static constexpr uint32_t kOffMisc = kOffLayout + kLayoutBytes;   // mbarrier 8, tmem 4, circuit 4
+    static constexpr uint32_t kSmemBytes = kOffMisc + 16;
+    static constexpr uint32_t kOffRed = kOffStage;
+    static_assert(kCtasPerSm * (kSmemBytes + 1024) <= 228 * 1024, "resident CTAs per SM");
+    static_assert(!kStageInA || 2 * kA == kStage, "the A region holds one tile of staging rows");
+    static_assert((4 + 4 * kMaxZZ) * 8 <= kStage, "reductions fit the staging rows");
+};
 
 struct BatchCirc {
     float *amp;                  // 2^nq_eff complex64
@@ -60,21 +70,23 @@ struct BatchParams {
     int *err;
 };
 
-__global__ void __launch_bounds__(kThreads, 2) k_batch(BatchParams P)
+template <int SUB>
+__global__ void __launch_bounds__(kThreads, BShape<SUB>::kCtasPerSm) k_batch(BatchParams P)
 {
+    using S = BShape<SUB>;
     extern __shared__ __align__(1024) uint8_t smem[];
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     if (smem_u32(smem) & 1023u) {
         if (tid == 0) atomicExch(P.err, 2);
         return;
     }
-    uint8_t *aHi = smem + kOffA, *aLo = smem + kOffA + kA;
-    Layout &L = *reinterpret_cast<Layout *>(smem + kOffLayout);
-    uint64_t *mbar = reinterpret_cast<uint64_t *>(smem + kOffMisc);
-    uint32_t *tmem_holder = reinterpret_cast<uint32_t *>(smem + kOffMisc + 8);
-    int32_t *s_circ = reinterpret_cast<int32_t *>(smem + kOffMisc + 12);
-    double *red = reinterpret_cast<double *>(smem + kOffRed);
-    const uint32_t stage = smem_u32(smem + kOffStage);
+    uint8_t *aHi = smem + S::kOffA, *aLo = smem + S::kOffA + kA;
+    Layout &L = *reinterpret_cast<Layout *>(smem + S::kOffLayout);
+    uint64_t *mbar = reinterpret_cast<uint64_t *>(smem + S::kOffMisc);
+    uint32_t *tmem_holder = reinterpret_cast<uint32_t *>(smem + S::kOffMisc + 8);
+    int32_t *s_circ = reinterpret_cast<int32_t *>(smem + S::kOffMisc + 12);
+    double *red = reinterpret_cast<double *>(smem + S::kOffRed);
+    const uint32_t stage = smem_u32(smem + S::kOffStage);
 
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
@@ -121,7 +133,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_batch(BatchParams P)
                 for (int i = tid; i < (int)(sizeof(Layout) / 4); i += kThreads) dst[i] = src[i];
             }
             __syncthreads();
-            load_b(smem + kOffB, C.mats + (size_t)L.pad * 2 * 64 * 64, L.nsub);
+            load_b(smem + S::kOffB, C.mats + (size_t)L.pad * 2 * 64 * 64, L.nsub);
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             __syncthreads();
             uint64_t gC0 = 0, gCl = 0;
@@ -154,7 +166,10 @@ __global__ void __launch_bounds__(kThreads, 2) k_batch(BatchParams P)
                 } else {
                     asm volatile("cp.async.wait_group 0;" ::: "memory");
                     read_stage_row(stage, row, x);
-                    if (tile + 1 < tiles) prefetch_row(C.amp, tnext | gC0, L, stage, row);
+                    if constexpr (S::kStageInA)
+                        __syncthreads();      // every staging row is read before A overwrites them
+                    else if (tile + 1 < tiles)
+                        prefetch_row(C.amp, tnext | gC0, L, stage, row);
 #pragma unroll
                     for (int e = 0; e < 64; ++e) x[e] *= scale;
                 }
@@ -165,12 +180,14 @@ __global__ void __launch_bounds__(kThreads, 2) k_batch(BatchParams P)
                     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
                     __syncthreads();
                     if (tid == 0)
-                        issue_block_mma(tmem, a_hi, a_lo, smem_u32(smem + kOffB + (2 * b) * kB),
-                                        smem_u32(smem + kOffB + (2 * b + 1) * kB), mb);
+                        issue_block_mma(tmem, a_hi, a_lo, smem_u32(smem + S::kOffB + (2 * b) * kB),
+                                        smem_u32(smem + S::kOffB + (2 * b + 1) * kB), mb);
                     const bool ok = mbar_wait(mb, phase);
                     phase ^= 1;
                     if (__syncthreads_or(!ok)) { failed = true; break; }
                     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                    if (S::kStageInA && p > 0 && b + 1 == L.nsub && tile + 1 < tiles)
+                        prefetch_row(C.amp, tnext | gC0, L, stage, row);   // the MMAs are done with A
                     uint32_t y[4][16];
 #pragma unroll
                     for (int q = 0; q < 4; ++q) tmem_ld16(taddr + 16 * q, y[q]);
@@ -306,7 +323,7 @@ std::string signature(int nq, const qs_gate *g, size_t count)
 extern "C" int qs_batch_default_opts(qs_batch_opts *o)
 {
     if (!o) return qs_fail(QS_ERR_ARG, "qs_batch_default_opts: null");
-    o->max_sub = 3;
+    o->max_sub = 2;              // three CTAs per SM (BShape)
     o->low_qubits = 3;
     o->order = QS_BATCH_LONGEST_FIRST;
     o->use_graph = 1;
@@ -474,8 +491,13 @@ int batch_launch(qs_batch *B, cudaStream_t st)
     P.ncirc = B->n;
     P.head = B->d_head;
     P.err = B->d_head + 1;
-    const unsigned grid = (unsigned)std::min(B->n, QS_SM_COUNT * 2);
-    k_batch<<<grid, kThreads, kSmemBytes, st>>>(P);
+    if (B->opts.max_sub <= 2) {
+        const unsigned grid = (unsigned)std::min(B->n, QS_SM_COUNT * BShape<2>::kCtasPerSm);
+        k_batch<2><<<grid, kThreads, BShape<2>::kSmemBytes, st>>>(P);
+    } else {
+        const unsigned grid = (unsigned)std::min(B->n, QS_SM_COUNT * BShape<3>::kCtasPerSm);
+        k_batch<3><<<grid, kThreads, BShape<3>::kSmemBytes, st>>>(P);
+    }
     QS_LAUNCH_CHECK("k_batch");
     return QS_OK;
 }
@@ -486,7 +508,8 @@ extern "C" int qs_batch_run(qs_batch *B, void *stream)
 {
     if (!B) return qs_fail(QS_ERR_ARG, "qs_batch_run: null batch");
     cudaStream_t st = static_cast<cudaStream_t>(stream);
-    QS_CUDA_TRY(cudaFuncSetAttribute(k_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes));
+    QS_CUDA_TRY(cudaFuncSetAttribute(k_batch<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, BShape<2>::kSmemBytes));
+    QS_CUDA_TRY(cudaFuncSetAttribute(k_batch<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, BShape<3>::kSmemBytes));
     if (!B->opts.use_graph) return batch_launch(B, st);
     if (!B->graph_exec) {
         // capture once on a private stream; replay on the caller's stream
