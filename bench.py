@@ -47,6 +47,8 @@ def parse():
     ap.add_argument("--path", default="fused", choices=["plain", "fused"])
     ap.add_argument("--kernel", default="tiled", choices=["tiled", "single"],
                     help="fused path: tiled passes (up to 3 blocks per pass) or one block per pass")
+    ap.add_argument("--remap", type=int, default=1, choices=[0, 1],
+                    help="tiled passes: 1 = contiguous tile writes through a second state-size buffer")
     ap.add_argument("--qubits", type=int, default=N_QUBITS)
     ap.add_argument("--depth", type=int, default=DEPTH)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -242,10 +244,17 @@ def timed_steps(L, h, gates, plan, steps, stream, torch, kinds, path):
     fused_name = ("k_fused_tile (tiled pass)" if getattr(plan, "kernel", "tiled") == "tiled"
                   else "k_fused_tc (5-qubit block)")
     gptr = [gates[i:i + 1].ctypes.data for i in range(ng)]
+    whole = path == "fused" and getattr(plan, "remap", False)
     ev = [[torch.cuda.Event(enable_timing=True) for _ in range(nl + 1)] for _ in range(steps)]
     for k in range(steps):
         check(L.qs_reset_zero(h))
         ev[k][0].record(stream)
+        if whole:
+            # a remapping plan's passes hand their layouts on to each other:
+            # one application, timed as a whole
+            check(L.qs_plan_apply(h, plan.handle))
+            ev[k][nl].record(stream)
+            continue
         for i in range(nl):
             if path == "fused":
                 check(L.qs_plan_apply_range(h, plan.handle, i, 1))
@@ -256,6 +265,9 @@ def timed_steps(L, h, gates, plan, steps, stream, torch, kinds, path):
     out = []
     for k in range(steps):
         out.append(ev[k][0].elapsed_time(ev[k][nl]) / 1e3)
+        if whole:
+            kinds.setdefault(fused_name, []).extend([out[-1] / nl] * nl)
+            continue
         for i in range(nl):
             kind = fused_name if path == "fused" else kernel_kind(gates[i])
             kinds.setdefault(kind, []).append(ev[k][i].elapsed_time(ev[k][i + 1]) / 1e3)
@@ -286,7 +298,9 @@ def run_b200(args):
     stream = torch.cuda.current_stream()
     sv = StateVector(n, "c64")
     h = sv.handle
-    plan = FusionPlan(n, gates, kernel=args.kernel)
+    remap = args.kernel == "tiled" and args.remap == 1
+    plan = FusionPlan(n, gates, kernel=args.kernel, remap=remap)
+    plan.remap = remap
     nb = plan.num_launches()
     nblocks = plan.num_blocks()
     path = args.path
@@ -342,7 +356,7 @@ def run_b200(args):
     if rank == 0 and n >= 30:
         nf = 30
         gf = workload(nf, depth)
-        pf = FusionPlan(nf, gf, kernel=args.kernel)
+        pf = FusionPlan(nf, gf, kernel=args.kernel, remap=remap)
         a = StateVector(nf, "c64")
         pf.apply(a)
         pf.status(a)
@@ -378,6 +392,7 @@ def run_b200(args):
             check(L.qs_plan_default_opts(C.byref(o)))
             if args.kernel == "single":
                 o.kernel, o.max_sub = 1, 1
+            o.remap = 1 if remap else 0
             check(L.qs_plan_create_ex(n, C.c_void_p(pin_g.data_ptr()), ng, C.byref(o), C.byref(ph)))
             check(L.qs_plan_apply(h, ph))
         else:
@@ -407,6 +422,7 @@ def run_b200(args):
             "data": "synthetic",
             "config": {"workload": f"random-circuit-{n}q-depth{depth}-c64", "qubits": n, "depth": depth,
                        "gates": ng, "fused_blocks": nblocks, "fused_passes": nb, "kernel": args.kernel,
+                       "remap": remap, "device_bytes": (amp_b << n) * (2 if remap and path == "fused" else 1),
                        "iswap_frac": ISWAP_FRAC, "seed": SEED, "path": path,
                        "state_bytes": amp_b << n, "l2": "inputs larger than L2 (32 GiB state), no flush",
                        "parallelism": f"replicas x{ws}"},

@@ -217,10 +217,16 @@ typedef struct qs_plan_opts {
     int max_sub;           /* tiled passes: blocks per pass, 1..3 */
     int low_qubits;        /* tiled passes: qubits 0..low_qubits-1 always in the tile (1..5) */
     int kernel;            /* QS_PLAN_SINGLE or QS_PLAN_TILED */
+    int remap;             /* tiled passes of states of >= 20 qubits: 0 = in place (default); 1 = every
+                              pass but the last writes its tiles as contiguous runs into a second
+                              state-size buffer (held by the state from its first such plan until
+                              qs_destroy or qs_release_spare) and the last writes the natural order
+                              back; 2 = as 1, but each pass writes the layout in which the next pass's
+                              tiles are contiguous (loads stream, stores scatter; measured slower) */
 } qs_plan_opts;
 /* Defaults: 5-qubit blocks, tiled passes of 12 qubits with up to 2 blocks
  * (a pass of 3 blocks saves a pass but runs on a kernel with fewer resident
- * CTAs, and measured slower overall), qubits 0..2 in every tile. */
+ * CTAs, and measured slower overall), qubits 0..2 in every tile, in place. */
 int qs_plan_default_opts(qs_plan_opts *opts);
 int qs_plan_create_ex(int n_qubits, const qs_gate *gates, size_t count, const qs_plan_opts *opts,
                       qs_plan **out);
@@ -245,6 +251,9 @@ int qs_plan_apply_range(qs_state *s, qs_plan *plan, size_t first, size_t count);
 /* Synchronize and report whether a bounded wait inside a fused pass expired
  * since the last qs_plan_apply (QS_ERR_STATE) - a watchdog, not expected. */
 int qs_plan_status(qs_state *s);
+/* Free the second state-size buffer that plans with remap = 1 keep with the
+ * state (no-op when there is none).  No reference counterpart. */
+int qs_release_spare(qs_state *s);
 
 /* ---- batched circuits: many circuits in one persistent launch ---------- */
 /* The reference runs one program per QPandaSDK::run (QPandaAPI.cpp:131-211); a

@@ -106,6 +106,7 @@ def lib():
         "qs_diff": (i, [vp, vp, dp, dp]),
         "qs_measure_noalloc": (i, [vp, i, i, i, d, vp, vp, vp]),
         "qs_plan_status": (i, [vp]),
+        "qs_release_spare": (i, [vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -146,6 +147,10 @@ class StateVector:
         if self._h:
             lib().qs_destroy(self._h)
             self._h = None
+
+    def release_spare(self):
+        """Free the second buffer that remapping plans keep with the state."""
+        check(lib().qs_release_spare(self._h))
 
     def __del__(self):
         try:
@@ -257,7 +262,7 @@ class StateVector:
 
 class PlanOpts(C.Structure):
     _fields_ = [("block_qubits", C.c_int), ("tile_qubits", C.c_int), ("max_sub", C.c_int),
-                ("low_qubits", C.c_int), ("kernel", C.c_int)]
+                ("low_qubits", C.c_int), ("kernel", C.c_int), ("remap", C.c_int)]
 
 
 PLAN_SINGLE, PLAN_TILED = 1, 2
@@ -266,9 +271,12 @@ PLAN_SINGLE, PLAN_TILED = 1, 2
 class FusionPlan:
     """Gate list fused into dense 5-qubit blocks (qs_plan_*).  kernel="tiled"
     (default) applies up to max_sub blocks per pass over the state;
-    kernel="single" one block per pass."""
+    kernel="single" one block per pass.  remap=1: tiled passes write their
+    tiles as contiguous runs into a second state-size buffer kept with the
+    state (twice the memory; faster passes on large states); remap=2: the
+    next pass's tiles contiguous instead (qs_plan_opts.remap)."""
 
-    def __init__(self, n, gates, max_k=5, kernel="tiled", max_sub=2, low_qubits=3):
+    def __init__(self, n, gates, max_k=5, kernel="tiled", max_sub=2, low_qubits=3, remap=False):
         g = np.ascontiguousarray(gates, dtype=GATE_DTYPE)
         self._keep = g
         h = C.c_void_p()
@@ -278,6 +286,7 @@ class FusionPlan:
             o = PlanOpts()
             check(lib().qs_plan_default_opts(C.byref(o)))
             o.block_qubits, o.max_sub, o.low_qubits = int(max_k), int(max_sub), int(low_qubits)
+            o.remap = int(remap)
             check(lib().qs_plan_create_ex(int(n), g.ctypes.data, g.size, C.byref(o), C.byref(h)))
         self._h = h
         self.n = int(n)

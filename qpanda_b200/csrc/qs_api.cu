@@ -137,6 +137,7 @@ extern "C" int qs_destroy(qs_state *s)
         qs_dev_free(s, s->amp);
         qs_dev_free(s, s->scratch);
         qs_dev_free(s, s->fused_norm);
+        qs_dev_free(s, s->spare);
         free(s->pinned);
     } else {
         cudaStreamSynchronize(s->stream);
@@ -144,6 +145,7 @@ extern "C" int qs_destroy(qs_state *s)
         if (s->scratch) cudaFree(s->scratch);
         if (s->pinned) cudaFreeHost(s->pinned);
         if (s->fused_norm) cudaFree(s->fused_norm);
+        if (s->spare) cudaFree(s->spare);
     }
     s->amp = nullptr;
     delete s;

@@ -52,6 +52,8 @@ struct qs_state {
     void *pinned = nullptr;
     // Norm partials of fused passes (3 x fused grid doubles), on first use.
     double *fused_norm = nullptr;
+    // Second state-size buffer of remapping plans (qs_plan_opts.remap), on first use.
+    void *spare = nullptr;
     // Stream-ordered memory (qs_create_async): cudaMallocAsync / cudaFreeAsync
     // on `stream`, and an ordinary host buffer instead of pinned memory.
     bool stream_alloc = false;

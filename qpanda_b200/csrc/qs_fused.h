@@ -23,9 +23,9 @@ int qs_fused_grid(const qs_state *s);
 // err_dev: device int set to 1 if a bounded wait inside the kernel expired.
 int qs_launch_fused(qs_state *s, const qs_fused_desc *d, int *err_dev);
 
-// One tiled pass: 12 tile qubits T (ascending) and nsub (1..3) blocks, each
-// on 5 of them (ascending), applied in order; mat_dev holds the blocks'
-// BF16 [2][64][64] matrices back to back.
+// One tiled pass: 12 tile positions T (ascending) and nsub (1..3) blocks,
+// each on 5 of them (in the column-bit order of its matrix), applied in
+// order; mat_dev holds the blocks' BF16 [2][64][64] matrices back to back.
 struct qs_tiled_desc {
     int T[12];
     int nsub;
@@ -37,6 +37,20 @@ struct qs_tiled_desc {
     const double *prev_out;
     double *in_parts;
     double *out_parts;
+    // Where the results go (qs_tile::StoreMap): with has_write, tile bit l
+    // (l-th of T) is written at position wtile[l] and tile index bit i at
+    // wpos[i] (wmode 2) or 12 + i (wmode 1); otherwise in place.
+    int has_write;
+    int wtile[12];
+    int wmode;
+    int wpos[52];
+    // Results go to amp_in -> amp_out (device, state-size, distinct) when
+    // both are set; in place in the state's buffer otherwise.  Passes with
+    // has_write need distinct buffers: a tile's results land where other
+    // tiles are still to be read.
+    const void *amp_in;
+    void *amp_out;
+    size_t first_block;          // the plan's index of block 0 of the pass (host bookkeeping)
 };
 
 int qs_tiled_grid(const qs_state *s);

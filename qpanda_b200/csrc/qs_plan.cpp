@@ -277,6 +277,7 @@ extern "C" int qs_plan_create(int n, const qs_gate *gates, size_t count, int max
     o.max_sub = 1;
     o.low_qubits = 0;
     o.kernel = QS_PLAN_SINGLE;
+    o.remap = 0;
     return qs_plan_create_ex(n, gates, count, &o, out);
 }
 
@@ -288,6 +289,7 @@ extern "C" int qs_plan_default_opts(qs_plan_opts *o)
     o->max_sub = 2;              // passes of <= 2 blocks run three CTAs per SM (qs_fused2.cu)
     o->low_qubits = 3;
     o->kernel = QS_PLAN_TILED;
+    o->remap = 0;
     return QS_OK;
 }
 
@@ -309,6 +311,7 @@ extern "C" int qs_plan_create_ex(int n, const qs_gate *gates, size_t count, cons
         (o.tile_qubits != 12 || o.max_sub < 1 || o.max_sub > 3 || o.low_qubits < 1 || o.low_qubits > 5))
         return qs_fail(QS_ERR_UNSUPPORTED,
                        "qs_plan_create: tiled passes need tile_qubits 12, max_sub 1..3, low_qubits 1..5");
+    if (o.remap < 0 || o.remap > 2) return qs_fail(QS_ERR_ARG, "qs_plan_create: remap must be 0, 1 or 2");
     if (count && !gates) return qs_fail(QS_ERR_ARG, "qs_plan_create: null gate list");
     qs_plan *P = new qs_plan();
     P->n = n;
@@ -420,6 +423,126 @@ extern "C" int qs_plan_apply(qs_state *s, qs_plan *P)
     return qs_plan_apply_range(s, P, 0, P ? plan_launches(P) : 0);
 }
 
+// Tiled pass u of a plan while its state is held with logical qubit q at
+// position pos[q].  Every pass but the last of an application writes its
+// tile as one contiguous run - the tile's qubits at positions 0..11, the
+// others at 12.. in their current order - so that its stores stream through
+// DRAM (stores scattered in short runs were the costlier half of a pass);
+// the tile qubits that the next pass also uses go lowest, so that its loads
+// come in runs of at least 2^low_qubits amplitudes.  The last pass writes the
+// natural order back.  Updates pos to the layout the pass leaves.
+static void tiled_pass_desc(const qs_plan *P, size_t u, bool last, int mode, std::vector<int> &pos,
+                            qs_tiled_desc &d)
+{
+    const PlanPass &pp = P->passes[u];
+    const int n = P->n;
+    std::vector<int> at(n);                 // at[p] = logical qubit at position p
+    for (int q = 0; q < n; ++q) at[pos[q]] = q;
+    int phys[12], tq[12];
+    uint64_t tmask = 0;
+    for (int i = 0; i < 12; ++i) { phys[i] = pos[pp.T[i]]; tmask |= 1ull << phys[i]; }
+    std::sort(phys, phys + 12);
+    for (int i = 0; i < 12; ++i) { d.T[i] = phys[i]; tq[i] = at[phys[i]]; }
+    d.nsub = (int)pp.count;
+    d.first_block = pp.first;
+    for (size_t b = 0; b < pp.count; ++b)
+        for (int j = 0; j < 5; ++j) d.qpos[b][j] = pos[P->blocks[pp.first + b].q[j]];
+    d.has_rows = 1;
+    for (size_t b = 0; b < pp.count; ++b)
+        for (int i = 0; i < 7; ++i) d.rows[b][i] = pos[pp.rows[b][i]];
+    bool ident = true;
+    for (int q = 0; q < n; ++q) ident = ident && pos[q] == q;
+    d.has_write = 0;
+    if (last && ident) return;              // natural in, natural out: in place
+    d.has_write = 1;
+    std::vector<int> npos(n);
+    if (last) {
+        for (int l = 0; l < 12; ++l) d.wtile[l] = tq[l];
+        for (int p = 0, i = 0; p < n; ++p)
+            if (!((tmask >> p) & 1)) d.wpos[i++] = at[p];
+        d.wmode = 2;
+        for (int q = 0; q < n; ++q) npos[q] = q;
+    } else if (mode == 2) {
+        // contiguous loads for the next pass: its tile qubits at 0..11 (those
+        // of this tile first, so that this pass's stores come in runs), every
+        // other qubit at 12.. in its current order
+        const PlanPass &nx = P->passes[u + 1];
+        uint64_t next = 0, here = 0;
+        for (int i = 0; i < 12; ++i) { next |= 1ull << nx.T[i]; here |= 1ull << tq[i]; }
+        std::vector<int> order;
+        const int c_next = P->blocks[nx.first].q[0];
+        order.push_back(c_next);                       // the next loads move column pairs
+        for (int i = 0; i < 12; ++i)
+            if (nx.T[i] != c_next && ((here >> nx.T[i]) & 1)) order.push_back(nx.T[i]);
+        for (int i = 0; i < 12; ++i)
+            if (nx.T[i] != c_next && !((here >> nx.T[i]) & 1)) order.push_back(nx.T[i]);
+        for (int k = 0; k < 12; ++k) npos[order[k]] = k;
+        for (int p = 0, k = 12; p < n; ++p)
+            if (!((next >> at[p]) & 1)) npos[at[p]] = k++;
+        for (int l = 0; l < 12; ++l) d.wtile[l] = npos[tq[l]];
+        for (int p = 0, i = 0; p < n; ++p)
+            if (!((tmask >> p) & 1)) d.wpos[i++] = npos[at[p]];
+        d.wmode = 2;
+    } else {
+        const PlanPass &nx = P->passes[u + 1];
+        uint64_t next = 0;
+        for (int i = 0; i < 12; ++i) next |= 1ull << nx.T[i];
+        // position 0: the next pass's block-0 first column qubit (its loads
+        // then move column pairs), else this pass's last-block first column
+        // qubit (its stores then move column pairs), if shared
+        const int c_next = P->blocks[nx.first].q[0];
+        const int c_last = P->blocks[pp.first + pp.count - 1].q[0];
+        auto in_tile = [&](int q) { return ((tmask >> pos[q]) & 1) != 0; };
+        int head = -1;
+        if (in_tile(c_next) && ((next >> c_next) & 1)) head = c_next;
+        else if (in_tile(c_last) && ((next >> c_last) & 1)) head = c_last;
+        std::vector<int> order;
+        if (head >= 0) order.push_back(head);
+        for (int l = 0; l < 12; ++l)
+            if (tq[l] != head && ((next >> tq[l]) & 1)) order.push_back(tq[l]);
+        for (int l = 0; l < 12; ++l)
+            if (!((next >> tq[l]) & 1)) order.push_back(tq[l]);
+        for (int k = 0; k < 12; ++k) npos[order[k]] = k;
+        for (int l = 0; l < 12; ++l) d.wtile[l] = npos[tq[l]];
+        for (int p = 0, i = 0; p < n; ++p)
+            if (!((tmask >> p) & 1)) { npos[at[p]] = 12 + i; d.wpos[i] = 12 + i; ++i; }
+        d.wmode = 1;
+    }
+    pos.swap(npos);
+}
+
+int qs_plan_tiled_schedule(const qs_plan *P, int n, size_t first, size_t count, int remap,
+                           std::vector<qs_tiled_desc> &descs, std::vector<int> &dst)
+{
+    if (P->opts.kernel != QS_PLAN_TILED || n != P->n || first > P->passes.size() ||
+        count > P->passes.size() - first)
+        return qs_fail(QS_ERR_ARG, "tiled schedule: bad plan or range");
+    descs.assign(count, qs_tiled_desc());
+    dst.assign(count, 0);
+    std::vector<int> pos(n);
+    for (int q = 0; q < n; ++q) pos[q] = q;
+    // Remapping ping-pongs between the state's buffer (0) and the spare one
+    // (1); with an odd number of passes the first runs in place, so that the
+    // last pass lands in the state's own buffer.
+    if (count < 2) remap = 0;
+    const size_t pong_from = remap ? (count & 1) : count;
+    int cur = 0;
+    for (size_t k = 0; k < count; ++k) {
+        qs_tiled_desc &d = descs[k];
+        memset(&d, 0, sizeof(d));
+        if (k < pong_from) {
+            std::vector<int> ident(pos);
+            tiled_pass_desc(P, first + k, true, 0, ident, d);  // natural in, natural out, in place
+            dst[k] = -1;
+        } else {
+            tiled_pass_desc(P, first + k, k + 1 == count, remap, pos, d);
+            dst[k] = cur ^ 1;
+            cur ^= 1;
+        }
+    }
+    return QS_OK;
+}
+
 extern "C" int qs_plan_apply_range(qs_state *s, qs_plan *P, size_t first, size_t count)
 {
     int r = qs_check_state(s);
@@ -470,16 +593,23 @@ extern "C" int qs_plan_apply_range(qs_state *s, qs_plan *P, size_t first, size_t
     const size_t per = 2 * 64 * 64 * sizeof(uint16_t);
     if (P->opts.kernel == QS_PLAN_TILED) {
         const int GT = qs_tiled_grid(s);
+        const int remap = (count >= 2 && s->n >= 20) ? P->opts.remap : 0;
+        if (remap && !s->spare) {
+            void *p = nullptr;
+            if ((r = qs_dev_alloc(s, s->amp_bytes(), &p))) return r;
+            s->spare = p;
+        }
+        std::vector<qs_tiled_desc> descs;
+        std::vector<int> dst;
+        if ((r = qs_plan_tiled_schedule(P, s->n, first, count, remap, descs, dst))) return r;
+        void *buf[2] = {s->amp, s->spare};
         for (size_t u = first; u < first + count; ++u) {
             const PlanPass &pp = P->passes[u];
-            qs_tiled_desc d;
-            memset(&d, 0, sizeof(d));
-            for (int i = 0; i < 12; ++i) d.T[i] = pp.T[i];
-            d.nsub = (int)pp.count;
-            for (size_t b = 0; b < pp.count; ++b)
-                for (int j = 0; j < 5; ++j) d.qpos[b][j] = P->blocks[pp.first + b].q[j];
-            d.has_rows = 1;
-            memcpy(d.rows, pp.rows, sizeof(d.rows));
+            qs_tiled_desc &d = descs[u - first];
+            if (dst[u - first] >= 0) {
+                d.amp_out = buf[dst[u - first]];
+                d.amp_in = buf[dst[u - first] ^ 1];
+            }
             d.mat_dev = static_cast<const char *>(P->mats) + pp.first * per;
             d.norm0 = u ? norm : nullptr;
             d.prev_out = u ? norm + GT * (1 + (u - 1) % 2) : nullptr;
@@ -498,6 +628,22 @@ extern "C" int qs_plan_apply_range(qs_state *s, qs_plan *P, size_t first, size_t
         d.in_parts = b ? nullptr : norm;
         d.out_parts = norm + G * (1 + b % 2);
         if ((r = qs_launch_fused(s, &d, flag))) return r;
+    }
+    return QS_OK;
+}
+
+extern "C" int qs_release_spare(qs_state *s)
+{
+    int r = qs_check_state(s);
+    if (r) return r;
+    if (s->spare) {
+        if (s->stream_alloc) {
+            qs_dev_free(s, s->spare);
+        } else {
+            QS_CUDA_TRY(cudaStreamSynchronize(s->stream));
+            QS_CUDA_TRY(cudaFree(s->spare));
+        }
+        s->spare = nullptr;
     }
     return QS_OK;
 }

@@ -46,3 +46,15 @@ struct qs_plan {
 int qs_plan_rebind(const qs_plan *proto, const qs_gate *gates, size_t count, qs_plan **out);
 // 2 x 64 x 64 BF16 bits (hi, lo) of block b's real matrix form.
 void qs_plan_block_bf16(const qs_plan *P, size_t b, uint16_t *out);
+
+struct qs_tiled_desc;
+// Launch descriptors of tiled passes [first, first + count) of P on an
+// n-qubit state (buffers and norm pointers left empty), and for each pass
+// the buffer it writes: -1 in place, 0 the state's own, 1 the spare (reading
+// the other).  With remap (qs_plan_opts.remap), passes ping-pong through the
+// spare buffer, each writing the layout that makes its own stores (1) or the
+// next pass's loads (2) contiguous tiles, and the last writes the natural
+// order; the state's own buffer holds the result.  Pure host code (also used by the CPU
+// emulation test of the tiled passes).
+int qs_plan_tiled_schedule(const qs_plan *P, int n, size_t first, size_t count, int remap,
+                           std::vector<qs_tiled_desc> &descs, std::vector<int> &dst);

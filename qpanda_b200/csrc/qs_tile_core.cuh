@@ -47,6 +47,19 @@ struct Layout {
     uint8_t tabJ[kMaxSub - 1][32];   // column j of block b -> column bits of block b+1
 };
 
+// Warp-contiguous copies of block 0's input (prefetch_tile): chunk c of a
+// tile holds tile indices 2c, 2c+1, with c = 128 k + thread.  Built on the
+// host beside the Layout (qs_tile_layout_build).
+struct LoadMap {
+    uint64_t gk[16];             // tile index bits 8..11 = k: global offset
+    uint8_t rk[16];              //   ... block-0 row bits
+    uint8_t jk[16];              //   ... block-0 column bits
+    int8_t tpos[12];             // global position of tile bit t
+    int8_t tmap0[12];            // tile bit t in block 0: row bit (>= 0) or ~column bit
+    int8_t rb0;                  // row bit of tile bit 0 in block 0, or -1 when it is column bit 0
+    int8_t pad[7];
+};
+
 // Thread part of the scatter offset (see Layout::scat).
 __device__ __forceinline__ uint32_t scatter_thread_part(const Layout &L, int t, int row)
 {
@@ -190,6 +203,85 @@ __device__ __forceinline__ void prefetch_row(const float *amp, uint64_t base, co
     asm volatile("cp.async.commit_group;" ::: "memory");
 }
 
+// Per-thread part of prefetch_tile's addresses: tile index bits 1..7 = the
+// thread's index within its 128.
+struct ChunkBase {
+    uint64_t g;
+    uint32_t r, j;
+};
+
+__device__ __forceinline__ ChunkBase chunk_base(const LoadMap &L, int t128)
+{
+    ChunkBase c{0, 0, 0};
+#pragma unroll
+    for (int t = 1; t < 8; ++t) {
+        if (!((t128 >> (t - 1)) & 1)) continue;
+        c.g |= 1ull << L.tpos[t];
+        const int m = L.tmap0[t];
+        if (m >= 0) c.r |= 1u << m;
+        else c.j |= 1u << (~m);
+    }
+    return c;
+}
+
+// Asynchronous copies of a whole tile of block 0's input into the staging
+// rows (same layout as prefetch_row), by 128 threads together: the 32 lanes
+// of a warp copy 32 consecutive 16-byte chunks of the tile, so every copy
+// instruction reads whole runs of contiguous memory and its data lands in
+// shared memory in a few wavefronts.  The staging rows are shared by the 128
+// threads: a barrier must separate the copies' completion from the reads, and
+// the reads from the next tile's copies.
+__device__ __forceinline__ void prefetch_tile(const float *amp, uint64_t base, const LoadMap &L, uint32_t stage,
+                                              const ChunkBase &cb)
+{
+    if (L.rb0 < 0) {
+        // tile bit 0 is block 0's column bit 0: a chunk is a column pair of one row
+#pragma unroll
+        for (int k = 0; k < 16; ++k) {
+            const float *src = amp + 2 * (base | cb.g | L.gk[k]);
+            const uint32_t row = cb.r ^ L.rk[k], jp = (cb.j ^ L.jk[k]) >> 1;
+            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" :: "r"(stage_addr(stage, row, jp)),
+                         "l"(src) : "memory");
+        }
+    } else {
+        // tile bit 0 is a row bit: a chunk is one column of two rows
+        const uint32_t rbm = 1u << L.rb0;
+#pragma unroll
+        for (int k = 0; k < 16; ++k) {
+            const float *src = amp + 2 * (base | cb.g | L.gk[k]);
+            const uint32_t row = cb.r ^ L.rk[k], j = cb.j ^ L.jk[k];
+            const uint32_t half = (j & 1) << 3;
+            asm volatile("cp.async.ca.shared.global [%0], [%1], 8;"
+                         :: "r"(stage_addr(stage, row, j >> 1) + half), "l"(src) : "memory");
+            asm volatile("cp.async.ca.shared.global [%0], [%1], 8;"
+                         :: "r"(stage_addr(stage, row | rbm, j >> 1) + half), "l"(src + 2) : "memory");
+        }
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+}
+
+// Where a pass writes a tile's results (k_fused_tile).  The 12 tile bits go
+// to the positions in the Layout's gl / cl_glob; the tile index bits (the
+// other n - 12 positions, ascending as read) go to
+//   mode 0: the positions they were read from (the pass writes in place);
+//   mode 1: positions 12, 13, ... (a tile's results are one contiguous run);
+//   mode 2: wpos[i] for tile index bit i.
+struct StoreMap {
+    int32_t mode;
+    int32_t ntb;                 // tile index bits (n - 12)
+    int8_t wpos[52];
+};
+
+// Global offset of a tile's results (see StoreMap).
+__device__ __forceinline__ uint64_t store_base(uint64_t tile, uint64_t read_base, const StoreMap &W)
+{
+    if (W.mode == 0) return read_base;
+    if (W.mode == 1) return tile << 12;
+    uint64_t b = 0;
+    for (int i = 0; i < W.ntb; ++i) b |= ((tile >> i) & 1ull) << W.wpos[i];
+    return b;
+}
+
 __device__ __forceinline__ void read_stage_row(uint32_t stage, int row, float (&x)[64])
 {
 #pragma unroll
@@ -260,5 +352,10 @@ __device__ __forceinline__ void load_b(uint8_t *dst, const uint16_t *mat, int ns
 
 // Host: the Layout of a pass with tile qubits T[12] (ascending, global) and
 // nsub blocks on qpos[b][5] (ascending, within T).  QS_OK or QS_ERR_ARG.
+// T: the 12 tile positions, ascending; qpos[b]: block b's 5 positions in
+// column-bit order (distinct tile positions); rows[b]: its other 7 in row-bit
+// order (NULL: ascending).  With M non-null, also the LoadMap of
+// prefetch_tile.  With wtile non-null, results are written with tile bit l at
+// position wtile[l] instead of T[l] (the last block's gl and cl_glob).
 int qs_tile_layout_build(int n, const int *T, int nsub, const int (*qpos)[5], const int (*rows)[7],
-                         qs_tile::Layout *L);
+                         qs_tile::Layout *L, qs_tile::LoadMap *M = nullptr, const int *wtile = nullptr);

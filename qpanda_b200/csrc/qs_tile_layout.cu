@@ -140,7 +140,7 @@ int qs_tile_row_orders(int n, const int *T, int nsub, const int (*qpos)[5], int 
 }
 
 int qs_tile_layout_build(int n, const int *T, int nsub, const int (*qpos)[5], const int (*rows)[7],
-                         qs_tile::Layout *L)
+                         qs_tile::Layout *L, qs_tile::LoadMap *M, const int *wtile)
 {
     using qs_tile::kMaxSub;
     if (nsub < 1 || nsub > kMaxSub) return qs_fail(QS_ERR_ARG, "tiled pass: %d blocks", nsub);
@@ -159,8 +159,8 @@ int qs_tile_layout_build(int n, const int *T, int nsub, const int (*qpos)[5], co
         uint32_t qm = 0;
         for (int i = 0; i < 5; ++i) {
             const int q = qpos[b][i];
-            if (q < 0 || q >= n || local[q] < 0 || (i && q <= qpos[b][i - 1]))
-                return qs_fail(QS_ERR_ARG, "tiled pass: block qubits must be ascending tile qubits");
+            if (q < 0 || q >= n || local[q] < 0 || (qm & (1u << local[q])))
+                return qs_fail(QS_ERR_ARG, "tiled pass: block qubits must be distinct tile qubits");
             Q[b][i] = local[q];
             qm |= 1u << local[q];
         }
@@ -177,12 +177,20 @@ int qs_tile_layout_build(int n, const int *T, int nsub, const int (*qpos)[5], co
             }
         }
     }
+    int WT[12];                                  // write position of each tile bit
+    uint64_t wseen = 0;
+    for (int i = 0; i < 12; ++i) {
+        WT[i] = wtile ? wtile[i] : T[i];
+        if (WT[i] < 0 || WT[i] >= n || ((wseen >> WT[i]) & 1))
+            return qs_fail(QS_ERR_ARG, "tiled pass: write positions must be distinct and in range");
+        wseen |= 1ull << WT[i];
+    }
     L->nsub = nsub;
     const int last = nsub - 1;
     for (int i = 0; i < 12; ++i) L->tpos[i] = (int8_t)T[i];
     for (int i = 0; i < 7; ++i) {
         L->c0_glob[i] = T[Cp[0][i]];
-        L->cl_glob[i] = T[Cp[last][i]];
+        L->cl_glob[i] = WT[Cp[last][i]];
         L->cl_loc[i] = (int8_t)Cp[last][i];
     }
     for (int j = 0; j < 32; ++j) {
@@ -194,12 +202,34 @@ int qs_tile_layout_build(int n, const int *T, int nsub, const int (*qpos)[5], co
     for (int j = 0; j < 32; ++j) {
         uint64_t a = 0, b = 0;
         for (int i = 0; i < 5; ++i)
-            if (j & (1 << i)) { a |= 1ull << T[Q[0][i]]; b |= 1ull << T[Q[last][i]]; }
+            if (j & (1 << i)) { a |= 1ull << T[Q[0][i]]; b |= 1ull << WT[Q[last][i]]; }
         L->g0[j] = a;
         L->gl[j] = b;
     }
     L->vec0 = T[Q[0][0]] == 0;
-    L->vecl = T[Q[last][0]] == 0;
+    L->vecl = WT[Q[last][0]] == 0;
+    if (M) {
+        // block 0's view of each tile bit, and the tables of prefetch_tile
+        memset(M, 0, sizeof(*M));
+        for (int p = 0; p < 12; ++p) M->tpos[p] = (int8_t)T[p];
+        for (int i = 0; i < 7; ++i) M->tmap0[Cp[0][i]] = (int8_t)i;
+        for (int i = 0; i < 5; ++i) M->tmap0[Q[0][i]] = (int8_t)~i;
+        M->rb0 = (int8_t)(M->tmap0[0] >= 0 ? M->tmap0[0] : -1);
+        for (int k = 0; k < 16; ++k) {
+            uint64_t g = 0;
+            uint32_t rr = 0, jj = 0;
+            for (int t = 8; t < 12; ++t) {
+                if (!((k >> (t - 8)) & 1)) continue;
+                g |= 1ull << T[t];
+                const int m = M->tmap0[t];
+                if (m >= 0) rr |= 1u << m;
+                else jj |= 1u << (~m);
+            }
+            M->gk[k] = g;
+            M->rk[k] = (uint8_t)rr;
+            M->jk[k] = (uint8_t)jj;
+        }
+    }
     for (int t = 0; t + 1 < nsub; ++t) {
         int rowbit[12], colbit[12];
         for (int p = 0; p < 12; ++p) rowbit[p] = colbit[p] = -1;

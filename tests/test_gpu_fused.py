@@ -22,13 +22,13 @@ def random_state(n, seed):
 KERNELS = ["single", "tiled"]
 
 
-def check_fused(n, g, init=None, kernel="tiled"):
+def check_fused(n, g, init=None, kernel="tiled", **kw):
     sv = StateVector(n, "c64")
     o = OracleState(n)
     if init is not None:
         sv.set_state(init.astype(np.complex64))
         o.set_state(init.astype(np.complex64).astype(np.complex128))
-    p = FusionPlan(n, g, kernel=kernel)
+    p = FusionPlan(n, g, kernel=kernel, **kw)
     p.apply(sv)
     p.status(sv)
     o.apply(g)
@@ -101,14 +101,39 @@ def test_fused_vqe_and_reuse(need_gpu, kernel):
     assert np.abs(a.get_state() - o.state()).max() < AMP_TOL
 
 
-@pytest.mark.parametrize("kernel", KERNELS)
-def test_fused_fidelity_26q_vs_fp64_gpu(need_gpu, kernel):
+@pytest.mark.parametrize("remap", [1, 2])
+@pytest.mark.parametrize("max_sub", [1, 2, 3])
+@pytest.mark.parametrize("n", [20, 21])
+def test_tiled_remap(need_gpu, n, max_sub, remap):
+    """Remapped passes (ping-pong through a second buffer, contiguous tile
+    writes, natural order back at the end) at an even and an odd count of
+    passes; a second application reuses the spare buffer, and releasing it
+    leaves the state intact."""
+    g = circuits.random_layers(n, 6, 90 + n + max_sub, iswap_frac=0.2)
+    init = random_state(n, n + max_sub)
+    check_fused(n, g, init=init, kernel="tiled", max_sub=max_sub, remap=remap)
+    sv = StateVector(n, "c64")
+    sv.set_state(init.astype(np.complex64))
+    p = FusionPlan(n, g, max_sub=max_sub, remap=remap)
+    p.apply(sv)
+    p.apply(sv)
+    p.status(sv)
+    o = OracleState(n)
+    o.set_state(init.astype(np.complex64).astype(np.complex128))
+    o.apply(g)
+    o.apply(g)
+    sv.release_spare()
+    assert np.abs(sv.get_state() - o.state()).max() < AMP_TOL
+
+
+@pytest.mark.parametrize("kernel,remap", [("single", 0), ("tiled", 0), ("tiled", 1), ("tiled", 2)])
+def test_fused_fidelity_26q_vs_fp64_gpu(need_gpu, kernel, remap):
     """26 qubits, 12 layers: fused complex64 against the complex128 per-gate
     path (itself pinned to the oracle by the other tests)."""
     n = 26
     g = circuits.random_layers(n, 12, 7, iswap_frac=0.1)
     f = StateVector(n, "c64")
-    p = FusionPlan(n, g, kernel=kernel)
+    p = FusionPlan(n, g, kernel=kernel, remap=remap)
     p.apply(f)
     p.status(f)
     d = StateVector(n, "c128")

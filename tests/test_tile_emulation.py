@@ -1,0 +1,89 @@
+"""CPU check of the tiled passes' index arithmetic (no GPU).
+
+tests/tile_emu/tile_emu.cpp replays a fused plan on the host exactly as
+k_fused_tile moves data - the library's own pass scheduler and layout tables,
+the warp-contiguous staging copies, the swizzled scatter between blocks, the
+in-place or remapped (ping-pong, contiguous tile writes) stores - with FP64
+block contractions in place of the tensor cores.  The result must match the
+FP64 oracle to rounding, and every staging slot, A slot and output amplitude
+must be written exactly once.
+"""
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from oracle.pyoracle import OracleState
+from qpanda_b200 import FusionPlan, circuits
+from qpanda_b200.capi import lib
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+CSRC = os.path.join(ROOT, "qpanda_b200", "csrc")
+LIBDIR = os.path.join(ROOT, "qpanda_b200", "_lib")
+SRC = os.path.join(ROOT, "tests", "tile_emu", "tile_emu.cpp")
+
+
+@pytest.fixture(scope="module")
+def emu(tmp_path_factory):
+    lib()                                     # the library must be built
+    out = str(tmp_path_factory.mktemp("tile_emu") / "libtile_emu.so")
+    cmd = ["/usr/local/cuda/bin/nvcc", "-O2", "-std=c++17", "-x", "cu", "-shared", "-Xcompiler", "-fPIC",
+           "-gencode", "arch=compute_100a,code=sm_100a", SRC, "-I" + CSRC, "-I" + os.path.join(ROOT, "include"),
+           "-L" + LIBDIR, "-lqsb200", "-Xlinker", "-rpath=" + LIBDIR, "-o", out]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    assert r.returncode == 0, r.stdout + r.stderr
+    E = C.CDLL(out)
+    E.tile_emu_apply.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.POINTER(C.c_int)]
+    E.tile_emu_apply.restype = C.c_int
+    E.tile_emu_error.restype = C.c_char_p
+    return E
+
+
+def random_state(n, seed):
+    rng = np.random.default_rng(seed)
+    v = rng.normal(size=1 << n) + 1j * rng.normal(size=1 << n)
+    return v / np.linalg.norm(v)
+
+
+def run_emu(E, n, g, init, remap, **kw):
+    p = FusionPlan(n, g, remap=remap, **kw)
+    st = np.ascontiguousarray(init.astype(np.complex128))
+    npass = C.c_int()
+    rc = E.tile_emu_apply(p.handle, n, st.ctypes.data, int(remap), C.byref(npass))
+    assert rc == 0, E.tile_emu_error().decode()
+    o = OracleState(n)
+    o.set_state(init)
+    o.apply(g)
+    err = np.abs(st - o.state()).max()
+    p.close()
+    return err, npass.value
+
+
+@pytest.mark.parametrize("remap", [0, 1, 2])
+@pytest.mark.parametrize("max_sub,low", [(1, 3), (2, 3), (3, 3), (2, 1), (2, 5), (3, 4)])
+def test_tiled_index_math_random_layers(emu, remap, max_sub, low):
+    n = 16
+    g = circuits.random_layers(n, 6, 300 + 10 * max_sub + low, iswap_frac=0.2)
+    err, npass = run_emu(emu, n, g, random_state(n, 1), remap, max_sub=max_sub, low_qubits=low)
+    assert npass >= 2
+    assert err < 1e-10, err
+
+
+@pytest.mark.parametrize("remap", [0, 1, 2])
+@pytest.mark.parametrize("n", [12, 13, 17])
+def test_tiled_index_math_sizes(emu, remap, n):
+    """One tile (12 qubits), two tiles, and an odd count of passes."""
+    g = circuits.random_layers(n, 5, 40 + n, iswap_frac=0.1)
+    err, _ = run_emu(emu, n, g, random_state(n, n), remap)
+    assert err < 1e-10, err
+
+
+@pytest.mark.parametrize("remap", [0, 1, 2])
+def test_tiled_index_math_qft_and_ansatz(emu, remap):
+    n = 15
+    err, _ = run_emu(emu, n, circuits.qft(n), random_state(n, 2), remap)
+    assert err < 1e-10, err
+    err, _ = run_emu(emu, n, circuits.vqe_ansatz(n, 3, seed=4), random_state(n, 3), remap)
+    assert err < 1e-10, err

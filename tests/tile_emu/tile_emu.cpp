@@ -1,0 +1,224 @@
+// tile_emu.cpp - CPU emulation of the tiled tensor-core passes, for tests.
+//
+// Runs a fused plan on a complex128 host state exactly the way k_fused_tile
+// (qpanda_b200/csrc/qs_fused2.cu) moves data: the launch descriptors come
+// from the library's own scheduler (qs_plan_tiled_schedule), the per-pass
+// tables from its own layout builder (qs_tile_layout_build), and each tile
+// goes through
+//   * the warp-contiguous staging copies of prefetch_tile (LoadMap) into the
+//     swizzled staging rows, read back row by row as read_stage_row does;
+//   * each block's contraction (in FP64 here, on the block unitaries of the
+//     plan, instead of split BF16 on the tensor cores);
+//   * the scatter of a block's results into the next block's swizzled A
+//     buffer by the kernel's XOR offsets (scatter_thread_part ^ scat), decoded
+//     back to (row, column);
+//   * the stores of the last block's results through StoreMap / gl / cl_glob,
+//     in place or into the other buffer of the ping-pong.
+// Every staging slot and every A slot must be written exactly once per tile
+// and every output amplitude exactly once per pass; the result is compared
+// with the oracle by the caller.  This checks all index arithmetic of the
+// tiled path on the CPU; the GPU tests check the tensor-core arithmetic.
+//
+// Built by tests/test_tile_emulation.py against the library (host code only
+// runs; nvcc because the shared headers hold device helpers):
+//   nvcc -O2 -std=c++17 -x cu -shared -Xcompiler -fPIC tile_emu.cpp
+//        -I<csrc> -I<include> -L<lib> -lqsb200
+#include <complex>
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+#include "qs_fused.h"
+#include "qs_plan_internal.h"
+#include "qs_tile_core.cuh"
+
+using qs_tile::Layout;
+using qs_tile::LoadMap;
+using qs_tile::StoreMap;
+typedef std::complex<double> cd;
+
+namespace {
+
+char g_err[256];
+
+uint64_t deposit_tile(uint64_t tile, const Layout &L)
+{
+    for (int j = 0; j < 12; ++j) {
+        const uint64_t low = (1ull << L.tpos[j]) - 1;
+        tile = ((tile & ~low) << 1) | (tile & low);
+    }
+    return tile;
+}
+
+uint32_t stage_off(int row, int chunk) { return row * 256 + ((chunk ^ (row & 15)) << 4); }
+
+// same formula as qs_tile::scatter_thread_part
+uint32_t emu_thread_part(const Layout &L, int t, int row)
+{
+    uint32_t r2 = 0, j2 = 0;
+    for (int b = 0; b < 7; ++b) {
+        const uint32_t bit = (row >> b) & 1;
+        const int m = L.rowmap[t][b];
+        if (m >= 0) r2 |= bit << m;
+        else j2 |= bit << (~m);
+    }
+    return (r2 << 7) | ((((j2 >> 2) ^ (r2 & 7)) & 7) << 4) | ((j2 & 3) << 2);
+}
+
+// same formula as qs_tile::store_base
+uint64_t emu_store_base(uint64_t tile, uint64_t read_base, const StoreMap &W)
+{
+    if (W.mode == 0) return read_base;
+    if (W.mode == 1) return tile << 12;
+    uint64_t b = 0;
+    for (int i = 0; i < W.ntb; ++i) b |= ((tile >> i) & 1ull) << W.wpos[i];
+    return b;
+}
+
+int fail(const char *msg, long long a = 0, long long b = 0)
+{
+    snprintf(g_err, sizeof(g_err), "%s (%lld, %lld)", msg, a, b);
+    return 1;
+}
+
+}  // namespace
+
+extern "C" const char *tile_emu_error(void) { return g_err; }
+
+// Apply plan passes [0, all) to state (2^n complex128, interleaved re/im).
+extern "C" int tile_emu_apply(const qs_plan *P, int n, double *state, int remap, int *n_passes_out)
+{
+    g_err[0] = 0;
+    const size_t npass = P->passes.size();
+    std::vector<qs_tiled_desc> descs;
+    std::vector<int> dst;
+    if (qs_plan_tiled_schedule(P, n, 0, npass, remap, descs, dst)) return fail("schedule failed");
+    if (n_passes_out) *n_passes_out = (int)npass;
+    const uint64_t N = 1ull << n, tiles = N >> 12;
+    std::vector<cd> buf0(reinterpret_cast<cd *>(state), reinterpret_cast<cd *>(state) + N), buf1(N, cd(0, 0));
+    std::vector<cd> *bufs[2] = {&buf0, &buf1};
+    std::vector<int> hits(N);
+    for (size_t k = 0; k < npass; ++k) {
+        const qs_tiled_desc &d = descs[k];
+        Layout L;
+        LoadMap M;
+        if (qs_tile_layout_build(n, d.T, d.nsub, d.qpos, d.has_rows ? d.rows : nullptr, &L, &M,
+                                 d.has_write ? d.wtile : nullptr))
+            return fail("layout build failed", (long long)k);
+        StoreMap W;
+        memset(&W, 0, sizeof(W));
+        W.mode = d.has_write ? d.wmode : 0;
+        W.ntb = n - 12;
+        for (int i = 0; i < W.ntb && i < 52; ++i) W.wpos[i] = (int8_t)d.wpos[i];
+        if (d.has_write && dst[k] < 0) return fail("remapped pass scheduled in place", (long long)k);
+        const std::vector<cd> &in = dst[k] < 0 ? buf0 : *bufs[dst[k] ^ 1];
+        std::vector<cd> in_copy;
+        if (dst[k] < 0) in_copy = buf0;            // in place: tiles read and write the same set
+        const std::vector<cd> &src = dst[k] < 0 ? in_copy : in;
+        std::vector<cd> &out = dst[k] < 0 ? buf0 : *bufs[dst[k]];
+        // block unitaries (row = output basis index, column = input)
+        std::vector<std::vector<cd>> U(d.nsub, std::vector<cd>(32 * 32));
+        for (int b = 0; b < d.nsub; ++b) {
+            int kq = 0, qs[5];
+            std::vector<double> m(2048);
+            if (qs_plan_block(P, d.first_block + b, &kq, qs, m.data())) return fail("block", b);
+            for (int e = 0; e < 1024; ++e) U[b][e] = cd(m[2 * e], m[2 * e + 1]);
+        }
+        std::fill(hits.begin(), hits.end(), 0);
+        std::vector<cd> stage(4096), x(128 * 32), a(128 * 32);
+        std::vector<int> sh(4096), ah(128 * 32);
+        for (uint64_t t = 0; t < tiles; ++t) {
+            const uint64_t tbase = deposit_tile(t, L);
+            // ---- prefetch_tile: 128 threads x 16 chunks into the staging rows
+            std::fill(sh.begin(), sh.end(), 0);
+            for (int th = 0; th < 128; ++th) {
+                uint64_t g = 0;
+                uint32_t r = 0, jj = 0;
+                for (int tb = 1; tb < 8; ++tb) {
+                    if (!((th >> (tb - 1)) & 1)) continue;
+                    g |= 1ull << M.tpos[tb];
+                    const int mm = M.tmap0[tb];
+                    if (mm >= 0) r |= 1u << mm;
+                    else jj |= 1u << (~mm);
+                }
+                for (int kk = 0; kk < 16; ++kk) {
+                    const uint64_t s = tbase | g | M.gk[kk];
+                    if (s + 1 >= N) return fail("load out of range", (long long)s);
+                    const uint32_t row = r ^ M.rk[kk], j = jj ^ M.jk[kk];
+                    if (row >= 128 || j >= 32) return fail("staging slot out of range", row, j);
+                    if (M.rb0 < 0) {
+                        const uint32_t o = stage_off(row, j >> 1) / 8;
+                        stage[o] = src[s];
+                        stage[o + 1] = src[s + 1];
+                        sh[o]++;
+                        sh[o + 1]++;
+                    } else {
+                        const uint32_t half = j & 1;
+                        const uint32_t o0 = stage_off(row, j >> 1) / 8 + half;
+                        const uint32_t o1 = stage_off(row | (1u << M.rb0), j >> 1) / 8 + half;
+                        stage[o0] = src[s];
+                        stage[o1] = src[s + 1];
+                        sh[o0]++;
+                        sh[o1]++;
+                    }
+                }
+            }
+            for (int o = 0; o < 4096; ++o)
+                if (sh[o] != 1) return fail("staging slot not written exactly once", (long long)t, o);
+            // ---- read_stage_row
+            for (int row = 0; row < 128; ++row)
+                for (int j = 0; j < 32; ++j) x[row * 32 + j] = stage[stage_off(row, j >> 1) / 8 + (j & 1)];
+            // check against the per-row gather (block 0's rows and columns)
+            for (int row = 0; row < 128; ++row) {
+                uint64_t rb = 0;
+                for (int b = 0; b < 7; ++b) if ((row >> b) & 1) rb |= 1ull << L.c0_glob[b];
+                for (int j = 0; j < 32; ++j)
+                    if (x[row * 32 + j] != src[tbase | rb | L.g0[j]]) return fail("staged value mismatch", row, j);
+            }
+            for (int b = 0; b < d.nsub; ++b) {
+                // contraction: y[row][jo] = sum_ji U[jo][ji] x[row][ji]
+                std::vector<cd> y(128 * 32);
+                for (int row = 0; row < 128; ++row)
+                    for (int jo = 0; jo < 32; ++jo) {
+                        cd acc(0, 0);
+                        for (int ji = 0; ji < 32; ++ji) acc += U[b][jo * 32 + ji] * x[row * 32 + ji];
+                        y[row * 32 + jo] = acc;
+                    }
+                if (b + 1 < d.nsub) {
+                    std::fill(ah.begin(), ah.end(), 0);
+                    for (int row = 0; row < 128; ++row) {
+                        const uint32_t tp = emu_thread_part(L, b, row);
+                        for (int jo = 0; jo < 32; ++jo) {
+                            const uint32_t off = tp ^ L.scat[b][jo];
+                            if (off >= 128 * 128) return fail("scatter offset out of range", row, jo);
+                            const uint32_t r2 = off >> 7, chunk = (off >> 4) & 7;
+                            const uint32_t j2 = (((chunk ^ (r2 & 7)) & 7) << 2) | ((off >> 2) & 3);
+                            a[r2 * 32 + j2] = y[row * 32 + jo];
+                            ah[r2 * 32 + j2]++;
+                        }
+                    }
+                    for (int e = 0; e < 128 * 32; ++e)
+                        if (ah[e] != 1) return fail("A slot not written exactly once", (long long)t, e);
+                    x.swap(a);
+                } else {
+                    const uint64_t ob = emu_store_base(t, tbase, W);
+                    for (int row = 0; row < 128; ++row) {
+                        uint64_t gcl = 0;
+                        for (int bb = 0; bb < 7; ++bb) if ((row >> bb) & 1) gcl |= 1ull << L.cl_glob[bb];
+                        for (int jo = 0; jo < 32; ++jo) {
+                            const uint64_t o = ob | gcl | L.gl[jo];
+                            if (o >= N) return fail("store out of range", (long long)o);
+                            out[o] = y[row * 32 + jo];
+                            hits[o]++;
+                        }
+                    }
+                }
+            }
+        }
+        for (uint64_t i = 0; i < N; ++i)
+            if (hits[i] != 1) return fail("output amplitude not written exactly once", (long long)k, (long long)i);
+    }
+    memcpy(state, buf0.data(), N * sizeof(cd));
+    return 0;
+}
