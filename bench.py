@@ -52,9 +52,14 @@ def parse():
     ap.add_argument("--qubits", type=int, default=N_QUBITS)
     ap.add_argument("--depth", type=int, default=DEPTH)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="circuit32", choices=["circuit32", "vqe-sweep", "requests"],
+    ap.add_argument("--workload", default="circuit32",
+                    choices=["circuit32", "vqe-sweep", "requests", "qft28", "passes"],
                     help="circuit32: the 32-qubit random circuit (default); vqe-sweep: 4096 "
-                         "hardware-efficient-ansatz circuits of 10-22 qubits in one persistent launch")
+                         "hardware-efficient-ansatz circuits of 10-22 qubits in one persistent launch; "
+                         "requests: Poisson request trace against the server; qft28: 28-qubit QFT on the "
+                         "plain per-gate path in complex64 and complex128; passes: the random circuit "
+                         "(--qubits) applied once per tiled layout (in place, remap 1, remap 2) with its "
+                         "pass structure, for per-launch profiling")
     ap.add_argument("--circuits", type=int, default=4096)
     ap.add_argument("--requests", type=int, default=20000, help="requests workload: trace length")
     ap.add_argument("--every", type=int, default=10, help="requests workload: serve every k-th request")
@@ -687,6 +692,181 @@ def run_requests(args):
         dist.destroy_process_group()
 
 
+# ----------------------------------------------------------------- 28-qubit QFT
+QFT_SEED = 28028
+
+
+def run_qft(args):
+    """28-qubit QFT (H and CR(pi/2^k) on all pairs, then the reversal swaps) on a
+    seeded normalised complex Gaussian state, on the plain per-gate path in
+    complex64 and complex128: per-kernel HBM GB/s from CUDA events after every
+    gate, and the complex64 error against the complex128 run."""
+    import ctypes as C
+
+    import torch
+    ws, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    dist_init(ws, "nccl")
+    from qpanda_b200 import FusionPlan, StateVector, circuits, lib
+    from qpanda_b200.capi import OP, check
+
+    n = 28 if args.qubits == N_QUBITS else args.qubits
+    gates = circuits.qft(n)
+    rng = np.random.default_rng(QFT_SEED)
+    init = rng.standard_normal(1 << n) + 1j * rng.standard_normal(1 << n)
+    init /= np.linalg.norm(init)
+    L = lib()
+    stream = torch.cuda.current_stream()
+    kind_of = {OP["H"]: "k_pair (H, dense 2x2)", OP["CR"]: "k_phase (CR, N/4 amplitudes)",
+               OP["SWAP"]: "k_pair (SWAP exchange, N/2 amplitudes)"}
+    frac_of = {OP["H"]: 1.0, OP["CR"]: 0.25, OP["SWAP"]: 0.5}
+    gptr = [gates[i:i + 1].ctypes.data for i in range(len(gates))]
+    peak, peak_kind = peaks()
+    out, states = {}, {}
+    props = torch.cuda.get_device_properties(local)
+    gpu_id = "GPU-" + str(props.uuid) if getattr(props, "uuid", None) else str(local)
+    clocks = ClockSampler(gpu_id)
+    for dt, amp_b, npdt in (("c64", 8, np.complex64), ("c128", 16, np.complex128)):
+        sv = StateVector(n, dt)
+        host = init.astype(npdt)
+        kinds, circ = {}, []
+        for k in range(args.warmup + args.steps):
+            sv.set_state(host)
+            torch.cuda.synchronize()
+            ev = [torch.cuda.Event(enable_timing=True) for _ in range(len(gates) + 1)]
+            ev[0].record(stream)
+            for i in range(len(gates)):
+                check(L.qs_gate_apply(sv.handle, C.c_void_p(gptr[i])))
+                ev[i + 1].record(stream)
+            torch.cuda.synchronize()
+            if k < args.warmup:
+                continue
+            circ.append(ev[0].elapsed_time(ev[-1]) / 1e3)
+            for i in range(len(gates)):
+                op = int(gates[i]["op"])
+                kinds.setdefault(op, []).append(ev[i].elapsed_time(ev[i + 1]) / 1e3)
+        table = {}
+        for op, ts in kinds.items():
+            t = statistics.mean(ts)
+            gbs = 2 * amp_b * frac_of[op] * (1 << n) / t / 1e9
+            table[kind_of[op]] = {"launches_per_circuit": len(ts) // args.steps, "mean_ms": t * 1e3,
+                                  "gbs": gbs, "frac": gbs / peak}
+        cs = statistics.mean(circ)
+        out[dt] = {"circuit_s": cs, "hbm_gbs_effective": circuits.gate_bytes(gates, n, amp_b) / cs / 1e9,
+                   "kernels": table}
+        states[dt] = sv
+    clk = clocks.stop()
+    a, d = states["c64"], states["c128"]
+    ip = a.inner(d)
+    mx, ss = a.diff(d)
+    err = {"max_abs_err": mx, "l2_err": math.sqrt(ss), "fidelity": abs(ip) ** 2 / (a.norm2() * d.norm2()),
+           "oracle": "complex128 per-gate path (pinned to the CPU oracle by the GPU tests)"}
+    # the fused path on the same input, for comparison
+    a.set_state(init.astype(np.complex64))
+    p = FusionPlan(n, gates, remap=1)
+    p.apply(a)
+    torch.cuda.synchronize()
+    a.set_state(init.astype(np.complex64))
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    p.apply(a)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    fmx, _ = a.diff(d)
+    fused = {"circuit_s": e0.elapsed_time(e1) / 1e3, "passes": p.num_launches(), "max_abs_err_vs_c128": fmx}
+    p.close()
+    # e2e through the C ABI: host state in, gates, host state out (complex64)
+    pin_in = torch.empty((1 << n) * 8, dtype=torch.uint8).pin_memory()
+    pin_in.numpy().view(np.complex64)[:] = init.astype(np.complex64)
+    pin_out = torch.empty((1 << n) * 8, dtype=torch.uint8).pin_memory()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    check(L.qs_set_state(a.handle, C.c_void_p(pin_in.data_ptr()), 0))
+    check(L.qs_gates_apply(a.handle, gates.ctypes.data, len(gates)))
+    check(L.qs_get_state(a.handle, C.c_void_p(pin_out.data_ptr()), 0))
+    e2e_s = time.perf_counter() - t0
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        try:
+            from oracle.pyoracle import RefState
+            ns = 22
+            r = RefState(ns, omp=True)
+            t0 = time.perf_counter()
+            r.apply(circuits.qft(ns))
+            secs = time.perf_counter() - t0
+            scale = (1 << (n - ns)) * len(gates) / len(circuits.qft(ns))
+            cpu = {"value": circuits.gate_bytes(gates, n, 16) / (secs * scale) / 1e9, "unit": "GB/s",
+                   "cores": os.cpu_count(), "kind": "reference",
+                   "sample": (f"reference CPUQuantumGates.cpp (-fopenmp, {os.cpu_count()} threads, complex128) "
+                              f"on the {ns}-qubit QFT: {secs:.2f} s, extrapolated x{scale:.0f} to {n} qubits "
+                              f"({secs * scale:.0f} s); value = the same algorithmic bytes per second")}
+        except Exception as ex:
+            cpu = {"value": None, "unit": "GB/s", "kind": "reference", "sample": f"unavailable: {ex}"}
+    if rank == 0:
+        dom = max(out["c64"]["kernels"], key=lambda k: out["c64"]["kernels"][k]["mean_ms"] *
+                  out["c64"]["kernels"][k]["launches_per_circuit"])
+        dk = out["c64"]["kernels"][dom]
+        print(json.dumps({
+            "metric": "28q QFT HBM GB/s, plain per-gate path", "value": out["c64"]["hbm_gbs_effective"],
+            "unit": "GB/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": out["c64"]["circuit_s"] * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32 (complex64 state); f64 line under complex128", "data": "synthetic",
+            "config": {"workload": f"qft-{n}q", "qubits": n, "gates": len(gates), "seed": QFT_SEED,
+                       "input": "normalised i.i.d. complex Gaussian", "l2": "2-4 GiB states > L2, no flush"},
+            "complex64": out["c64"], "complex128": out["c128"], "error_c64": err, "fused_c64": fused,
+            "roofline": {"bound": "hbm", "kernel": dom, "achieved": dk["gbs"], "peak": peak, "unit": "GB/s",
+                         "frac": dk["gbs"] / peak, "peak_source": peak_kind, "traffic": None,
+                         "algorithmic_bytes_per_launch": None, "launch_s": dk["mean_ms"] / 1e3},
+            "cpu_baseline": cpu,
+            "e2e": {"value": circuits.gate_bytes(gates, n, 8) / e2e_s / 1e9, "unit": "GB/s",
+                    "h2d_bytes_per_step": 8 << n, "d2h_bytes_per_step": 8 << n,
+                    "includes": "host state in, the QFT per gate, host state out (complex64)"},
+            "gpu_launches": len(gates) * (args.warmup + args.steps) * 2, "clocks": clk,
+        }))
+    a.close()
+    d.close()
+
+
+# ----------------------------------------------------------------- pass profile
+def run_passes(args):
+    """The random circuit at --qubits applied once in each tiled layout (in
+    place, remap 1, remap 2) after one warm-up each; prints the pass structure
+    and each application's time.  Meant to run under a per-launch profiler."""
+    import ctypes as C
+
+    import torch
+    torch.cuda.set_device(0)
+    from qpanda_b200 import FusionPlan, StateVector, lib
+
+    n = args.qubits
+    gates = workload(n, args.depth)
+    sv = StateVector(n, "c64")
+    stream = torch.cuda.current_stream()
+    res = {}
+    for remap in (0, 1, 2):
+        p = FusionPlan(n, gates, remap=remap)
+        p.apply(sv)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        p.apply(sv)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        res[f"remap{remap}"] = {"passes": p.num_launches(), "circuit_ms": e0.elapsed_time(e1)}
+        if remap == 0:
+            L = lib()
+            struct = []
+            for i in range(p.num_launches()):
+                nb, T, Q = C.c_int(), (C.c_int * 12)(), (C.c_int * 15)()
+                L.qs_plan_pass(p.handle, i, C.byref(nb), T, Q)
+                struct.append({"tile": list(T), "blocks": [list(Q[5 * b:5 * b + 5]) for b in range(nb.value)]})
+            res["structure"] = struct
+        p.close()
+    sv.close()
+    print(json.dumps({"workload": f"passes-{n}q-depth{args.depth}", **res}))
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -695,6 +875,10 @@ def main():
         run_vqe_sweep(args)
     elif args.workload == "requests":
         run_requests(args)
+    elif args.workload == "qft28":
+        run_qft(args)
+    elif args.workload == "passes":
+        run_passes(args)
     else:
         run_b200(args)
 
