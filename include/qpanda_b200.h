@@ -41,6 +41,7 @@ extern "C" {
 #define QS_ERR_UNSUPPORTED -4   /* valid request this build does not provide */
 #define QS_ERR_NOT_UNITARY -5   /* matrix failed the |det|==1 check (CPUQuantumGates.cpp:1182-1186) */
 #define QS_ERR_STATE       -6   /* state handle is unusable (e.g. a measured probability of 0) */
+#define QS_ERR_IO          -7   /* a file could not be opened or written */
 
 /* ---- element types ----------------------------------------------------- */
 #define QS_C64   0              /* complex64: float re, float im  */
@@ -254,6 +255,38 @@ int qs_plan_status(qs_state *s);
 /* Free the second state-size buffer that plans with remap = 1 keep with the
  * state (no-op when there is none).  No reference counterpart. */
 int qs_release_spare(qs_state *s);
+
+/* ---- result formats ------------------------------------------------------ */
+/* Write the state to "<path_prefix>.fullstate" (binary = 0) or
+ * "<path_prefix>.fullstate.binary" (binary = 1), streamed from the device in
+ * chunks (the whole state never sits in host memory at once).
+ * Text: the reference's getQState text, one line per amplitude,
+ *   "state[i].real = <re> state[i].imag = <im>\n" with the default C++ stream
+ *   formatting (6 significant digits), which QCommandRun::saveQstate writes
+ *   verbatim (QPandaSDK/QuantumCommandControl/QCommand.cpp:402-428,
+ *   CPUQuantumGates.cpp:64-82).
+ * Binary: per amplitude the record { double real; double imag; } in native
+ *   byte order, index order - the layout QCommandRun::saveQstateBinary declares
+ *   (QCommand.cpp:437-480); the reference fills it by parsing the text lines
+ *   with atof, which yields 0.0 and an unset imaginary part, so its files do
+ *   not hold the amplitudes; this writer stores the amplitudes.
+ * complex64 states are widened to double for both.  Synchronizes the state's
+ * stream.  QS_ERR_IO if the file cannot be written. */
+int qs_write_fullstate(qs_state *s, const char *path_prefix, int binary);
+
+/* The result text of QPandaSDK::getResult (QPandaAPI.cpp:220-238): one line
+ * "<key> <value>\n" per outcome, the key as a width-bit binary string, most
+ * significant bit first (QPandaSDK::integerToBinary, QPandaAPI.cpp:295-305),
+ * the value with the default stream formatting, lines in ascending key order
+ * (the reference's std::map<string, double>).  For PMEASURE results the keys
+ * are pMeasure indices (width = number of measured qubits); for MEASURE
+ * results they are the classical-register bit strings read as numbers
+ * (width = number of registers) and the values their frequencies.  Writes at
+ * most cap bytes including the terminating NUL into buf (buf may be NULL to
+ * query); *needed receives the full length including the NUL.  Duplicate keys
+ * are rejected (QS_ERR_ARG), as a map cannot hold them. */
+int qs_format_outcomes(const uint64_t *keys, const double *values, size_t count, int width, char *buf,
+                       size_t cap, size_t *needed);
 
 /* ---- batched circuits: many circuits in one persistent launch ---------- */
 /* The reference runs one program per QPandaSDK::run (QPandaAPI.cpp:131-211); a

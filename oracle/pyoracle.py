@@ -154,6 +154,7 @@ def ref_lib(omp=False):
         "ref_pmeasure": (_i, [_vp, _ip, _i, C.POINTER(C.c_size_t), _dp]),
         "ref_sample": (_i, [_vp, _ip, _i, _dp, _sz, C.POINTER(C.c_uint64)]),
         "ref_rng_seed": (None, [_i]), "ref_rng_set_next": (None, [_d]),
+        "ref_qstate_text": (C.c_long, [_vp, C.c_char_p, _sz]),
     }
     for k, (r, a) in sig.items():
         f = getattr(L, k)
@@ -203,6 +204,15 @@ class RefState:
         cnt = self.L.ref_pmeasure(self.h, qs.ctypes.data_as(_ip), len(qs),
                                   idx.ctypes.data_as(C.POINTER(C.c_size_t)), p.ctypes.data_as(_dp))
         return list(zip(idx[:cnt].tolist(), p[:cnt].tolist()))
+
+    def qstate_text(self):
+        """The reference's getQState text (CPUQuantumGates.cpp:64-82)."""
+        need = -self.L.ref_qstate_text(self.h, None, 0)
+        buf = C.create_string_buffer(int(need))
+        r = self.L.ref_qstate_text(self.h, buf, need)
+        if r < 0:
+            raise RuntimeError("reference getQState failed")
+        return buf.value.decode()
 
     def sample(self, qubits, u):
         qs = np.asarray(qubits, dtype=np.int32)

@@ -164,4 +164,17 @@ int ref_sample(void *h, const int *qubits, int m, const double *u, size_t shots,
     return 0;
 }
 
+// The reference's getQState text (CPUQuantumGates.cpp:64-82) into buf (cap
+// bytes, NUL-terminated).  Returns its length, or -(length + 1) when buf is
+// too small, or -1 on failure.
+long ref_qstate_text(void *h, char *buf, size_t cap)
+{
+    RefState *s = static_cast<RefState *>(h);
+    std::string t;
+    if (!s->g.getQState(t, &s->param)) return -1;
+    if (t.size() + 1 > cap) return -(long)(t.size() + 1);
+    memcpy(buf, t.c_str(), t.size() + 1);
+    return (long)t.size();
+}
+
 }  // extern "C"

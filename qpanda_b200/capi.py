@@ -107,6 +107,8 @@ def lib():
         "qs_measure_noalloc": (i, [vp, i, i, i, d, vp, vp, vp]),
         "qs_plan_status": (i, [vp]),
         "qs_release_spare": (i, [vp]),
+        "qs_write_fullstate": (i, [vp, C.c_char_p, i]),
+        "qs_format_outcomes": (i, [C.POINTER(C.c_uint64), dp, sz, i, C.c_char_p, sz, C.POINTER(sz)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -119,6 +121,19 @@ def lib():
 def check(code):
     if code != QS_OK:
         raise QSError(code, lib().qs_last_error().decode(errors="replace"))
+
+
+def format_outcomes(keys, values, width):
+    """QPandaSDK::getResult text of an outcome map (qs_format_outcomes)."""
+    k = np.ascontiguousarray(keys, dtype=np.uint64)
+    v = np.ascontiguousarray(values, dtype=np.float64)
+    need = C.c_size_t()
+    check(lib().qs_format_outcomes(k.ctypes.data_as(C.POINTER(C.c_uint64)), _dptr(v), k.size, int(width),
+                                   None, 0, C.byref(need)))
+    buf = C.create_string_buffer(need.value)
+    check(lib().qs_format_outcomes(k.ctypes.data_as(C.POINTER(C.c_uint64)), _dptr(v), k.size, int(width),
+                                   buf, need.value, C.byref(need)))
+    return buf.value.decode()
 
 
 def _dptr(a):
@@ -151,6 +166,10 @@ class StateVector:
     def release_spare(self):
         """Free the second buffer that remapping plans keep with the state."""
         check(lib().qs_release_spare(self._h))
+
+    def write_fullstate(self, path_prefix, binary=False):
+        """Write <prefix>.fullstate (getQState text) or <prefix>.fullstate.binary."""
+        check(lib().qs_write_fullstate(self._h, os.fsencode(path_prefix), 1 if binary else 0))
 
     def __del__(self):
         try:

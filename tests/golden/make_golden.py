@@ -120,6 +120,13 @@ def main():
     for name, d in cases.items():
         np.savez_compressed(os.path.join(OUT, name + ".npz"), **d)
         print("wrote", name)
+    # 5) the reference's getQState text of the gates_n7 state: the .fullstate
+    #    file format (QCommand.cpp:402-428 writes this text verbatim)
+    r = RefState(7)
+    r.apply(cases["gates_n7"]["gates"])
+    with open(os.path.join(OUT, "qstate_n7.txt"), "w") as f:
+        f.write(r.qstate_text())
+    print("wrote qstate_n7.txt")
 
 
 if __name__ == "__main__":
