@@ -3,7 +3,9 @@
 Every .cu under qpanda_b200/csrc is compiled for sm_100a only
 (-gencode arch=compute_100a,code=sm_100a), every host-only .cpp with g++, and
 all are linked into one shared library that exports the C ABI declared in
-include/qpanda_b200.h.
+include/qpanda_b200.h.  Beside it, qpanda_b200/_lib/libGPUEmulator.so: the
+reference GPU compute unit's plug-in library (include/qpanda_b200_gpuemu.h,
+qpanda_b200/host/GPUEmulatorShim.cpp) over that C ABI.
 """
 import concurrent.futures as cf
 import os
@@ -65,8 +67,18 @@ def build(verbose=False):
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError("link failed:\n" + " ".join(cmd) + "\n" + r.stdout + r.stderr)
+    shim_src = os.path.join(HERE, "host", "GPUEmulatorShim.cpp")
+    shim = os.path.join(LIB, "libGPUEmulator.so")
+    shim_deps = [shim_src, so, os.path.join(ROOT, "include", "qpanda_b200_gpuemu.h"),
+                 os.path.join(ROOT, "include", "qpanda_b200.h")]
+    if _newer(shim_deps, shim):
+        cmd = [CXX] + CXXFLAGS + ["-shared", shim_src, "-o", shim, "-L" + LIB, "-lqsb200", "-ldl",
+                                  "-Wl,-rpath,$ORIGIN", "-Wl,-soname,libGPUEmulator.so"]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError("libGPUEmulator.so failed:\n" + " ".join(cmd) + "\n" + r.stdout + r.stderr)
     if verbose:
-        print("built", so)
+        print("built", so, "and", shim)
     return so
 
 

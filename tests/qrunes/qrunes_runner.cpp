@@ -6,6 +6,11 @@
 // behind the QuantumGates interface.  The QuantumGates base (constructor and
 // the 16807 generator) comes from oracle/ref_shim.cpp, seeded explicitly.
 //
+// Backend 3 is the reference's own GPU compute unit (GPUQuantumGates.cpp,
+// unmodified), which dlopens "libGPUEmulator.so" - here this repository's
+// qpanda_b200/_lib/libGPUEmulator.so, loaded by the caller beforehand - and is
+// handed the same generator as the other backends.
+//
 // qr_run mirrors QPandaSDK::loadFile + QPandaSDK::run (QPandaAPI.cpp:59-96,
 // 131-211): parse, initState, then per shot transmit() - an END node (reset
 // to |0...0>, QuantumInstructionHandleAPI.cpp:96-100) followed by every node -
@@ -19,12 +24,19 @@
 #include <sstream>
 #include <string>
 
+#include <dlfcn.h>
+
 #include "CPUQuantumGates.h"
+#include "GPUQuantumGates.h"
 #include "QRunesParserAPI.h"
 #include "QuantumInstructionGet.h"
 #include "B200QuantumGates.h"
 
 extern "C" void ref_rng_seed(int seed);
+
+// The GPU compute unit's gates draw from the program's QuantumGates generator.
+static QuantumGates *g_rng_owner = nullptr;
+static double program_rng() { return g_rng_owner->randGenerator(); }
 
 static bool transmit(QList &list, QuantumGateParam *param, QuantumGates *g)
 {
@@ -43,7 +55,8 @@ static std::string to_binary(size_t v, size_t len)
     return s;
 }
 
-// backend: 0 = reference CPU, 1 = B200 complex128, 2 = B200 complex64.
+// backend: 0 = reference CPU, 1 = B200 complex128, 2 = B200 complex64,
+// 3 = the reference's GPUQuantumGates over libGPUEmulator.so.
 // Writes "MEASURE bits:freq,..." or "PMEASURE bits:prob,..." into out.
 // Returns the qubit count, or a negative value on failure.
 extern "C" int qr_run(const char *path, int backend, int seed, int repeat, char *out, size_t out_len)
@@ -53,8 +66,24 @@ extern "C" int qr_run(const char *path, int backend, int seed, int repeat, char 
     int n = QRunesParser(file, list);
     if (n <= 0 || n > 30) return -1;
     std::unique_ptr<QuantumGates> g;
-    if (backend == 0) g.reset(new CPUQuantumGates());
-    else g.reset(new B200QuantumGates(backend == 2 ? QS_C64 : QS_C128));
+    if (backend == 0) {
+        g.reset(new CPUQuantumGates());
+    } else if (backend == 3) {
+        void *emu = dlopen("libGPUEmulator.so", RTLD_NOW | RTLD_NOLOAD);
+        if (!emu) return -5;
+        typedef void (*set_rng_fn)(double (*)(void));
+        set_rng_fn set_rng = reinterpret_cast<set_rng_fn>(dlsym(emu, "qs_gpuemu_set_rng"));
+        if (!set_rng) return -5;
+        try {
+            g.reset(new GPUQuantumGates());
+        } catch (...) {
+            return -5;
+        }
+        g_rng_owner = g.get();
+        set_rng(&program_rng);
+    } else {
+        g.reset(new B200QuantumGates(backend == 2 ? QS_C64 : QS_C128));
+    }
     QuantumGateParam param;
     param.mQuantumBitNumber = n;
     if (g->initState(&param) != qErrorNone) return -2;
@@ -86,6 +115,13 @@ extern "C" int qr_run(const char *path, int backend, int seed, int repeat, char 
         first = false;
     }
     std::string s = os.str();
+    // the GPU compute unit's destructor does not free its state
+    if (backend == 3) {
+        g->destroyState((size_t)n);
+        typedef void (*set_rng_fn)(double (*)(void));
+        void *emu = dlopen("libGPUEmulator.so", RTLD_NOW | RTLD_NOLOAD);
+        if (emu) reinterpret_cast<set_rng_fn>(dlsym(emu, "qs_gpuemu_set_rng"))(nullptr);
+    }
     if (s.size() + 1 > out_len) return -4;
     memcpy(out, s.c_str(), s.size() + 1);
     return n;

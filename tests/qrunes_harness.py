@@ -6,7 +6,8 @@ import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 RUNNER_SO = os.path.join(HERE, "qrunes", "_build", "libqrunes_runner.so")
-CPU, B200_C128, B200_C64 = 0, 1, 2
+CPU, B200_C128, B200_C64, GPU_UNIT = 0, 1, 2, 3
+EMU_SO = os.path.join(os.path.dirname(HERE), "qpanda_b200", "_lib", "libGPUEmulator.so")
 
 
 def available():
@@ -21,6 +22,8 @@ def runner():
     if _lib is None:
         import qpanda_b200
         qpanda_b200.lib()                      # the product library first (same process)
+        # the GPU compute unit dlopens "libGPUEmulator.so" by name: load ours first
+        C.CDLL(EMU_SO, mode=C.RTLD_GLOBAL)
         _lib = C.CDLL(RUNNER_SO)
         _lib.qr_run.restype = C.c_int
         _lib.qr_run.argtypes = [C.c_char_p, C.c_int, C.c_int, C.c_int, C.c_char_p, C.c_size_t]

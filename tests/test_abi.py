@@ -12,14 +12,44 @@ from qpanda_b200.capi import GATE_DTYPE, LIB_PATH
 HDR = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "include")
 
 
+EMU_HDR = "qpanda_b200_gpuemu.h"
+EMU_LIB = os.path.join(os.path.dirname(LIB_PATH), "libGPUEmulator.so")
+
+
 def declared():
     names = set()
     for f in os.listdir(HDR):
-        if f.endswith(".h"):
+        if f.endswith(".h") and f != EMU_HDR:
             txt = open(os.path.join(HDR, f)).read()
             txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
             names |= set(re.findall(r"^\s*(?:const\s+)?[\w\s\*]+?\b(qs\w+)\s*\(", txt, flags=re.M))
     return sorted(names)
+
+
+def declared_emu():
+    """Every function of the GPU-emulator plug-in header (gate names of the
+    reference's GPUGatesDecl.h plus the two qs_gpuemu_* calls)."""
+    txt = open(os.path.join(HDR, EMU_HDR)).read()
+    txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+    names = set(re.findall(r"^(?:bool|int|void)\s+(\w+)\s*\(", txt, flags=re.M))
+    # C++ names bound to another exported symbol with an assembler label
+    for cxx, sym in re.findall(r"^(?:bool|int|void)\s+(\w+)\s*\([^;]*?__asm__\(\"(\w+)\"\)", txt, flags=re.M | re.S):
+        names.discard(cxx)
+        names.add(sym)
+    return sorted(names)
+
+
+def test_emulator_header_lists_the_reference_names():
+    names = declared_emu()
+    for n in ("initstate", "clearState", "Hadamard", "RXdagger", "qubitmeasure", "controlRZdagger",
+              "toffoli", "qbReset", "pMeasurenew", "getState", "pCRdagger"):
+        assert n in names
+
+
+@pytest.mark.parametrize("name", declared_emu())
+def test_emulator_symbol_exported(name):
+    L = ctypes.CDLL(EMU_LIB)
+    assert hasattr(L, name), f"{name} declared in {EMU_HDR} but not exported by libGPUEmulator.so"
 
 
 def test_library_exists_and_loads():

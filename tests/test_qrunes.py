@@ -97,6 +97,56 @@ def test_b200_backend_measure_counts_bit_exact(need_gpu, tmp_path):
     assert r0 == r1
 
 
+def gpu_unit_programs(tmp_path):
+    """Programs within what the reference GPU compute unit implements: its
+    controlled NOT / CNOT / iSWAP / sqiSWAP overloads and controlSwap return
+    without doing anything (GPUQuantumGates.cpp:587-594, 729-733, 975-983)."""
+    paths = programs(tmp_path)
+    from tests.golden.make_golden import every_gate_circuit
+    eg = every_gate_circuit(7, 33)
+    keep = [i for i in range(len(eg))
+            if not (int(eg[i]["op"]) in (2, 6, 8, 9) and eg[i]["nctrl"] > 0)
+            and not (int(eg[i]["op"]) == 8 and eg[i]["nctrl"] == 0) and int(eg[i]["op"]) != 11]
+    eg = eg[keep]
+    for i in range(len(eg)):
+        if int(eg[i]["op"]) == 7:
+            eg[i]["nctrl"] = 0
+    p = tmp_path / "gpu_unit_every_gate.txt"
+    p.write_text(to_qrunes(7, eg, pmeasure=[6, 0, 3, 1]))
+    paths["gpu_unit_every_gate_pmeasure"] = str(p)
+    del paths["every_gate_pmeasure"]
+    return paths
+
+
+@needs_runner
+@pytest.mark.gpu
+def test_reference_gpu_unit_over_shim_pmeasure(need_gpu, tmp_path):
+    """The reference's own GPUQuantumGates (compiled from its sources,
+    unmodified) over libGPUEmulator.so gives the CPU backend's PMEASURE
+    results."""
+    for name, path in gpu_unit_programs(tmp_path).items():
+        if "pmeasure" not in name:
+            continue
+        k0, r0, _ = H.run(path, H.CPU)
+        k1, r1, _ = H.run(path, H.GPU_UNIT)
+        assert k0 == k1 == "PMEASURE"
+        assert set(r0) == set(r1), name
+        for b in r0:
+            assert abs(r0[b] - r1[b]) < 1e-12, (name, b)
+
+
+@needs_runner
+@pytest.mark.gpu
+def test_reference_gpu_unit_over_shim_measure_counts(need_gpu, tmp_path):
+    """Same generator seed: the same MEASURE counts as the CPU backend, shot
+    by shot (each gate and measurement draws like the CPU backend)."""
+    path = programs(tmp_path)["layers_measure"]
+    k0, r0, _ = H.run(path, H.CPU, seed=99, repeat=64)
+    k1, r1, _ = H.run(path, H.GPU_UNIT, seed=99, repeat=64)
+    assert k0 == k1 == "MEASURE"
+    assert r0 == r1
+
+
 @needs_runner
 def test_cpu_harness_every_gate_program_matches_oracle(tmp_path):
     """The generated every-gate program (nested CONTROL and DAGGER blocks)
