@@ -47,6 +47,10 @@ def parse():
     ap.add_argument("--path", default="fused", choices=["plain", "fused"])
     ap.add_argument("--kernel", default="tiled", choices=["tiled", "single"],
                     help="fused path: tiled passes (up to 3 blocks per pass) or one block per pass")
+    ap.add_argument("--max-sub", type=int, default=2, choices=[1, 2, 3],
+                    help="tiled passes: fused blocks per pass")
+    ap.add_argument("--low", type=int, default=3, choices=[1, 2, 3, 4, 5],
+                    help="tiled passes: qubits 0..low-1 in every tile (contiguous runs of 2^low amplitudes)")
     ap.add_argument("--remap", type=int, default=1, choices=[0, 1],
                     help="tiled passes: 1 = contiguous tile writes through a second state-size buffer")
     ap.add_argument("--qubits", type=int, default=N_QUBITS)
@@ -304,7 +308,7 @@ def run_b200(args):
     sv = StateVector(n, "c64")
     h = sv.handle
     remap = args.kernel == "tiled" and args.remap == 1
-    plan = FusionPlan(n, gates, kernel=args.kernel, remap=remap)
+    plan = FusionPlan(n, gates, kernel=args.kernel, remap=remap, low_qubits=args.low, max_sub=args.max_sub)
     plan.remap = remap
     nb = plan.num_launches()
     nblocks = plan.num_blocks()
@@ -361,7 +365,7 @@ def run_b200(args):
     if rank == 0 and n >= 30:
         nf = 30
         gf = workload(nf, depth)
-        pf = FusionPlan(nf, gf, kernel=args.kernel, remap=remap)
+        pf = FusionPlan(nf, gf, kernel=args.kernel, remap=remap, low_qubits=args.low, max_sub=args.max_sub)
         a = StateVector(nf, "c64")
         pf.apply(a)
         pf.status(a)
@@ -398,6 +402,9 @@ def run_b200(args):
             if args.kernel == "single":
                 o.kernel, o.max_sub = 1, 1
             o.remap = 1 if remap else 0
+            o.low_qubits = args.low
+            if args.kernel == "tiled":
+                o.max_sub = args.max_sub
             check(L.qs_plan_create_ex(n, C.c_void_p(pin_g.data_ptr()), ng, C.byref(o), C.byref(ph)))
             check(L.qs_plan_apply(h, ph))
         else:
@@ -427,7 +434,7 @@ def run_b200(args):
             "data": "synthetic",
             "config": {"workload": f"random-circuit-{n}q-depth{depth}-c64", "qubits": n, "depth": depth,
                        "gates": ng, "fused_blocks": nblocks, "fused_passes": nb, "kernel": args.kernel,
-                       "remap": remap, "device_bytes": (amp_b << n) * (2 if remap and path == "fused" else 1),
+                       "remap": remap, "low_qubits": args.low, "max_sub": args.max_sub, "device_bytes": (amp_b << n) * (2 if remap and path == "fused" else 1),
                        "iswap_frac": ISWAP_FRAC, "seed": SEED, "path": path,
                        "state_bytes": amp_b << n, "l2": "inputs larger than L2 (32 GiB state), no flush",
                        "parallelism": f"replicas x{ws}"},
@@ -845,7 +852,7 @@ def run_passes(args):
     stream = torch.cuda.current_stream()
     res = {}
     for remap in (0, 1, 2):
-        p = FusionPlan(n, gates, remap=remap)
+        p = FusionPlan(n, gates, remap=remap, low_qubits=args.low, max_sub=args.max_sub)
         p.apply(sv)
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -864,7 +871,7 @@ def run_passes(args):
             res["structure"] = struct
         p.close()
     sv.close()
-    print(json.dumps({"workload": f"passes-{n}q-depth{args.depth}", **res}))
+    print(json.dumps({"workload": f"passes-{n}q-depth{args.depth}", "low_qubits": args.low, **res}))
 
 
 def main():

@@ -11,11 +11,12 @@
 //
 // Per tile, a lane of 128 threads (thread i owns row i and TMEM lane i,
 // qs_tile_core.cuh) does:
-//   1. its row of block 0 arrives by cp.async in a staging row of its own; it
-//      reads it to registers, writes the BF16 hi/lo split into the swizzled
-//      K-major A buffer (16-byte chunks), and at once issues the copies of its
-//      row of the lane's next tile into the same staging row, so that they
-//      land while this tile is computed;
+//   1. the tile arrives by cp.async in tile order, each thread copying 16
+//      chunks of 16 bytes (the 32 lanes of a warp fill 512 contiguous bytes of
+//      shared memory per instruction); each thread then splits its own chunks
+//      into BF16 hi/lo at their rows and columns of the swizzled K-major A
+//      buffer and at once issues its copies of the lane's next tile into the
+//      same slots, so that they land while this tile is computed;
 //   2. for each block: one thread issues the 12 MMAs and commits to the
 //      lane's mbarrier; every thread waits, loads its 64 FP32 results from
 //      TMEM, and either scatters them as BF16 hi/lo into the next block's A
@@ -188,28 +189,19 @@ __global__ void __launch_bounds__(Shape<SUB>::kCtaThreads, 1) k_fused_tile(const
     uint64_t tile = (uint64_t)blockIdx.x * S::kLanes + lane;
     const uint64_t step = tile_base(stride, L);
     uint64_t tbase = tile_base(tile, L);
-    if (tile < P.tiles) prefetch_tile(amp, tbase, P.M, stage, cb);
+    if (tile < P.tiles) prefetch_tile_linear(amp, tbase, P.M, stage, cb.g, ltid);
     for (; tile < P.tiles; tile += stride) {
         const uint64_t tnext = tile_base_advance(tbase, step, L.tmask);
-        const bool more = tile + stride < P.tiles;
-        // ---- block 0 input: staging row -> registers -> A
+        // ---- block 0 input: this thread's staged chunks -> A; then its
+        // chunks of the lane's next tile (its own staging slots, just read)
         asm volatile("cp.async.wait_group 0;" ::: "memory");
-        lane_bar(bar_id);                     // every thread's copies of this tile have landed
-        float x[64];
-        read_stage_row(stage, row, x);
-        if (want_in) {
-            float t = 0.f;
-#pragma unroll
-            for (int e = 0; e < 64; ++e) t = fmaf(x[e], x[e], t);
-            acc_in += (double)t;
-        }
-        a_store_row(aHi, aLo, row, x);
+        const float ss = convert_tile(stage, aHi, aLo, P.M, cb, ltid);
+        if (want_in) acc_in += (double)ss;
+        if (tile + stride < P.tiles) prefetch_tile_linear(amp, tnext, P.M, stage, cb.g, ltid);
 
         for (int b = 0; b < L.nsub; ++b) {
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             lane_bar(bar_id);
-            // every staging row has been read: refill them with the lane's next tile
-            if (b == 0 && more) prefetch_tile(amp, tnext, P.M, stage, cb);
             if (ltid == 0)
                 issue_block_mma(tmem, a_hi, a_lo, smem_u32(smem + S::kOffB + (2 * b) * kB),
                                 smem_u32(smem + S::kOffB + (2 * b + 1) * kB), mb);

@@ -448,10 +448,15 @@ static void tiled_pass_desc(const qs_plan *P, size_t u, bool last, int mode, std
     for (size_t b = 0; b < pp.count; ++b)
         for (int j = 0; j < 5; ++j) d.qpos[b][j] = pos[P->blocks[pp.first + b].q[j]];
     d.has_rows = 1;
-    for (size_t b = 0; b < pp.count; ++b)
-        for (int i = 0; i < 7; ++i) d.rows[b][i] = pos[pp.rows[b][i]];
     bool ident = true;
     for (int q = 0; q < n; ++q) ident = ident && pos[q] == q;
+    // row orders: the plan's for the natural layout, chosen afresh for a
+    // permuted one (which tile bits are lowest - and so which lanes hold what -
+    // depends on the positions)
+    if (ident || qs_tile_row_orders(n, d.T, d.nsub, d.qpos, d.rows) != QS_OK) {
+        for (size_t b = 0; b < pp.count; ++b)
+            for (int i = 0; i < 7; ++i) d.rows[b][i] = pos[pp.rows[b][i]];
+    }
     d.has_write = 0;
     if (last && ident) return;              // natural in, natural out: in place
     d.has_write = 1;

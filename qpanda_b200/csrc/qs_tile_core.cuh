@@ -56,8 +56,11 @@ struct LoadMap {
     uint8_t jk[16];              //   ... block-0 column bits
     int8_t tpos[12];             // global position of tile bit t
     int8_t tmap0[12];            // tile bit t in block 0: row bit (>= 0) or ~column bit
-    int8_t rb0;                  // row bit of tile bit 0 in block 0, or -1 when it is column bit 0
-    int8_t pad[7];
+    // A chunk's second amplitude (tile bit 0 set) sits at (row ^ dr, column ^ dj)
+    // of the first; pair = 1 when tile bit 0 is block 0's column bit 0 (dj = 1,
+    // dr = 0: the two are adjacent columns of one row).
+    uint8_t dr, dj, pair;
+    int8_t pad[5];
 };
 
 // Thread part of the scatter offset (see Layout::scat).
@@ -224,40 +227,80 @@ __device__ __forceinline__ ChunkBase chunk_base(const LoadMap &L, int t128)
     return c;
 }
 
-// Asynchronous copies of a whole tile of block 0's input into the staging
-// rows (same layout as prefetch_row), by 128 threads together: the 32 lanes
-// of a warp copy 32 consecutive 16-byte chunks of the tile, so every copy
-// instruction reads whole runs of contiguous memory and its data lands in
-// shared memory in a few wavefronts.  The staging rows are shared by the 128
-// threads: a barrier must separate the copies' completion from the reads, and
-// the reads from the next tile's copies.
-__device__ __forceinline__ void prefetch_tile(const float *amp, uint64_t base, const LoadMap &L, uint32_t stage,
-                                              const ChunkBase &cb)
+// Tile-order staging (k_fused_tile): chunk c of the tile - tile indices 2c,
+// 2c+1 - is copied to byte 16c, chunk c = 128 k + thread, so the 32 lanes of a
+// warp fill 512 contiguous bytes of shared memory per copy instruction, however
+// short the tile's contiguous runs in global memory are.  Each thread later
+// reads back only its own chunks (convert_tile): no barrier separates the
+// copies from the reads, nor the reads from the next tile's copies.
+__device__ __forceinline__ void prefetch_tile_linear(const float *amp, uint64_t base, const LoadMap &M,
+                                                     uint32_t stage, uint64_t g_thread, int t128)
 {
-    if (L.rb0 < 0) {
-        // tile bit 0 is block 0's column bit 0: a chunk is a column pair of one row
 #pragma unroll
-        for (int k = 0; k < 16; ++k) {
-            const float *src = amp + 2 * (base | cb.g | L.gk[k]);
-            const uint32_t row = cb.r ^ L.rk[k], jp = (cb.j ^ L.jk[k]) >> 1;
-            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" :: "r"(stage_addr(stage, row, jp)),
-                         "l"(src) : "memory");
-        }
-    } else {
-        // tile bit 0 is a row bit: a chunk is one column of two rows
-        const uint32_t rbm = 1u << L.rb0;
-#pragma unroll
-        for (int k = 0; k < 16; ++k) {
-            const float *src = amp + 2 * (base | cb.g | L.gk[k]);
-            const uint32_t row = cb.r ^ L.rk[k], j = cb.j ^ L.jk[k];
-            const uint32_t half = (j & 1) << 3;
-            asm volatile("cp.async.ca.shared.global [%0], [%1], 8;"
-                         :: "r"(stage_addr(stage, row, j >> 1) + half), "l"(src) : "memory");
-            asm volatile("cp.async.ca.shared.global [%0], [%1], 8;"
-                         :: "r"(stage_addr(stage, row | rbm, j >> 1) + half), "l"(src + 2) : "memory");
-        }
+    for (int k = 0; k < 16; ++k) {
+        const float *src = amp + 2 * (base | g_thread | M.gk[k]);
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" :: "r"(stage + (uint32_t)(128 * k + t128) * 16u),
+                     "l"(src) : "memory");
     }
     asm volatile("cp.async.commit_group;" ::: "memory");
+}
+
+__device__ __forceinline__ void read_stage_row(uint32_t stage, int row, float (&x)[64])
+{
+#pragma unroll
+    for (int k = 0; k < 16; ++k) {
+        float4 v;
+        asm volatile("ld.shared.v4.f32 {%0,%1,%2,%3}, [%4];"
+                     : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w) : "r"(stage_addr(stage, row, k)));
+        x[4 * k] = v.x; x[4 * k + 1] = v.y; x[4 * k + 2] = v.z; x[4 * k + 3] = v.w;
+    }
+}
+
+// BF16 hi/lo split of a complex pair: hi = bf16(x), lo = bf16(x - hi).
+__device__ __forceinline__ void split_pair(float re, float im, uint32_t &hv, uint32_t &lv)
+{
+    hv = pack_bf16x2(re, im);
+    lv = pack_bf16x2(re - __uint_as_float(hv << 16), im - __uint_as_float(hv & 0xffff0000u));
+}
+
+// Byte offset of (row r, column j) in a swizzled K-major A buffer.
+__device__ __forceinline__ uint32_t a_offset(uint32_t r, uint32_t j)
+{
+    return r * 128 + ((((j >> 2) ^ (r & 7)) & 7) << 4) + ((j & 3) << 2);
+}
+
+// Each thread splits its own 16 staged chunks into block 0's A buffers (BF16
+// hi/lo), at the rows and columns the LoadMap gives; returns the chunks'
+// sum of squares.  Column pairs (tile bit 0 = block-0 column bit 0) go out as
+// one 8-byte store per buffer; otherwise the two amplitudes of a chunk sit at
+// (r, j) and (r | dr, j | dj) and go out as 4-byte stores.
+__device__ __forceinline__ float convert_tile(uint32_t stage, uint8_t *aHi, uint8_t *aLo, const LoadMap &M,
+                                              const ChunkBase &cb, int t128)
+{
+    float ss = 0.f;
+#pragma unroll
+    for (int k = 0; k < 16; ++k) {
+        float4 v;
+        asm volatile("ld.shared.v4.f32 {%0,%1,%2,%3}, [%4];"
+                     : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w) : "r"(stage + (uint32_t)(128 * k + t128) * 16u));
+        ss = fmaf(v.x, v.x, fmaf(v.y, v.y, fmaf(v.z, v.z, fmaf(v.w, v.w, ss))));
+        const uint32_t row = cb.r ^ M.rk[k], j = cb.j ^ M.jk[k];
+        uint32_t h0, l0, h1, l1;
+        split_pair(v.x, v.y, h0, l0);
+        split_pair(v.z, v.w, h1, l1);
+        if (M.pair) {
+            const uint32_t off = a_offset(row, j);            // j even: columns j, j+1 are adjacent
+            *reinterpret_cast<uint2 *>(aHi + off) = make_uint2(h0, h1);
+            *reinterpret_cast<uint2 *>(aLo + off) = make_uint2(l0, l1);
+        } else {
+            const uint32_t o0 = a_offset(row, j), o1 = a_offset(row | M.dr, j | M.dj);
+            *reinterpret_cast<uint32_t *>(aHi + o0) = h0;
+            *reinterpret_cast<uint32_t *>(aLo + o0) = l0;
+            *reinterpret_cast<uint32_t *>(aHi + o1) = h1;
+            *reinterpret_cast<uint32_t *>(aLo + o1) = l1;
+        }
+    }
+    return ss;
 }
 
 // Where a pass writes a tile's results (k_fused_tile).  The 12 tile bits go
@@ -280,24 +323,6 @@ __device__ __forceinline__ uint64_t store_base(uint64_t tile, uint64_t read_base
     uint64_t b = 0;
     for (int i = 0; i < W.ntb; ++i) b |= ((tile >> i) & 1ull) << W.wpos[i];
     return b;
-}
-
-__device__ __forceinline__ void read_stage_row(uint32_t stage, int row, float (&x)[64])
-{
-#pragma unroll
-    for (int k = 0; k < 16; ++k) {
-        float4 v;
-        asm volatile("ld.shared.v4.f32 {%0,%1,%2,%3}, [%4];"
-                     : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w) : "r"(stage_addr(stage, row, k)));
-        x[4 * k] = v.x; x[4 * k + 1] = v.y; x[4 * k + 2] = v.z; x[4 * k + 3] = v.w;
-    }
-}
-
-// BF16 hi/lo split of a complex pair: hi = bf16(x), lo = bf16(x - hi).
-__device__ __forceinline__ void split_pair(float re, float im, uint32_t &hv, uint32_t &lv)
-{
-    hv = pack_bf16x2(re, im);
-    lv = pack_bf16x2(re - __uint_as_float(hv << 16), im - __uint_as_float(hv & 0xffff0000u));
 }
 
 // One complex amplitude as BF16 hi/lo pairs at row r, column j of the

@@ -15,8 +15,12 @@ using qs_tile::kMaxSub;
 // A block's 7 row bits may be listed in any order: rows are independent
 // columns of the contraction.  The order decides which tile bits a warp's 32
 // lanes (row bits 0..4) run over, and with it
-//   * how many 32-byte sectors one warp-wide global load (block 0) or store
-//     (last block) touches: lanes on qubits 0 and 1 share sectors;
+//   * how many shared-memory wavefronts the block-0 input stores take
+//     (convert_tile: the lanes of a warp hold consecutive chunks, i.e. tile
+//     bits 1..5, and write them at their rows and columns of the swizzled A
+//     buffer - row bits 0..2 and column bits land on different bank bits);
+//   * how many 32-byte sectors one warp-wide global store of the last block
+//     touches: lanes on qubits 0 and 1 share sectors;
 //   * how many shared-memory wavefronts one warp-wide 4-byte scatter store
 //     into the next block's swizzled A buffer takes: the bank of a store is
 //     offset bits 2..6 = the next block's column bits 0..1 and (column bits
@@ -34,6 +38,30 @@ int glob_cost(unsigned lanes, int loc0, int loc1, bool vec)
     if (loc1 >= 0) k += (lanes >> loc1) & 1;
     if (!vec && loc0 >= 0) k += (lanes >> loc0) & 1;
     return (vec ? 16 : 32) * (32 >> k);
+}
+
+// Wavefronts of convert_tile's stores for block 0 with columns Q0 and row
+// bits 0..2 on tile bits t[0..2]: a lane's store lands at byte bits 2..6
+// (4-byte stores) or 3..6 (8-byte column pairs) given by the lane's tile bits
+// 1..5 (1..4): column c -> bit 2 + c (c < 2) or c + 2, XOR'd with row bits
+// 0..2 -> bits 4..6; row bits 3.. land in the same banks.  Each lane bit that
+// finds no bit of its own doubles the wavefronts.
+int convert_cost(const int *Q0, const int *t)
+{
+    int col[12], rlo[12];
+    for (int b = 0; b < 12; ++b) col[b] = rlo[b] = -1;
+    for (int c = 0; c < 5; ++c) col[Q0[c]] = c;
+    for (int r = 0; r < 3; ++r) rlo[t[r]] = r;
+    const bool pair = col[0] == 0;
+    const int nl = pair ? 4 : 5, lo = pair ? 3 : 2;
+    unsigned hit = 0;
+    for (int b = 1; b <= nl; ++b) {
+        int a = -1;
+        if (col[b] >= 0) a = col[b] < 2 ? 2 + col[b] : col[b] + 2;
+        else if (rlo[b] >= 0) a = rlo[b] + 4;
+        if (a >= lo && a <= 6) hit |= 1u << a;
+    }
+    return 64 << (nl - __builtin_popcount(hit));
 }
 
 int scatter_cost(unsigned lanes, const int *Qn, const int *t)
@@ -54,7 +82,7 @@ void choose_row_orders(const int *T, int nsub, const int (*Q)[5], int (*Cp)[7])
         if (T[i] == 0) loc0 = i;
         if (T[i] == 1) loc1 = i;
     }
-    const bool vec0 = T[Q[0][0]] == 0, vecl = T[Q[nsub - 1][0]] == 0;
+    const bool vecl = T[Q[nsub - 1][0]] == 0;
     std::vector<RowCfg> cfg[kMaxSub];
     for (int b = 0; b < nsub; ++b) {
         const int *C = Cp[b];
@@ -74,7 +102,7 @@ void choose_row_orders(const int *T, int nsub, const int (*Q)[5], int (*Cp)[7])
     }
     std::vector<int> best[kMaxSub], from[kMaxSub];
     best[0].resize(cfg[0].size());
-    for (size_t i = 0; i < cfg[0].size(); ++i) best[0][i] = glob_cost(cfg[0][i].lanes, loc0, loc1, vec0);
+    for (size_t i = 0; i < cfg[0].size(); ++i) best[0][i] = convert_cost(Q[0], cfg[0][i].t);
     for (int b = 1; b < nsub; ++b) {
         // the previous block enters only through its lane set: keep its cheapest configuration per set
         std::vector<std::pair<unsigned, int>> sets;     // (lanes, configuration)
@@ -99,7 +127,7 @@ void choose_row_orders(const int *T, int nsub, const int (*Q)[5], int (*Cp)[7])
         if (c < bestc) { bestc = c; sel[last] = (int)i; }
     }
     // cost of the ascending orders (configuration 0 everywhere)
-    int base = glob_cost(cfg[0][0].lanes, loc0, loc1, vec0) + glob_cost(cfg[last][0].lanes, loc0, loc1, vecl);
+    int base = convert_cost(Q[0], cfg[0][0].t) + glob_cost(cfg[last][0].lanes, loc0, loc1, vecl);
     for (int b = 1; b < nsub; ++b) base += scatter_cost(cfg[b - 1][0].lanes, Q[b], cfg[b][0].t);
     if (bestc >= base) return;
     for (int b = last; b > 0; --b) sel[b - 1] = from[b][sel[b]];
@@ -214,7 +242,10 @@ int qs_tile_layout_build(int n, const int *T, int nsub, const int (*qpos)[5], co
         for (int p = 0; p < 12; ++p) M->tpos[p] = (int8_t)T[p];
         for (int i = 0; i < 7; ++i) M->tmap0[Cp[0][i]] = (int8_t)i;
         for (int i = 0; i < 5; ++i) M->tmap0[Q[0][i]] = (int8_t)~i;
-        M->rb0 = (int8_t)(M->tmap0[0] >= 0 ? M->tmap0[0] : -1);
+        const int m0 = M->tmap0[0];
+        M->dr = (uint8_t)(m0 >= 0 ? 1u << m0 : 0);
+        M->dj = (uint8_t)(m0 >= 0 ? 0 : 1u << (~m0));
+        M->pair = (uint8_t)(m0 == ~0);
         for (int k = 0; k < 16; ++k) {
             uint64_t g = 0;
             uint32_t rr = 0, jj = 0;

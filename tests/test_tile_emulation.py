@@ -35,9 +35,12 @@ def emu(tmp_path_factory):
     r = subprocess.run(cmd, capture_output=True, text=True)
     assert r.returncode == 0, r.stdout + r.stderr
     E = C.CDLL(out)
-    E.tile_emu_apply.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.POINTER(C.c_int)]
+    E.tile_emu_apply.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.POINTER(C.c_int),
+                                 C.POINTER(C.c_int)]
     E.tile_emu_apply.restype = C.c_int
     E.tile_emu_error.restype = C.c_char_p
+    E.tile_emu_check_input.argtypes = [C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]
+    E.tile_emu_check_input.restype = C.c_int
     return E
 
 
@@ -47,11 +50,15 @@ def random_state(n, seed):
     return v / np.linalg.norm(v)
 
 
-def run_emu(E, n, g, init, remap, **kw):
+def run_emu(E, n, g, init, remap, kinds=None, **kw):
     p = FusionPlan(n, g, remap=remap, **kw)
     st = np.ascontiguousarray(init.astype(np.complex128))
     npass = C.c_int()
-    rc = E.tile_emu_apply(p.handle, n, st.ctypes.data, int(remap), C.byref(npass))
+    k = (C.c_int * 3)()
+    rc = E.tile_emu_apply(p.handle, n, st.ctypes.data, int(remap), C.byref(npass), k)
+    if kinds is not None:
+        for i in range(3):
+            kinds[i] += k[i]
     assert rc == 0, E.tile_emu_error().decode()
     o = OracleState(n)
     o.set_state(init)
@@ -87,3 +94,37 @@ def test_tiled_index_math_qft_and_ansatz(emu, remap):
     assert err < 1e-10, err
     err, _ = run_emu(emu, n, circuits.vqe_ansatz(n, 3, seed=4), random_state(n, 3), remap)
     assert err < 1e-10, err
+
+
+def test_tiled_index_math_chunk_pairings_in_plans(emu):
+    """In-place and remapped plans meet both common pairings (tile bit 0 as
+    block 0's column 0, or as a row bit) and reproduce the oracle."""
+    kinds = [0, 0, 0]
+    for seed in range(12):
+        n = 14 + seed % 3
+        g = circuits.random_layers(n, 5, 900 + seed, iswap_frac=0.2)
+        for remap in (0, 1, 2):
+            err, _ = run_emu(emu, n, g, random_state(n, seed), remap, kinds=kinds)
+            assert err < 1e-10, (seed, remap, err)
+    assert kinds[0] > 0 and kinds[2] > 0, kinds
+
+
+def test_block0_input_mapping_any_column_order(emu):
+    """Arbitrary passes: tile bit 0 as column 0, as a later column (block
+    columns in any order - remapped layouts can give this) and as a row; every
+    A slot of every tile gets exactly its amplitude."""
+    rng = np.random.default_rng(3)
+    kinds = [0, 0, 0]
+    for it in range(300):
+        n = 12 + int(rng.integers(0, 9))
+        rest = rng.permutation(np.arange(1, n))[:11]
+        T = np.sort(np.concatenate([[0], rest])).astype(np.int32)
+        q = rng.permutation(T)[:5].astype(np.int32)
+        if it % 3 == 0 and 0 not in q:
+            q[int(rng.integers(1, 5))] = 0           # tile bit 0 as a later column
+        kind = C.c_int(-1)
+        rc = emu.tile_emu_check_input(n, T.ctypes.data_as(C.POINTER(C.c_int)),
+                                      q.ctypes.data_as(C.POINTER(C.c_int)), C.byref(kind))
+        assert rc == 0, (it, emu.tile_emu_error().decode())
+        kinds[kind.value] += 1
+    assert all(k > 0 for k in kinds), kinds

@@ -5,8 +5,9 @@
 // from the library's own scheduler (qs_plan_tiled_schedule), the per-pass
 // tables from its own layout builder (qs_tile_layout_build), and each tile
 // goes through
-//   * the warp-contiguous staging copies of prefetch_tile (LoadMap) into the
-//     swizzled staging rows, read back row by row as read_stage_row does;
+//   * the tile-order staging copies of prefetch_tile_linear (LoadMap) and
+//     convert_tile, which puts each thread's chunks at their block-0 rows and
+//     columns;
 //   * each block's contraction (in FP64 here, on the block unitaries of the
 //     plan, instead of split BF16 on the tensor cores);
 //   * the scatter of a block's results into the next block's swizzled A
@@ -87,7 +88,9 @@ int fail(const char *msg, long long a = 0, long long b = 0)
 extern "C" const char *tile_emu_error(void) { return g_err; }
 
 // Apply plan passes [0, all) to state (2^n complex128, interleaved re/im).
-extern "C" int tile_emu_apply(const qs_plan *P, int n, double *state, int remap, int *n_passes_out)
+// *kinds_out (may be NULL) counts the passes whose chunk pairs are adjacent
+// columns [0], other columns [1], two rows [2].
+extern "C" int tile_emu_apply(const qs_plan *P, int n, double *state, int remap, int *n_passes_out, int *kinds_out)
 {
     g_err[0] = 0;
     const size_t npass = P->passes.size();
@@ -106,6 +109,7 @@ extern "C" int tile_emu_apply(const qs_plan *P, int n, double *state, int remap,
         if (qs_tile_layout_build(n, d.T, d.nsub, d.qpos, d.has_rows ? d.rows : nullptr, &L, &M,
                                  d.has_write ? d.wtile : nullptr))
             return fail("layout build failed", (long long)k);
+        if (kinds_out) kinds_out[M.pair ? 0 : (M.dj ? 1 : 2)]++;
         StoreMap W;
         memset(&W, 0, sizeof(W));
         W.mode = d.has_write ? d.wmode : 0;
@@ -130,8 +134,11 @@ extern "C" int tile_emu_apply(const qs_plan *P, int n, double *state, int remap,
         std::vector<int> sh(4096), ah(128 * 32);
         for (uint64_t t = 0; t < tiles; ++t) {
             const uint64_t tbase = deposit_tile(t, L);
-            // ---- prefetch_tile: 128 threads x 16 chunks into the staging rows
+            // ---- prefetch_tile_linear: chunk c = 128 k + thread (tile indices
+            // 2c, 2c+1) into staging slot c, then convert_tile: each thread's
+            // chunks into block 0's rows and columns
             std::fill(sh.begin(), sh.end(), 0);
+            std::fill(ah.begin(), ah.end(), 0);
             for (int th = 0; th < 128; ++th) {
                 uint64_t g = 0;
                 uint32_t r = 0, jj = 0;
@@ -145,30 +152,27 @@ extern "C" int tile_emu_apply(const qs_plan *P, int n, double *state, int remap,
                 for (int kk = 0; kk < 16; ++kk) {
                     const uint64_t s = tbase | g | M.gk[kk];
                     if (s + 1 >= N) return fail("load out of range", (long long)s);
+                    const int c = 128 * kk + th;
+                    stage[2 * c] = src[s];
+                    stage[2 * c + 1] = src[s + 1];
+                    sh[2 * c]++;
+                    sh[2 * c + 1]++;
                     const uint32_t row = r ^ M.rk[kk], j = jj ^ M.jk[kk];
-                    if (row >= 128 || j >= 32) return fail("staging slot out of range", row, j);
-                    if (M.rb0 < 0) {
-                        const uint32_t o = stage_off(row, j >> 1) / 8;
-                        stage[o] = src[s];
-                        stage[o + 1] = src[s + 1];
-                        sh[o]++;
-                        sh[o + 1]++;
-                    } else {
-                        const uint32_t half = j & 1;
-                        const uint32_t o0 = stage_off(row, j >> 1) / 8 + half;
-                        const uint32_t o1 = stage_off(row | (1u << M.rb0), j >> 1) / 8 + half;
-                        stage[o0] = src[s];
-                        stage[o1] = src[s + 1];
-                        sh[o0]++;
-                        sh[o1]++;
-                    }
+                    const uint32_t row1 = row | M.dr, j1 = j | M.dj;
+                    if (row >= 128 || j >= 32 || row1 >= 128 || j1 >= 32 || row1 * 32 + j1 == row * 32 + j)
+                        return fail("A slot out of range", row, j);
+                    if (M.pair && !(M.dj == 1 && M.dr == 0 && (j & 1) == 0))
+                        return fail("column pair not adjacent", row, j);
+                    x[row * 32 + j] = stage[2 * c];
+                    x[row1 * 32 + j1] = stage[2 * c + 1];
+                    ah[row * 32 + j]++;
+                    ah[row1 * 32 + j1]++;
                 }
             }
             for (int o = 0; o < 4096; ++o)
                 if (sh[o] != 1) return fail("staging slot not written exactly once", (long long)t, o);
-            // ---- read_stage_row
-            for (int row = 0; row < 128; ++row)
-                for (int j = 0; j < 32; ++j) x[row * 32 + j] = stage[stage_off(row, j >> 1) / 8 + (j & 1)];
+            for (int o = 0; o < 4096; ++o)
+                if (ah[o] != 1) return fail("block-0 A slot not written exactly once", (long long)t, o);
             // check against the per-row gather (block 0's rows and columns)
             for (int row = 0; row < 128; ++row) {
                 uint64_t rb = 0;
@@ -220,5 +224,59 @@ extern "C" int tile_emu_apply(const qs_plan *P, int n, double *state, int remap,
             if (hits[i] != 1) return fail("output amplitude not written exactly once", (long long)k, (long long)i);
     }
     memcpy(state, buf0.data(), N * sizeof(cd));
+    return 0;
+}
+
+// One pass's block-0 input mapping for an arbitrary descriptor (columns in
+// any order, so that tile bit 0 can be any column or row of block 0): with
+// amplitude i of an n-qubit state set to i, every A slot (row, column) of
+// every tile must receive exactly the amplitude at tile base | row bits |
+// column bits.  Returns 0, or 1 with tile_emu_error() set; *kind = 0 adjacent
+// column pair, 1 other column, 2 rows.
+extern "C" int tile_emu_check_input(int n, const int *T, const int *qpos0, int *kind)
+{
+    g_err[0] = 0;
+    int qpos[3][5];
+    for (int j = 0; j < 5; ++j) qpos[0][j] = qpos0[j];
+    Layout L;
+    LoadMap M;
+    if (qs_tile_layout_build(n, T, 1, qpos, nullptr, &L, &M, nullptr)) return fail("layout build failed");
+    *kind = M.pair ? 0 : (M.dj ? 1 : 2);
+    const uint64_t N = 1ull << n, tiles = N >> 12;
+    std::vector<int> ah(4096);
+    std::vector<uint64_t> a(4096);
+    for (uint64_t t = 0; t < tiles; t += (tiles > 64 ? tiles / 64 : 1)) {
+        const uint64_t tbase = deposit_tile(t, L);
+        std::fill(ah.begin(), ah.end(), 0);
+        for (int th = 0; th < 128; ++th) {
+            uint64_t g = 0;
+            uint32_t r = 0, jj = 0;
+            for (int tb = 1; tb < 8; ++tb) {
+                if (!((th >> (tb - 1)) & 1)) continue;
+                g |= 1ull << M.tpos[tb];
+                const int mm = M.tmap0[tb];
+                if (mm >= 0) r |= 1u << mm;
+                else jj |= 1u << (~mm);
+            }
+            for (int kk = 0; kk < 16; ++kk) {
+                const uint64_t s0 = tbase | g | M.gk[kk];
+                const uint32_t row = r ^ M.rk[kk], j = jj ^ M.jk[kk];
+                const uint32_t row1 = row | M.dr, j1 = j | M.dj;
+                if (row1 >= 128 || j1 >= 32) return fail("A slot out of range", row1, j1);
+                a[row * 32 + j] = s0;
+                a[row1 * 32 + j1] = s0 + 1;
+                ah[row * 32 + j]++;
+                ah[row1 * 32 + j1]++;
+            }
+        }
+        for (int row = 0; row < 128; ++row) {
+            uint64_t rb = 0;
+            for (int b = 0; b < 7; ++b) if ((row >> b) & 1) rb |= 1ull << L.c0_glob[b];
+            for (int j = 0; j < 32; ++j) {
+                if (ah[row * 32 + j] != 1) return fail("A slot not written exactly once", row, j);
+                if (a[row * 32 + j] != (tbase | rb | L.g0[j])) return fail("A slot holds the wrong amplitude", row, j);
+            }
+        }
+    }
     return 0;
 }
