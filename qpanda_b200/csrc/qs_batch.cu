@@ -413,7 +413,7 @@ extern "C" int qs_batch_create(int n_circ, const int *n_qubits, const qs_gate *g
             for (size_t b = 0; b < pass.count; ++b)
                 for (int j = 0; j < 5; ++j) qpos[b][j] = pp->blocks[pass.first + b].q[j];
             int rows[3][7];
-            if ((r = qs_tile_row_orders(pp->n, pass.T, (int)pass.count, qpos, rows))) break;
+            if ((r = qs_tile_row_orders(pp->n, pass.T, (int)pass.count, qpos, rows, nullptr, 1))) break;
             if ((r = qs_tile_layout_build(pp->n, pass.T, (int)pass.count, qpos, rows, &L))) break;
             L.pad = (int32_t)pass.first;
             layouts.push_back(L);

@@ -55,7 +55,10 @@ struct qs_tiled_desc {
 
 int qs_tiled_grid(const qs_state *s);
 // Row-bit orders for a pass's blocks that keep warp-wide accesses coalesced
-// and the scatter between blocks free of shared-memory bank conflicts as far
-// as possible (qs_tile_layout.cu).  rows[b][i] = global qubit of row bit i.
-int qs_tile_row_orders(int n, const int *T, int nsub, const int (*qpos)[5], int (*rows)[7]);
+// and the shared-memory stores free of bank conflicts as far as possible
+// (qs_tile_layout.cu).  rows[b][i] = global qubit of row bit i.  wtile: the
+// write position of each tile bit (NULL: written where read); input_mode 0
+// for k_fused_tile's tile-order staging, 1 for k_batch's per-row loads.
+int qs_tile_row_orders(int n, const int *T, int nsub, const int (*qpos)[5], int (*rows)[7],
+                       const int *wtile = nullptr, int input_mode = 0);
 int qs_launch_tiled(qs_state *s, const qs_tiled_desc *d, int *err_dev);

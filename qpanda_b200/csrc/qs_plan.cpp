@@ -450,13 +450,10 @@ static void tiled_pass_desc(const qs_plan *P, size_t u, bool last, int mode, std
     d.has_rows = 1;
     bool ident = true;
     for (int q = 0; q < n; ++q) ident = ident && pos[q] == q;
-    // row orders: the plan's for the natural layout, chosen afresh for a
-    // permuted one (which tile bits are lowest - and so which lanes hold what -
-    // depends on the positions)
-    if (ident || qs_tile_row_orders(n, d.T, d.nsub, d.qpos, d.rows) != QS_OK) {
-        for (size_t b = 0; b < pp.count; ++b)
-            for (int i = 0; i < 7; ++i) d.rows[b][i] = pos[pp.rows[b][i]];
-    }
+    // row orders: the plan's (chosen for the natural layout, written in
+    // place); a permuted layout or write map gets its own at the end
+    for (size_t b = 0; b < pp.count; ++b)
+        for (int i = 0; i < 7; ++i) d.rows[b][i] = pos[pp.rows[b][i]];
     d.has_write = 0;
     if (last && ident) return;              // natural in, natural out: in place
     d.has_write = 1;
@@ -513,6 +510,10 @@ static void tiled_pass_desc(const qs_plan *P, size_t u, bool last, int mode, std
             if (!((tmask >> p) & 1)) { npos[at[p]] = 12 + i; d.wpos[i] = 12 + i; ++i; }
         d.wmode = 1;
     }
+    // which tile bits are lowest - and so which lanes read and write what -
+    // depends on the positions: choose the row orders for this layout
+    int rows[3][7];
+    if (qs_tile_row_orders(n, d.T, d.nsub, d.qpos, rows, d.wtile, 0) == QS_OK) memcpy(d.rows, rows, sizeof(rows));
     pos.swap(npos);
 }
 

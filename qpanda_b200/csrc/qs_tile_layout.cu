@@ -40,6 +40,17 @@ int glob_cost(unsigned lanes, int loc0, int loc1, bool vec)
     return (vec ? 16 : 32) * (32 >> k);
 }
 
+// 128-byte lines one warp-wide store of the last block touches, times the
+// stores per thread: lanes whose tile bits are written at positions 1..3
+// (0..3 without column pairs) share lines.
+int store_cost(unsigned lanes, const int *W, bool vec)
+{
+    int k = 0;
+    for (int b = 0; b < 12; ++b)
+        if (((lanes >> b) & 1) && W[b] <= 3 && (W[b] >= 1 || !vec)) ++k;
+    return (vec ? 16 : 32) * (32 >> (k > 5 ? 5 : k));
+}
+
 // Wavefronts of convert_tile's stores for block 0 with columns Q0 and row
 // bits 0..2 on tile bits t[0..2]: a lane's store lands at byte bits 2..6
 // (4-byte stores) or 3..6 (8-byte column pairs) given by the lane's tile bits
@@ -75,14 +86,19 @@ int scatter_cost(unsigned lanes, const int *Qn, const int *t)
 // Row orders (tile bits) for each block minimising the costs above, by
 // dynamic programming over the blocks; ascending order unless another order
 // is strictly cheaper.
-void choose_row_orders(const int *T, int nsub, const int (*Q)[5], int (*Cp)[7])
+void choose_row_orders(const int *T, int nsub, const int (*Q)[5], int (*Cp)[7], const int *W, int input_mode)
 {
     int loc0 = -1, loc1 = -1;
     for (int i = 0; i < 12; ++i) {
         if (T[i] == 0) loc0 = i;
         if (T[i] == 1) loc1 = i;
     }
-    const bool vecl = T[Q[nsub - 1][0]] == 0;
+    const bool vecl = W[Q[nsub - 1][0]] == 0, vec0 = T[Q[0][0]] == 0;
+    // block 0's input: tile-order staging converted per chunk (k_fused_tile),
+    // or one row per thread gathered from global memory (k_batch)
+    auto in_cost = [&](const RowCfg &c) {
+        return input_mode == 0 ? convert_cost(Q[0], c.t) : glob_cost(c.lanes, loc0, loc1, vec0);
+    };
     std::vector<RowCfg> cfg[kMaxSub];
     for (int b = 0; b < nsub; ++b) {
         const int *C = Cp[b];
@@ -102,7 +118,7 @@ void choose_row_orders(const int *T, int nsub, const int (*Q)[5], int (*Cp)[7])
     }
     std::vector<int> best[kMaxSub], from[kMaxSub];
     best[0].resize(cfg[0].size());
-    for (size_t i = 0; i < cfg[0].size(); ++i) best[0][i] = convert_cost(Q[0], cfg[0][i].t);
+    for (size_t i = 0; i < cfg[0].size(); ++i) best[0][i] = in_cost(cfg[0][i]);
     for (int b = 1; b < nsub; ++b) {
         // the previous block enters only through its lane set: keep its cheapest configuration per set
         std::vector<std::pair<unsigned, int>> sets;     // (lanes, configuration)
@@ -123,11 +139,11 @@ void choose_row_orders(const int *T, int nsub, const int (*Q)[5], int (*Cp)[7])
     const int last = nsub - 1;
     int sel[kMaxSub] = {0, 0, 0}, bestc = 1 << 30;
     for (size_t i = 0; i < cfg[last].size(); ++i) {
-        const int c = best[last][i] + glob_cost(cfg[last][i].lanes, loc0, loc1, vecl);
+        const int c = best[last][i] + store_cost(cfg[last][i].lanes, W, vecl);
         if (c < bestc) { bestc = c; sel[last] = (int)i; }
     }
     // cost of the ascending orders (configuration 0 everywhere)
-    int base = convert_cost(Q[0], cfg[0][0].t) + glob_cost(cfg[last][0].lanes, loc0, loc1, vecl);
+    int base = in_cost(cfg[0][0]) + store_cost(cfg[last][0].lanes, W, vecl);
     for (int b = 1; b < nsub; ++b) base += scatter_cost(cfg[b - 1][0].lanes, Q[b], cfg[b][0].t);
     if (bestc >= base) return;
     for (int b = last; b > 0; --b) sel[b - 1] = from[b][sel[b]];
@@ -146,11 +162,14 @@ void choose_row_orders(const int *T, int nsub, const int (*Q)[5], int (*Cp)[7])
 
 }  // namespace
 
-int qs_tile_row_orders(int n, const int *T, int nsub, const int (*qpos)[5], int (*rows)[7])
+int qs_tile_row_orders(int n, const int *T, int nsub, const int (*qpos)[5], int (*rows)[7], const int *wtile,
+                       int input_mode)
 {
     qs_tile::Layout L;
-    int r = qs_tile_layout_build(n, T, nsub, qpos, nullptr, &L);   // validates the pass
+    int r = qs_tile_layout_build(n, T, nsub, qpos, nullptr, &L, nullptr, wtile);   // validates the pass
     if (r) return r;
+    int W[12];
+    for (int i = 0; i < 12; ++i) W[i] = wtile ? wtile[i] : T[i];
     int local[64];
     for (int i = 0; i < 64; ++i) local[i] = -1;
     for (int i = 0; i < 12; ++i) local[T[i]] = i;
@@ -161,7 +180,7 @@ int qs_tile_row_orders(int n, const int *T, int nsub, const int (*qpos)[5], int 
         for (int p = 0, c = 0; p < 12; ++p)
             if (!(qm & (1u << p))) Cp[b][c++] = p;
     }
-    choose_row_orders(T, nsub, Q, Cp);
+    choose_row_orders(T, nsub, Q, Cp, W, input_mode);
     for (int b = 0; b < nsub; ++b)
         for (int i = 0; i < 7; ++i) rows[b][i] = T[Cp[b][i]];
     return QS_OK;
