@@ -65,6 +65,8 @@ def parse():
                          "(--qubits) applied once per tiled layout (in place, remap 1, remap 2) with its "
                          "pass structure, for per-launch profiling")
     ap.add_argument("--circuits", type=int, default=4096)
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="vqe-sweep: run with the default batch options instead of the autotuned ones")
     ap.add_argument("--requests", type=int, default=20000, help="requests workload: trace length")
     ap.add_argument("--every", type=int, default=10, help="requests workload: serve every k-th request")
     return ap.parse_args()
@@ -493,7 +495,12 @@ def run_vqe_sweep(args):
 
     sweep = circuits.vqe_sweep(args.circuits, SWEEP_SEED + rank)
     t0 = time.perf_counter()
-    opts, tune_ms = autotune_batch(sweep, stride=16)
+    if args.no_autotune:
+        from qpanda_b200.capi import BatchOpts
+        opts, tune_ms = BatchOpts(), None
+        check(lib().qs_batch_default_opts(C.byref(opts)))
+    else:
+        opts, tune_ms = autotune_batch(sweep, stride=16)
     tune_s = time.perf_counter() - t0
     t0 = time.perf_counter()
     b = Batch(sweep, opts=opts)

@@ -32,10 +32,14 @@ using namespace qs_tile;
 
 constexpr int kMaxZZ = 23;                        // circuits of up to 24 qubits
 constexpr uint32_t kLayoutBytes = (sizeof(Layout) + 15) & ~15u;
+constexpr uint32_t kLoadBytes = (sizeof(LoadMap) + 15) & ~15u;
 
-// Shared memory of the two shapes (as in qs_fused2.cu): with up to 2 blocks
-// per pass the staging rows live in the A region and three CTAs fit per SM;
-// with 3 blocks there is a separate staging area and two CTAs per SM.
+// Shared memory of the two shapes: with up to 2 blocks per pass the staging
+// area is the A region and three CTAs fit per SM - the tile arrives in tile
+// order (prefetch_tile_linear), each thread reads its own chunks to registers,
+// and after a barrier writes them at their rows and columns of A; with 3
+// blocks there is a separate staging area, each thread copies its own row
+// (prefetch_row), and two CTAs fit per SM.
 // Reductions (4 + 4 x kMaxZZ doubles) reuse the staging rows: they run only
 // when no copy into staging is in flight and no MMA reads A.
 template <int SUB>
@@ -46,7 +50,8 @@ struct BShape {
     static constexpr uint32_t kOffB = 2 * kA;
     static constexpr uint32_t kOffStage = kStageInA ? kOffA : kOffB + SUB * 2 * kB;
     static constexpr uint32_t kOffLayout = kOffB + SUB * 2 * kB + (kStageInA ? 0 : kStage);
-    static constexpr uint32_t kOffMisc = kOffLayout + kLayoutBytes;   // mbarrier 8, tmem 4, circuit 4
+    static constexpr uint32_t kOffLoad = kOffLayout + kLayoutBytes;            // tile-order shape only
+    static constexpr uint32_t kOffMisc = kOffLoad + (kStageInA ? kLoadBytes : 0);   // mbarrier 8, tmem 4, circuit 4
     static constexpr uint32_t kSmemBytes = kOffMisc + 16;
     static constexpr uint32_t kOffRed = kOffStage;
     static_assert(kCtasPerSm * (kSmemBytes + 1024) <= 228 * 1024, "resident CTAs per SM");
@@ -58,6 +63,7 @@ struct BatchCirc {
     float *amp;                  // 2^nq_eff complex64
     const uint16_t *mats;        // the circuit's blocks, [2][64][64] BF16 each
     const Layout *layouts;       // its passes (Layout::pad = first block of the pass)
+    const LoadMap *loads;        // their tile-order copy maps
     double *zz;                  // nq - 1 outputs
     int32_t npass, nq, nq_eff, pad;
 };
@@ -131,6 +137,11 @@ __global__ void __launch_bounds__(kThreads, BShape<SUB>::kCtasPerSm) k_batch(Bat
                 const uint32_t *src = reinterpret_cast<const uint32_t *>(C.layouts + p);
                 uint32_t *dst = reinterpret_cast<uint32_t *>(&L);
                 for (int i = tid; i < (int)(sizeof(Layout) / 4); i += kThreads) dst[i] = src[i];
+                if constexpr (S::kStageInA) {
+                    const uint32_t *ls = reinterpret_cast<const uint32_t *>(C.loads + p);
+                    uint32_t *ld = reinterpret_cast<uint32_t *>(smem + S::kOffLoad);
+                    for (int i = tid; i < (int)(sizeof(LoadMap) / 4); i += kThreads) ld[i] = ls[i];
+                }
             }
             __syncthreads();
             load_b(smem + S::kOffB, C.mats + (size_t)L.pad * 2 * 64 * 64, L.nsub);
@@ -154,27 +165,63 @@ __global__ void __launch_bounds__(kThreads, BShape<SUB>::kCtasPerSm) k_batch(Bat
             double acc_out = 0;
             const uint64_t step = tile_base(1, L);
             uint64_t tbase = 0;                       // tile_base(0)
-            if (p > 0) prefetch_row(C.amp, tbase | gC0, L, stage, row);
+            const LoadMap &M = *reinterpret_cast<const LoadMap *>(smem + S::kOffLoad);
+            ChunkBase cb{0, 0, 0};
+            if constexpr (S::kStageInA) cb = chunk_base(M, tid);
+            if (p > 0) {
+                if constexpr (S::kStageInA) prefetch_tile_linear(C.amp, tbase, M, stage, cb.g, tid);
+                else prefetch_row(C.amp, tbase | gC0, L, stage, row);
+            }
             for (uint64_t tile = 0; tile < tiles; ++tile) {
                 const uint64_t tnext = tile_base_advance(tbase, step, L.tmask);
-                float x[64];
                 if (p == 0) {
                     // |0...0>: amplitude 0 is tile 0, the row with no row bits, column 0
+                    float x[64];
 #pragma unroll
                     for (int e = 0; e < 64; ++e) x[e] = 0.f;
                     if (tile == 0 && gC0 == 0) x[0] = 1.f;
+#pragma unroll
+                    for (int j = 0; j < 32; ++j) a_store_pair(aHi, aLo, row, j, x[2 * j], x[2 * j + 1]);
+                } else if constexpr (S::kStageInA) {
+                    // this thread's chunks of the tile (tile order, in the A
+                    // region) to registers; once every thread has its chunks,
+                    // their BF16 split at their rows and columns of A
+                    asm volatile("cp.async.wait_group 0;" ::: "memory");
+                    float4 v[16];
+#pragma unroll
+                    for (int k = 0; k < 16; ++k)
+                        asm volatile("ld.shared.v4.f32 {%0,%1,%2,%3}, [%4];"
+                                     : "=f"(v[k].x), "=f"(v[k].y), "=f"(v[k].z), "=f"(v[k].w)
+                                     : "r"(stage + (uint32_t)(128 * k + tid) * 16u));
+                    __syncthreads();
+#pragma unroll
+                    for (int k = 0; k < 16; ++k) {
+                        const uint32_t r0 = cb.r ^ M.rk[k], j0 = cb.j ^ M.jk[k];
+                        uint32_t h0, l0, h1, l1;
+                        split_pair(v[k].x * scale, v[k].y * scale, h0, l0);
+                        split_pair(v[k].z * scale, v[k].w * scale, h1, l1);
+                        if (M.pair) {
+                            const uint32_t off = a_offset(r0, j0);
+                            *reinterpret_cast<uint2 *>(aHi + off) = make_uint2(h0, h1);
+                            *reinterpret_cast<uint2 *>(aLo + off) = make_uint2(l0, l1);
+                        } else {
+                            const uint32_t o0 = a_offset(r0, j0), o1 = a_offset(r0 | M.dr, j0 | M.dj);
+                            *reinterpret_cast<uint32_t *>(aHi + o0) = h0;
+                            *reinterpret_cast<uint32_t *>(aLo + o0) = l0;
+                            *reinterpret_cast<uint32_t *>(aHi + o1) = h1;
+                            *reinterpret_cast<uint32_t *>(aLo + o1) = l1;
+                        }
+                    }
                 } else {
                     asm volatile("cp.async.wait_group 0;" ::: "memory");
+                    float x[64];
                     read_stage_row(stage, row, x);
-                    if constexpr (S::kStageInA)
-                        __syncthreads();      // every staging row is read before A overwrites them
-                    else if (tile + 1 < tiles)
-                        prefetch_row(C.amp, tnext | gC0, L, stage, row);
+                    if (tile + 1 < tiles) prefetch_row(C.amp, tnext | gC0, L, stage, row);
 #pragma unroll
                     for (int e = 0; e < 64; ++e) x[e] *= scale;
-                }
 #pragma unroll
-                for (int j = 0; j < 32; ++j) a_store_pair(aHi, aLo, row, j, x[2 * j], x[2 * j + 1]);
+                    for (int j = 0; j < 32; ++j) a_store_pair(aHi, aLo, row, j, x[2 * j], x[2 * j + 1]);
+                }
 
                 for (int b = 0; b < L.nsub; ++b) {
                     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -186,8 +233,9 @@ __global__ void __launch_bounds__(kThreads, BShape<SUB>::kCtasPerSm) k_batch(Bat
                     phase ^= 1;
                     if (__syncthreads_or(!ok)) { failed = true; break; }
                     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-                    if (S::kStageInA && p > 0 && b + 1 == L.nsub && tile + 1 < tiles)
-                        prefetch_row(C.amp, tnext | gC0, L, stage, row);   // the MMAs are done with A
+                    if constexpr (S::kStageInA)
+                        if (p > 0 && b + 1 == L.nsub && tile + 1 < tiles)
+                            prefetch_tile_linear(C.amp, tnext, M, stage, cb.g, tid);   // the MMAs are done with A
                     uint32_t y[4][16];
 #pragma unroll
                     for (int q = 0; q < 4; ++q) tmem_ld16(taddr + 16 * q, y[q]);
@@ -285,6 +333,7 @@ struct qs_batch {
     void *d_states = nullptr;            // all states
     void *d_mats = nullptr;              // all block matrices
     void *d_layouts = nullptr;           // layouts of the distinct plan structures
+    void *d_loads = nullptr;             // their tile-order copy maps
     void *d_circ = nullptr;              // BatchCirc[n]
     void *d_order = nullptr;
     double *d_zz = nullptr;
@@ -301,7 +350,8 @@ void batch_free(qs_batch *B)
 {
     if (B->graph_exec) cudaGraphExecDestroy(B->graph_exec);
     if (B->graph) cudaGraphDestroy(B->graph);
-    for (void *p : {B->d_states, B->d_mats, B->d_layouts, B->d_circ, B->d_order, (void *)B->d_zz, (void *)B->d_head})
+    for (void *p : {B->d_states, B->d_mats, B->d_layouts, B->d_loads, B->d_circ, B->d_order, (void *)B->d_zz,
+                    (void *)B->d_head})
         if (p) cudaFree(p);
     delete B;
 }
@@ -403,20 +453,24 @@ extern "C" int qs_batch_create(int n_circ, const int *n_qubits, const qs_gate *g
     }
     // ---- device memory
     std::vector<Layout> layouts;                      // per proto, concatenated
+    std::vector<LoadMap> loads;                       // their tile-order copy maps
     std::vector<size_t> layout_first(protos.size());
+    const int input_mode = o.max_sub <= 2 ? 0 : 1;   // tile-order staging, or per-row copies
     for (size_t pi = 0; pi < protos.size() && !r; ++pi) {
         layout_first[pi] = layouts.size();
         const qs_plan *pp = protos[pi];
         for (const PlanPass &pass : pp->passes) {
             Layout L;
+            LoadMap M;
             int qpos[3][5];
             for (size_t b = 0; b < pass.count; ++b)
                 for (int j = 0; j < 5; ++j) qpos[b][j] = pp->blocks[pass.first + b].q[j];
             int rows[3][7];
-            if ((r = qs_tile_row_orders(pp->n, pass.T, (int)pass.count, qpos, rows, nullptr, 1))) break;
-            if ((r = qs_tile_layout_build(pp->n, pass.T, (int)pass.count, qpos, rows, &L))) break;
+            if ((r = qs_tile_row_orders(pp->n, pass.T, (int)pass.count, qpos, rows, nullptr, input_mode))) break;
+            if ((r = qs_tile_layout_build(pp->n, pass.T, (int)pass.count, qpos, rows, &L, &M))) break;
             L.pad = (int32_t)pass.first;
             layouts.push_back(L);
+            loads.push_back(M);
         }
     }
     std::vector<size_t> mat_off(n_circ);
@@ -440,6 +494,7 @@ extern "C" int qs_batch_create(int n_circ, const int *n_qubits, const qs_gate *g
         e = cudaMalloc(&B->d_states, B->state_bytes);
         if (e == cudaSuccess) e = cudaMalloc(&B->d_mats, std::max<size_t>(hm.size() * 2, 16));
         if (e == cudaSuccess) e = cudaMalloc(&B->d_layouts, std::max<size_t>(layouts.size() * sizeof(Layout), 16));
+        if (e == cudaSuccess) e = cudaMalloc(&B->d_loads, std::max<size_t>(loads.size() * sizeof(LoadMap), 16));
         if (e == cudaSuccess) e = cudaMalloc(&B->d_circ, sizeof(BatchCirc) * n_circ);
         if (e == cudaSuccess) e = cudaMalloc(&B->d_order, sizeof(int32_t) * n_circ);
         if (e == cudaSuccess) e = cudaMalloc((void **)&B->d_zz, std::max<size_t>(B->zz_count, 1) * sizeof(double));
@@ -447,6 +502,8 @@ extern "C" int qs_batch_create(int n_circ, const int *n_qubits, const qs_gate *g
         if (e == cudaSuccess) e = cudaMemcpy(B->d_mats, hm.data(), hm.size() * 2, cudaMemcpyHostToDevice);
         if (e == cudaSuccess && !layouts.empty())
             e = cudaMemcpy(B->d_layouts, layouts.data(), layouts.size() * sizeof(Layout), cudaMemcpyHostToDevice);
+        if (e == cudaSuccess && !loads.empty())
+            e = cudaMemcpy(B->d_loads, loads.data(), loads.size() * sizeof(LoadMap), cudaMemcpyHostToDevice);
         if (e != cudaSuccess) r = qs_cuda_fail(e, "qs_batch_create: device memory");
     }
     if (!r) {
@@ -456,6 +513,7 @@ extern "C" int qs_batch_create(int n_circ, const int *n_qubits, const qs_gate *g
             bc.amp = reinterpret_cast<float *>(static_cast<char *>(B->d_states) + B->amp_off[c]);
             bc.mats = static_cast<const uint16_t *>(B->d_mats) + mat_off[c];
             bc.layouts = static_cast<const Layout *>(B->d_layouts) + layout_first[proto_id[c]];
+            bc.loads = static_cast<const LoadMap *>(B->d_loads) + layout_first[proto_id[c]];
             bc.zz = B->d_zz + B->zz_off[c];
             bc.npass = (int32_t)pp->passes.size();
             bc.nq = B->nq[c];
