@@ -21,9 +21,10 @@
 //      lane's mbarrier; every thread waits, loads its 64 FP32 results from
 //      TMEM, and either scatters them as BF16 hi/lo into the next block's A
 //      layout (one XOR per result gives its offset there), or - after the last
-//      block - stores them to HBM in place.
+//      block - stores them to HBM: in place, or - for a remapping plan - into
+//      the other buffer at the positions the pass's StoreMap gives.
 // One CTA per SM holds three such lanes (two for passes of three blocks),
-// each with its own A buffers, staging rows, mbarrier, named barrier and 64
+// each with its own A buffers, staging area, mbarrier, named barrier and 64
 // TMEM columns; the blocks' B operands are loaded once per CTA and shared.
 // Each lane's tile is a serial chain (copy, split, MMA, wait, scatter, MMA,
 // wait, store); three independent lanes per SM overlap each other's chains,
