@@ -605,9 +605,17 @@ extern "C" int qs_plan_apply_range(qs_state *s, qs_plan *P, size_t first, size_t
             if ((r = qs_dev_alloc(s, s->amp_bytes(), &p))) return r;
             s->spare = p;
         }
-        std::vector<qs_tiled_desc> descs;
-        std::vector<int> dst;
-        if ((r = qs_plan_tiled_schedule(P, s->n, first, count, remap, descs, dst))) return r;
+        // the schedule (host work of ~0.5 ms per remapped pass) is kept with
+        // the plan for its next application over the same range
+        if (P->sched_remap != remap || P->sched_first != first || P->sched_count != count) {
+            P->sched_remap = -1;
+            if ((r = qs_plan_tiled_schedule(P, s->n, first, count, remap, P->sched, P->sched_dst))) return r;
+            P->sched_remap = remap;
+            P->sched_first = first;
+            P->sched_count = count;
+        }
+        std::vector<qs_tiled_desc> descs(P->sched);
+        const std::vector<int> &dst = P->sched_dst;
         void *buf[2] = {s->amp, s->spare};
         for (size_t u = first; u < first + count; ++u) {
             const PlanPass &pp = P->passes[u];

@@ -36,6 +36,11 @@ struct qs_plan {
     void *mats = nullptr;                // [blocks][2][64][64] bf16
     cudaStream_t mats_stream = nullptr;  // stream-ordered mats: freed with cudaFreeAsync on it
     bool mats_async = false;
+    // the last tiled schedule (qs_plan_tiled_schedule) and what it was for
+    std::vector<struct qs_tiled_desc> sched;
+    std::vector<int> sched_dst;
+    size_t sched_first = 0, sched_count = 0;
+    int sched_remap = -1;
 };
 
 
