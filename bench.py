@@ -53,6 +53,8 @@ def parse():
                     help="tiled passes: qubits 0..low-1 in every tile (contiguous runs of 2^low amplitudes)")
     ap.add_argument("--remap", type=int, default=1, choices=[0, 1],
                     help="tiled passes: 1 = contiguous tile writes through a second state-size buffer")
+    ap.add_argument("--tpr", type=int, default=1, choices=[1, 2],
+                    help="tiled passes: threads per tile row (1: 128 per lane, 2: 256, 16 columns each)")
     ap.add_argument("--qubits", type=int, default=N_QUBITS)
     ap.add_argument("--depth", type=int, default=DEPTH)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -310,7 +312,8 @@ def run_b200(args):
     sv = StateVector(n, "c64")
     h = sv.handle
     remap = args.kernel == "tiled" and args.remap == 1
-    plan = FusionPlan(n, gates, kernel=args.kernel, remap=remap, low_qubits=args.low, max_sub=args.max_sub)
+    plan = FusionPlan(n, gates, kernel=args.kernel, remap=remap, low_qubits=args.low, max_sub=args.max_sub,
+                      threads_per_row=args.tpr)
     plan.remap = remap
     nb = plan.num_launches()
     nblocks = plan.num_blocks()
@@ -367,7 +370,8 @@ def run_b200(args):
     if rank == 0 and n >= 30:
         nf = 30
         gf = workload(nf, depth)
-        pf = FusionPlan(nf, gf, kernel=args.kernel, remap=remap, low_qubits=args.low, max_sub=args.max_sub)
+        pf = FusionPlan(nf, gf, kernel=args.kernel, remap=remap, low_qubits=args.low, max_sub=args.max_sub,
+                        threads_per_row=args.tpr)
         a = StateVector(nf, "c64")
         pf.apply(a)
         pf.status(a)
@@ -392,11 +396,13 @@ def run_b200(args):
     pin_u.numpy()[:] = rng.uniform(size=SHOTS * n)
     pin_o = torch.empty(SHOTS, dtype=torch.int64).pin_memory()
     e2e_steps = max(1, min(args.steps, 2))
-    barrier(ws)
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    for _ in range(e2e_steps):
+
+    phase_s = {"reset": 0.0, "plan_build": 0.0, "circuit": 0.0, "sample": 0.0}
+
+    def e2e_step():
+        c0 = time.perf_counter()
         check(L.qs_reset_zero(h))
+        c1 = time.perf_counter()
         if path == "fused":
             from qpanda_b200.capi import PlanOpts
             ph, o = C.c_void_p(), PlanOpts()
@@ -407,15 +413,33 @@ def run_b200(args):
             o.low_qubits = args.low
             if args.kernel == "tiled":
                 o.max_sub = args.max_sub
+                o.threads_per_row = args.tpr
             check(L.qs_plan_create_ex(n, C.c_void_p(pin_g.data_ptr()), ng, C.byref(o), C.byref(ph)))
+            c2 = time.perf_counter()
             check(L.qs_plan_apply(h, ph))
         else:
+            c2 = time.perf_counter()
             check(L.qs_gates_apply(h, C.c_void_p(pin_g.data_ptr()), ng))
+        check(L.qs_synchronize(h))
+        c3 = time.perf_counter()
         check(L.qs_sample(h, qs.ctypes.data_as(C.POINTER(C.c_int)), n,
                           C.cast(C.c_void_p(pin_u.data_ptr()), C.POINTER(C.c_double)), SHOTS,
                           C.cast(C.c_void_p(pin_o.data_ptr()), C.POINTER(C.c_uint64))))
         if path == "fused":
             L.qs_plan_destroy(ph)
+        c4 = time.perf_counter()
+        for k, v in (("reset", c1 - c0), ("plan_build", c2 - c1), ("circuit", c3 - c2), ("sample", c4 - c3)):
+            phase_s[k] += v
+
+    # one untimed step first: the sampler's scratch and first kernel loads
+    e2e_step()
+    for k in phase_s:
+        phase_s[k] = 0.0
+    barrier(ws)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        e2e_step()
     torch.cuda.synchronize()
     e2e_s = max_over_ranks((time.perf_counter() - t0) / e2e_steps, ws, device=f"cuda:{local}")
 
@@ -436,7 +460,7 @@ def run_b200(args):
             "data": "synthetic",
             "config": {"workload": f"random-circuit-{n}q-depth{depth}-c64", "qubits": n, "depth": depth,
                        "gates": ng, "fused_blocks": nblocks, "fused_passes": nb, "kernel": args.kernel,
-                       "remap": remap, "low_qubits": args.low, "max_sub": args.max_sub, "device_bytes": (amp_b << n) * (2 if remap and path == "fused" else 1),
+                       "remap": remap, "low_qubits": args.low, "max_sub": args.max_sub, "threads_per_row": args.tpr, "device_bytes": (amp_b << n) * (2 if remap and path == "fused" else 1),
                        "iswap_frac": ISWAP_FRAC, "seed": SEED, "path": path,
                        "state_bytes": amp_b << n, "l2": "inputs larger than L2 (32 GiB state), no flush",
                        "parallelism": f"replicas x{ws}"},
@@ -453,7 +477,8 @@ def run_b200(args):
             "e2e": {"value": ws / e2e_s, "unit": "circuits/s",
                     "h2d_bytes_per_step": int(gates.nbytes + SHOTS * n * 8),
                     "d2h_bytes_per_step": SHOTS * 8, "shots": SHOTS,
-                    "includes": "plan build on the host, circuit, 1024-shot sampling"},
+                    "includes": "plan build on the host, circuit, 1024-shot sampling",
+                    "phase_ms": {k: 1e3 * v / e2e_steps for k, v in phase_s.items()}},
             "gpu_launches": launches,
             "clocks": clk,
         }
@@ -859,7 +884,7 @@ def run_passes(args):
     stream = torch.cuda.current_stream()
     res = {}
     for remap in (0, 1, 2):
-        p = FusionPlan(n, gates, remap=remap, low_qubits=args.low, max_sub=args.max_sub)
+        p = FusionPlan(n, gates, remap=remap, low_qubits=args.low, max_sub=args.max_sub, threads_per_row=args.tpr)
         p.apply(sv)
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)

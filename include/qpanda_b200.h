@@ -224,6 +224,8 @@ typedef struct qs_plan_opts {
                               qs_destroy or qs_release_spare) and the last writes the natural order
                               back; 2 = as 1, but each pass writes the layout in which the next pass's
                               tiles are contiguous (loads stream, stores scatter; measured slower) */
+    int threads_per_row;   /* tiled passes: 1 = each of a lane's 128 threads owns a row of the tile (default);
+                              2 = 256 threads per lane, two per row, each with 16 of its 32 columns */
 } qs_plan_opts;
 /* Defaults: 5-qubit blocks, tiled passes of 12 qubits with up to 2 blocks
  * (a pass of 3 blocks saves a pass but runs on a kernel with fewer resident

@@ -281,7 +281,7 @@ class StateVector:
 
 class PlanOpts(C.Structure):
     _fields_ = [("block_qubits", C.c_int), ("tile_qubits", C.c_int), ("max_sub", C.c_int),
-                ("low_qubits", C.c_int), ("kernel", C.c_int), ("remap", C.c_int)]
+                ("low_qubits", C.c_int), ("kernel", C.c_int), ("remap", C.c_int), ("threads_per_row", C.c_int)]
 
 
 PLAN_SINGLE, PLAN_TILED = 1, 2
@@ -295,7 +295,7 @@ class FusionPlan:
     state (twice the memory; faster passes on large states); remap=2: the
     next pass's tiles contiguous instead (qs_plan_opts.remap)."""
 
-    def __init__(self, n, gates, max_k=5, kernel="tiled", max_sub=2, low_qubits=3, remap=False):
+    def __init__(self, n, gates, max_k=5, kernel="tiled", max_sub=2, low_qubits=3, remap=False, threads_per_row=1):
         g = np.ascontiguousarray(gates, dtype=GATE_DTYPE)
         self._keep = g
         h = C.c_void_p()
@@ -306,6 +306,7 @@ class FusionPlan:
             check(lib().qs_plan_default_opts(C.byref(o)))
             o.block_qubits, o.max_sub, o.low_qubits = int(max_k), int(max_sub), int(low_qubits)
             o.remap = int(remap)
+            o.threads_per_row = int(threads_per_row)
             check(lib().qs_plan_create_ex(int(n), g.ctypes.data, g.size, C.byref(o), C.byref(h)))
         self._h = h
         self.n = int(n)

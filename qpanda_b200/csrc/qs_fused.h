@@ -51,6 +51,7 @@ struct qs_tiled_desc {
     const void *amp_in;
     void *amp_out;
     size_t first_block;          // the plan's index of block 0 of the pass (host bookkeeping)
+    int threads_per_row;         // 1: 128 threads per lane, a row each; 2: 256, half a row each
 };
 
 int qs_tiled_grid(const qs_state *s);

@@ -43,17 +43,18 @@ namespace {
 
 using namespace qs_tile;
 
-template <int SUB>
+template <int SUB, int TPR>
 struct Shape {
     static constexpr int kLanes = SUB <= 2 ? 3 : 2;
-    static constexpr int kCtaThreads = kThreads * kLanes;
+    static constexpr int kLaneThreads = kThreads * TPR;       // 128 rows, TPR threads per row
+    static constexpr int kCtaThreads = kLaneThreads * kLanes;
     static constexpr uint32_t kOffB = 0;                          // B hi/lo per block
     static constexpr uint32_t kLaneBytes = 2 * kA + kStage;       // A hi, A lo, staging rows
     static constexpr uint32_t kOffLane = kOffB + SUB * 2 * kB;
     static constexpr uint32_t kOffMisc = kOffLane + kLanes * kLaneBytes;
     // misc: one mbarrier per lane (8 B each, 32 reserved), tmem address (4), scale (4)
     static constexpr uint32_t kSmemBytes = kOffMisc + 48;
-    static constexpr uint32_t kCols = kLanes <= 2 ? 128 : 256;  // TMEM columns (power of two >= 64 x lanes)
+    static constexpr uint32_t kCols = kLanes <= 2 ? 128 : 256;    // TMEM columns (power of two >= 64 x lanes)
     static_assert(kSmemBytes + 1024 <= 228 * 1024, "one CTA per SM");
     static_assert(kLanes * kTmemCols <= kCols, "TMEM columns per lane");
     static_assert((kOffLane & 1023) == 0 && (kLaneBytes & 1023) == 0, "swizzled operands are 1024-byte aligned");
@@ -73,21 +74,21 @@ struct TileParams {
     double *out_parts;
 };
 
-__device__ __forceinline__ void lane_bar(int id)
+__device__ __forceinline__ void lane_bar(int id, int nthreads)
 {
-    asm volatile("bar.sync %0, 128;" :: "r"(id) : "memory");
+    asm volatile("bar.sync %0, %1;" :: "r"(id), "r"(nthreads) : "memory");
 }
 
-// Named-barrier OR over the lane's 128 threads.
-__device__ __forceinline__ bool lane_bar_or(int id, bool v)
+// Named-barrier OR over the lane's threads.
+__device__ __forceinline__ bool lane_bar_or(int id, int nthreads, bool v)
 {
     uint32_t r;
     asm volatile(
         "{\n\t.reg .pred p, q;\n\t"
         "setp.ne.u32 p, %1, 0;\n\t"
-        "bar.red.or.pred q, %2, 128, p;\n\t"
+        "bar.red.or.pred q, %2, %3, p;\n\t"
         "selp.u32 %0, 1, 0, q;\n\t}\n"
-        : "=r"(r) : "r"((uint32_t)v), "r"(id) : "memory");
+        : "=r"(r) : "r"((uint32_t)v), "r"(id), "r"(nthreads) : "memory");
     return r != 0;
 }
 
@@ -122,13 +123,16 @@ __device__ __forceinline__ void load_b_scaled(uint8_t *dst, const uint16_t *mat,
     }
 }
 
-template <int SUB>
-__global__ void __launch_bounds__(Shape<SUB>::kCtaThreads, 1) k_fused_tile(const float *amp, float *out, TileParams P)
+template <int SUB, int TPR>
+__global__ void __launch_bounds__(Shape<SUB, TPR>::kCtaThreads, 1) k_fused_tile(const float *amp, float *out,
+                                                                              TileParams P)
 {
-    using S = Shape<SUB>;
+    using S = Shape<SUB, TPR>;
+    constexpr int kQ = 4 / TPR;                // 16-column TMEM loads per thread per block
     extern __shared__ __align__(1024) uint8_t smem[];
     const int tid = threadIdx.x, warp = tid >> 5;
-    const int lane = tid >> 7, ltid = tid & (kThreads - 1), lwarp = ltid >> 5;
+    const int lane = tid / S::kLaneThreads, ltid = tid % S::kLaneThreads, lwarp = (ltid >> 5) & 3;
+    const int half = TPR == 2 ? ltid >> 7 : 0;   // which 16 of a row's 32 columns (two threads per row)
     if (smem_u32(smem) & 1023u) {             // swizzled operands need 1024-byte alignment
         if (tid == 0) atomicExch(P.err, 2);
         return;
@@ -170,7 +174,7 @@ __global__ void __launch_bounds__(Shape<SUB>::kCtaThreads, 1) k_fused_tile(const
     const uint32_t tmem_base = *tmem_holder;
     const uint32_t tmem = tmem_base + (uint32_t)(lane * kTmemCols);      // this lane's 64 columns
 
-    const int row = ltid;
+    const int row = ltid & (kThreads - 1);
     uint64_t gCl = 0;
 #pragma unroll
     for (int b = 0; b < 7; ++b) gCl |= (uint64_t)((row >> b) & 1) << L.cl_glob[b];
@@ -185,49 +189,54 @@ __global__ void __launch_bounds__(Shape<SUB>::kCtaThreads, 1) k_fused_tile(const
     bool failed = false;
     double acc_in = 0, acc_out = 0;
 
-    const ChunkBase cb = chunk_base(P.M, ltid);
+    const ChunkBase cb = chunk_base<TPR>(P.M, ltid);
     const uint64_t stride = (uint64_t)gridDim.x * S::kLanes;
     uint64_t tile = (uint64_t)blockIdx.x * S::kLanes + lane;
     const uint64_t step = tile_base(stride, L);
     uint64_t tbase = tile_base(tile, L);
-    if (tile < P.tiles) prefetch_tile_linear(amp, tbase, P.M, stage, cb.g, ltid);
+    const int j0 = 16 * half;                 // this thread's columns: all 32, or 16 of them from j0
+    if (tile < P.tiles) prefetch_tile_linear<TPR>(amp, tbase, P.M, stage, cb.g, ltid);
     for (; tile < P.tiles; tile += stride) {
         const uint64_t tnext = tile_base_advance(tbase, step, L.tmask);
         // ---- block 0 input: this thread's staged chunks -> A; then its
         // chunks of the lane's next tile (its own staging slots, just read)
         asm volatile("cp.async.wait_group 0;" ::: "memory");
-        const float ss = convert_tile(stage, aHi, aLo, P.M, cb, ltid);
-        if (want_in) acc_in += (double)ss;
-        if (tile + stride < P.tiles) prefetch_tile_linear(amp, tnext, P.M, stage, cb.g, ltid);
+        {
+            uint32_t hv[16 / TPR][2], lv[16 / TPR][2];
+            const float ss = convert_load<TPR>(stage, ltid, hv, lv);
+            if (want_in) acc_in += (double)ss;
+            convert_store<TPR>(aHi, aLo, P.M, cb, hv, lv);
+        }
+        if (tile + stride < P.tiles) prefetch_tile_linear<TPR>(amp, tnext, P.M, stage, cb.g, ltid);
 
         for (int b = 0; b < L.nsub; ++b) {
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-            lane_bar(bar_id);
+            lane_bar(bar_id, S::kLaneThreads);
             if (ltid == 0)
                 issue_block_mma(tmem, a_hi, a_lo, smem_u32(smem + S::kOffB + (2 * b) * kB),
                                 smem_u32(smem + S::kOffB + (2 * b + 1) * kB), mb);
             const bool ok = mbar_wait(mb, phase);
             phase ^= 1;
-            if (lane_bar_or(bar_id, !ok)) { failed = true; break; }
+            if (lane_bar_or(bar_id, S::kLaneThreads, !ok)) { failed = true; break; }
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            uint32_t y[4][16];
+            uint32_t y[kQ][16];
 #pragma unroll
-            for (int q = 0; q < 4; ++q) tmem_ld16(taddr + 16 * q, y[q]);
+            for (int q = 0; q < kQ; ++q) tmem_ld16(taddr + 2 * j0 + 16 * q, y[q]);
             asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
             if (b + 1 < L.nsub) {
                 // results become the next block's A operand
                 const uint32_t tp = scat_t[b];
 #pragma unroll
-                for (int q = 0; q < 4; ++q)
+                for (int q = 0; q < kQ; ++q)
 #pragma unroll
                     for (int e = 0; e < 8; ++e)
-                        a_store_at(aHi, aLo, tp ^ L.scat[b][8 * q + e], __uint_as_float(y[q][2 * e]),
+                        a_store_at(aHi, aLo, tp ^ L.scat[b][j0 + 8 * q + e], __uint_as_float(y[q][2 * e]),
                                    __uint_as_float(y[q][2 * e + 1]));
             } else {
                 float t = 0.f;
                 const uint64_t obase = store_base(tile, tbase, P.W) | gCl;
 #pragma unroll
-                for (int q = 0; q < 4; ++q) {
+                for (int q = 0; q < kQ; ++q) {
 #pragma unroll
                     for (int e = 0; e < 16; ++e) t = fmaf(__uint_as_float(y[q][e]), __uint_as_float(y[q][e]), t);
                     if (L.vecl) {
@@ -235,13 +244,13 @@ __global__ void __launch_bounds__(Shape<SUB>::kCtaThreads, 1) k_fused_tile(const
                         for (int e = 0; e < 8; e += 2) {
                             float4 v = make_float4(__uint_as_float(y[q][2 * e]), __uint_as_float(y[q][2 * e + 1]),
                                                    __uint_as_float(y[q][2 * e + 2]), __uint_as_float(y[q][2 * e + 3]));
-                            *reinterpret_cast<float4 *>(out + 2 * (obase | L.gl[8 * q + e])) = v;
+                            *reinterpret_cast<float4 *>(out + 2 * (obase | L.gl[j0 + 8 * q + e])) = v;
                         }
                     } else {
 #pragma unroll
                         for (int e = 0; e < 8; ++e) {
                             float2 v = make_float2(__uint_as_float(y[q][2 * e]), __uint_as_float(y[q][2 * e + 1]));
-                            *reinterpret_cast<float2 *>(out + 2 * (obase | L.gl[8 * q + e])) = v;
+                            *reinterpret_cast<float2 *>(out + 2 * (obase | L.gl[j0 + 8 * q + e])) = v;
                         }
                     }
                 }
@@ -291,18 +300,19 @@ __global__ void __launch_bounds__(Shape<SUB>::kCtaThreads, 1) k_fused_tile(const
 template <int SUB>
 uint64_t grid_for(const qs_state *s)
 {
-    constexpr int lanes = Shape<SUB>::kLanes;
+    constexpr int lanes = Shape<SUB, 1>::kLanes;
     const uint64_t tiles = s->N >> 12, need = (tiles + lanes - 1) / lanes;
     return need < QS_SM_COUNT ? need : QS_SM_COUNT;
 }
 
-template <int SUB>
+template <int SUB, int TPR>
 int launch(qs_state *s, const float *in, float *out, TileParams &P)
 {
-    using S = Shape<SUB>;
-    QS_CUDA_TRY(cudaFuncSetAttribute(k_fused_tile<SUB>, cudaFuncAttributeMaxDynamicSharedMemorySize, S::kSmemBytes));
+    using S = Shape<SUB, TPR>;
+    QS_CUDA_TRY(cudaFuncSetAttribute(k_fused_tile<SUB, TPR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     S::kSmemBytes));
     const unsigned grid = (unsigned)grid_for<SUB>(s);
-    k_fused_tile<SUB><<<grid, S::kCtaThreads, S::kSmemBytes, s->stream>>>(in, out, P);
+    k_fused_tile<SUB, TPR><<<grid, S::kCtaThreads, S::kSmemBytes, s->stream>>>(in, out, P);
     QS_LAUNCH_CHECK("k_fused_tile");
     return QS_OK;
 }
@@ -356,5 +366,7 @@ int qs_launch_tiled(qs_state *s, const qs_tiled_desc *d, int *err_dev)
         return qs_fail(QS_ERR_ARG, "tiled pass: set both buffers, and distinct, or neither");
     if (d->has_write && !d->amp_out)
         return qs_fail(QS_ERR_ARG, "tiled pass: remapped results need a separate output buffer");
-    return d->nsub <= 2 ? launch<2>(s, in, out, P) : launch<3>(s, in, out, P);
+    if (d->threads_per_row == 2)
+        return d->nsub <= 2 ? launch<2, 2>(s, in, out, P) : launch<3, 2>(s, in, out, P);
+    return d->nsub <= 2 ? launch<2, 1>(s, in, out, P) : launch<3, 1>(s, in, out, P);
 }

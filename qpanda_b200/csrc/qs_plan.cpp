@@ -278,6 +278,7 @@ extern "C" int qs_plan_create(int n, const qs_gate *gates, size_t count, int max
     o.low_qubits = 0;
     o.kernel = QS_PLAN_SINGLE;
     o.remap = 0;
+    o.threads_per_row = 1;
     return qs_plan_create_ex(n, gates, count, &o, out);
 }
 
@@ -290,6 +291,7 @@ extern "C" int qs_plan_default_opts(qs_plan_opts *o)
     o->low_qubits = 3;
     o->kernel = QS_PLAN_TILED;
     o->remap = 0;
+    o->threads_per_row = 1;
     return QS_OK;
 }
 
@@ -312,6 +314,8 @@ extern "C" int qs_plan_create_ex(int n, const qs_gate *gates, size_t count, cons
         return qs_fail(QS_ERR_UNSUPPORTED,
                        "qs_plan_create: tiled passes need tile_qubits 12, max_sub 1..3, low_qubits 1..5");
     if (o.remap < 0 || o.remap > 2) return qs_fail(QS_ERR_ARG, "qs_plan_create: remap must be 0, 1 or 2");
+    if (o.threads_per_row != 1 && o.threads_per_row != 2)
+        return qs_fail(QS_ERR_ARG, "qs_plan_create: threads_per_row must be 1 or 2");
     if (count && !gates) return qs_fail(QS_ERR_ARG, "qs_plan_create: null gate list");
     qs_plan *P = new qs_plan();
     P->n = n;
@@ -620,6 +624,7 @@ extern "C" int qs_plan_apply_range(qs_state *s, qs_plan *P, size_t first, size_t
         for (size_t u = first; u < first + count; ++u) {
             const PlanPass &pp = P->passes[u];
             qs_tiled_desc &d = descs[u - first];
+            d.threads_per_row = P->opts.threads_per_row;
             if (dst[u - first] >= 0) {
                 d.amp_out = buf[dst[u - first]];
                 d.amp_in = buf[dst[u - first] ^ 1];

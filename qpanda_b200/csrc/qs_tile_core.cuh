@@ -100,6 +100,17 @@ __device__ __forceinline__ uint64_t tile_base_advance(uint64_t base, uint64_t st
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
+// Stores to shared memory by 32-bit shared-window address (st.shared, never
+// the generic path).
+__device__ __forceinline__ void sts32(uint32_t addr, uint32_t v)
+{
+    asm volatile("st.shared.b32 [%0], %1;" :: "r"(addr), "r"(v));
+}
+__device__ __forceinline__ void sts64(uint32_t addr, uint32_t a, uint32_t b)
+{
+    asm volatile("st.shared.v2.b32 [%0], {%1, %2};" :: "r"(addr), "r"(a), "r"(b));
+}
+
 // UMMA shared-memory descriptor: K-major, 128-byte swizzle, rows of 128 B in
 // 8-row groups 1024 B apart, version 1 (sm_100).
 __device__ __forceinline__ uint64_t umma_desc(uint32_t saddr)
@@ -213,11 +224,15 @@ struct ChunkBase {
     uint32_t r, j;
 };
 
+// t: the thread's index among the lane's nt = 128 x tpr threads, which copy
+// chunks c = nt k + t: tile index bits 1 .. log2(nt) come from t.
+template <int TPR = 1>
 __device__ __forceinline__ ChunkBase chunk_base(const LoadMap &L, int t128)
 {
     ChunkBase c{0, 0, 0};
+    constexpr int kBits = TPR == 2 ? 9 : 8;
 #pragma unroll
-    for (int t = 1; t < 8; ++t) {
+    for (int t = 1; t < kBits; ++t) {
         if (!((t128 >> (t - 1)) & 1)) continue;
         c.g |= 1ull << L.tpos[t];
         const int m = L.tmap0[t];
@@ -231,16 +246,20 @@ __device__ __forceinline__ ChunkBase chunk_base(const LoadMap &L, int t128)
 // 2c+1 - is copied to byte 16c, chunk c = 128 k + thread, so the 32 lanes of a
 // warp fill 512 contiguous bytes of shared memory per copy instruction, however
 // short the tile's contiguous runs in global memory are.  Each thread later
-// reads back only its own chunks (convert_tile): no barrier separates the
+// reads back only its own chunks (convert_load): no barrier separates the
 // copies from the reads, nor the reads from the next tile's copies.
+// With tpr threads per row the lane's 128 tpr threads each copy 16 / tpr
+// chunks, c = 128 tpr k + t; tile index bits above log2(128 tpr) come from k,
+// so the LoadMap's tables (indexed by tile bits 8..11) are read at k tpr.
+template <int TPR = 1>
 __device__ __forceinline__ void prefetch_tile_linear(const float *amp, uint64_t base, const LoadMap &M,
                                                      uint32_t stage, uint64_t g_thread, int t128)
 {
 #pragma unroll
-    for (int k = 0; k < 16; ++k) {
-        const float *src = amp + 2 * (base | g_thread | M.gk[k]);
-        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" :: "r"(stage + (uint32_t)(128 * k + t128) * 16u),
-                     "l"(src) : "memory");
+    for (int k = 0; k < 16 / TPR; ++k) {
+        const float *src = amp + 2 * (base | g_thread | M.gk[k * TPR]);
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;"
+                     :: "r"(stage + (uint32_t)(128 * TPR * k + t128) * 16u), "l"(src) : "memory");
     }
     asm volatile("cp.async.commit_group;" ::: "memory");
 }
@@ -269,38 +288,58 @@ __device__ __forceinline__ uint32_t a_offset(uint32_t r, uint32_t j)
     return r * 128 + ((((j >> 2) ^ (r & 7)) & 7) << 4) + ((j & 3) << 2);
 }
 
-// Each thread splits its own 16 staged chunks into block 0's A buffers (BF16
-// hi/lo), at the rows and columns the LoadMap gives; returns the chunks'
-// sum of squares.  Column pairs (tile bit 0 = block-0 column bit 0) go out as
-// one 8-byte store per buffer; otherwise the two amplitudes of a chunk sit at
-// (r, j) and (r | dr, j | dj) and go out as 4-byte stores.
-__device__ __forceinline__ float convert_tile(uint32_t stage, uint8_t *aHi, uint8_t *aLo, const LoadMap &M,
-                                              const ChunkBase &cb, int t128)
+// Block 0's input in two steps, so that the wait for the tensor cores to
+// release the A buffers can sit between them (k_fused_tile):
+// convert_load reads the thread's own staged chunks (all reads issued before
+// the first use) and splits them into BF16 hi/lo pairs in registers, returning
+// their sum of squares; convert_store writes the pairs at their block-0 rows
+// and columns of the swizzled A buffers.  Column pairs (tile bit 0 = block-0
+// column bit 0) go out as one 8-byte store per buffer; otherwise the two
+// amplitudes of a chunk sit at (r, j) and (r | dr, j | dj) and go out as
+// 4-byte stores.
+template <int TPR = 1>
+__device__ __forceinline__ float convert_load(uint32_t stage, int t128, uint32_t (&hv)[16 / TPR][2],
+                                              uint32_t (&lv)[16 / TPR][2])
 {
+    constexpr int kChunks = 16 / TPR;
+    float4 vv[kChunks];
+#pragma unroll
+    for (int k = 0; k < kChunks; ++k)
+        asm volatile("ld.shared.v4.f32 {%0,%1,%2,%3}, [%4];"
+                     : "=f"(vv[k].x), "=f"(vv[k].y), "=f"(vv[k].z), "=f"(vv[k].w)
+                     : "r"(stage + (uint32_t)(128 * TPR * k + t128) * 16u));
     float ss = 0.f;
 #pragma unroll
-    for (int k = 0; k < 16; ++k) {
-        float4 v;
-        asm volatile("ld.shared.v4.f32 {%0,%1,%2,%3}, [%4];"
-                     : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w) : "r"(stage + (uint32_t)(128 * k + t128) * 16u));
+    for (int k = 0; k < kChunks; ++k) {
+        const float4 v = vv[k];
         ss = fmaf(v.x, v.x, fmaf(v.y, v.y, fmaf(v.z, v.z, fmaf(v.w, v.w, ss))));
-        const uint32_t row = cb.r ^ M.rk[k], j = cb.j ^ M.jk[k];
-        uint32_t h0, l0, h1, l1;
-        split_pair(v.x, v.y, h0, l0);
-        split_pair(v.z, v.w, h1, l1);
-        if (M.pair) {
-            const uint32_t off = a_offset(row, j);            // j even: columns j, j+1 are adjacent
-            *reinterpret_cast<uint2 *>(aHi + off) = make_uint2(h0, h1);
-            *reinterpret_cast<uint2 *>(aLo + off) = make_uint2(l0, l1);
-        } else {
-            const uint32_t o0 = a_offset(row, j), o1 = a_offset(row | M.dr, j | M.dj);
-            *reinterpret_cast<uint32_t *>(aHi + o0) = h0;
-            *reinterpret_cast<uint32_t *>(aLo + o0) = l0;
-            *reinterpret_cast<uint32_t *>(aHi + o1) = h1;
-            *reinterpret_cast<uint32_t *>(aLo + o1) = l1;
-        }
+        split_pair(v.x, v.y, hv[k][0], lv[k][0]);
+        split_pair(v.z, v.w, hv[k][1], lv[k][1]);
     }
     return ss;
+}
+
+template <int TPR = 1>
+__device__ __forceinline__ void convert_store(uint8_t *aHi, uint8_t *aLo, const LoadMap &M, const ChunkBase &cb,
+                                              const uint32_t (&hv)[16 / TPR][2], const uint32_t (&lv)[16 / TPR][2])
+{
+    constexpr int kChunks = 16 / TPR;
+    const uint32_t hi_s = smem_u32(aHi), lo_s = smem_u32(aLo);
+#pragma unroll
+    for (int k = 0; k < kChunks; ++k) {
+        const uint32_t row = cb.r ^ M.rk[k * TPR], j = cb.j ^ M.jk[k * TPR];
+        if (M.pair) {
+            const uint32_t off = a_offset(row, j);            // j even: columns j, j+1 are adjacent
+            sts64(hi_s + off, hv[k][0], hv[k][1]);
+            sts64(lo_s + off, lv[k][0], lv[k][1]);
+        } else {
+            const uint32_t o0 = a_offset(row, j), o1 = a_offset(row | M.dr, j | M.dj);
+            sts32(hi_s + o0, hv[k][0]);
+            sts32(lo_s + o0, lv[k][0]);
+            sts32(hi_s + o1, hv[k][1]);
+            sts32(lo_s + o1, lv[k][1]);
+        }
+    }
 }
 
 // Where a pass writes a tile's results (k_fused_tile).  The 12 tile bits go
@@ -341,8 +380,8 @@ __device__ __forceinline__ void a_store_at(uint8_t *aHi, uint8_t *aLo, uint32_t 
 {
     uint32_t hv, lv;
     split_pair(re, im, hv, lv);
-    *reinterpret_cast<uint32_t *>(aHi + off) = hv;
-    *reinterpret_cast<uint32_t *>(aLo + off) = lv;
+    sts32(smem_u32(aHi) + off, hv);
+    sts32(smem_u32(aLo) + off, lv);
 }
 
 // A whole row (32 complex = 64 floats) as 16-byte chunks: chunk c (columns

@@ -16,7 +16,7 @@ using qs_tile::kMaxSub;
 // columns of the contraction.  The order decides which tile bits a warp's 32
 // lanes (row bits 0..4) run over, and with it
 //   * how many shared-memory wavefronts the block-0 input stores take
-//     (convert_tile: the lanes of a warp hold consecutive chunks, i.e. tile
+//     (convert_store: the lanes of a warp hold consecutive chunks, i.e. tile
 //     bits 1..5, and write them at their rows and columns of the swizzled A
 //     buffer - row bits 0..2 and column bits land on different bank bits);
 //   * how many 32-byte sectors one warp-wide global store of the last block
@@ -51,7 +51,7 @@ int store_cost(unsigned lanes, const int *W, bool vec)
     return (vec ? 16 : 32) * (32 >> (k > 5 ? 5 : k));
 }
 
-// Wavefronts of convert_tile's stores for block 0 with columns Q0 and row
+// Wavefronts of convert_store's stores for block 0 with columns Q0 and row
 // bits 0..2 on tile bits t[0..2]: a lane's store lands at byte bits 2..6
 // (4-byte stores) or 3..6 (8-byte column pairs) given by the lane's tile bits
 // 1..5 (1..4): column c -> bit 2 + c (c < 2) or c + 2, XOR'd with row bits

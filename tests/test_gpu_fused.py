@@ -126,14 +126,26 @@ def test_tiled_remap(need_gpu, n, max_sub, remap):
     assert np.abs(sv.get_state() - o.state()).max() < AMP_TOL
 
 
-@pytest.mark.parametrize("kernel,remap", [("single", 0), ("tiled", 0), ("tiled", 1), ("tiled", 2)])
-def test_fused_fidelity_26q_vs_fp64_gpu(need_gpu, kernel, remap):
+@pytest.mark.parametrize("remap", [0, 1])
+@pytest.mark.parametrize("max_sub", [1, 2, 3])
+@pytest.mark.parametrize("n", [13, 20])
+def test_tiled_two_threads_per_row(need_gpu, n, max_sub, remap):
+    """The 256-threads-per-lane variant of the tiled kernel (two threads per
+    tile row, 16 columns each) in place and remapped."""
+    g = circuits.random_layers(n, 6, 130 + n + max_sub, iswap_frac=0.2)
+    check_fused(n, g, init=random_state(n, n + 7 * max_sub), kernel="tiled", max_sub=max_sub, remap=remap,
+                threads_per_row=2)
+
+
+@pytest.mark.parametrize("kernel,remap,tpr", [("single", 0, 1), ("tiled", 0, 1), ("tiled", 1, 1), ("tiled", 2, 1),
+                                              ("tiled", 1, 2)])
+def test_fused_fidelity_26q_vs_fp64_gpu(need_gpu, kernel, remap, tpr):
     """26 qubits, 12 layers: fused complex64 against the complex128 per-gate
     path (itself pinned to the oracle by the other tests)."""
     n = 26
     g = circuits.random_layers(n, 12, 7, iswap_frac=0.1)
     f = StateVector(n, "c64")
-    p = FusionPlan(n, g, kernel=kernel, remap=remap)
+    p = FusionPlan(n, g, kernel=kernel, remap=remap, threads_per_row=tpr)
     p.apply(f)
     p.status(f)
     d = StateVector(n, "c128")

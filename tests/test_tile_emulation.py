@@ -35,11 +35,12 @@ def emu(tmp_path_factory):
     r = subprocess.run(cmd, capture_output=True, text=True)
     assert r.returncode == 0, r.stdout + r.stderr
     E = C.CDLL(out)
-    E.tile_emu_apply.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.POINTER(C.c_int),
+    E.tile_emu_apply.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_int),
                                  C.POINTER(C.c_int)]
     E.tile_emu_apply.restype = C.c_int
     E.tile_emu_error.restype = C.c_char_p
-    E.tile_emu_check_input.argtypes = [C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]
+    E.tile_emu_check_input.argtypes = [C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int), C.c_int,
+                                       C.POINTER(C.c_int)]
     E.tile_emu_check_input.restype = C.c_int
     return E
 
@@ -50,12 +51,13 @@ def random_state(n, seed):
     return v / np.linalg.norm(v)
 
 
-def run_emu(E, n, g, init, remap, kinds=None, **kw):
+def run_emu(E, n, g, init, remap, kinds=None, tpr=1, **kw):
+    """tpr: the kernel's threads per tile row (1: 128 threads per lane, 2: 256)."""
     p = FusionPlan(n, g, remap=remap, **kw)
     st = np.ascontiguousarray(init.astype(np.complex128))
     npass = C.c_int()
     k = (C.c_int * 3)()
-    rc = E.tile_emu_apply(p.handle, n, st.ctypes.data, int(remap), C.byref(npass), k)
+    rc = E.tile_emu_apply(p.handle, n, st.ctypes.data, int(remap), int(tpr), C.byref(npass), k)
     if kinds is not None:
         for i in range(3):
             kinds[i] += k[i]
@@ -68,22 +70,24 @@ def run_emu(E, n, g, init, remap, kinds=None, **kw):
     return err, npass.value
 
 
+@pytest.mark.parametrize("tpr", [1, 2])
 @pytest.mark.parametrize("remap", [0, 1, 2])
 @pytest.mark.parametrize("max_sub,low", [(1, 3), (2, 3), (3, 3), (2, 1), (2, 5), (3, 4)])
-def test_tiled_index_math_random_layers(emu, remap, max_sub, low):
+def test_tiled_index_math_random_layers(emu, remap, max_sub, low, tpr):
     n = 16
     g = circuits.random_layers(n, 6, 300 + 10 * max_sub + low, iswap_frac=0.2)
-    err, npass = run_emu(emu, n, g, random_state(n, 1), remap, max_sub=max_sub, low_qubits=low)
+    err, npass = run_emu(emu, n, g, random_state(n, 1), remap, tpr=tpr, max_sub=max_sub, low_qubits=low)
     assert npass >= 2
     assert err < 1e-10, err
 
 
+@pytest.mark.parametrize("tpr", [1, 2])
 @pytest.mark.parametrize("remap", [0, 1, 2])
 @pytest.mark.parametrize("n", [12, 13, 17])
-def test_tiled_index_math_sizes(emu, remap, n):
+def test_tiled_index_math_sizes(emu, remap, n, tpr):
     """One tile (12 qubits), two tiles, and an odd count of passes."""
     g = circuits.random_layers(n, 5, 40 + n, iswap_frac=0.1)
-    err, _ = run_emu(emu, n, g, random_state(n, n), remap)
+    err, _ = run_emu(emu, n, g, random_state(n, n), remap, tpr=tpr)
     assert err < 1e-10, err
 
 
@@ -104,7 +108,7 @@ def test_tiled_index_math_chunk_pairings_in_plans(emu):
         n = 14 + seed % 3
         g = circuits.random_layers(n, 5, 900 + seed, iswap_frac=0.2)
         for remap in (0, 1, 2):
-            err, _ = run_emu(emu, n, g, random_state(n, seed), remap, kinds=kinds)
+            err, _ = run_emu(emu, n, g, random_state(n, seed), remap, kinds=kinds, tpr=1 + seed % 2)
             assert err < 1e-10, (seed, remap, err)
     assert kinds[0] > 0 and kinds[2] > 0, kinds
 
@@ -122,9 +126,10 @@ def test_block0_input_mapping_any_column_order(emu):
         q = rng.permutation(T)[:5].astype(np.int32)
         if it % 3 == 0 and 0 not in q:
             q[int(rng.integers(1, 5))] = 0           # tile bit 0 as a later column
-        kind = C.c_int(-1)
-        rc = emu.tile_emu_check_input(n, T.ctypes.data_as(C.POINTER(C.c_int)),
-                                      q.ctypes.data_as(C.POINTER(C.c_int)), C.byref(kind))
-        assert rc == 0, (it, emu.tile_emu_error().decode())
+        for tpr in (1, 2):
+            kind = C.c_int(-1)
+            rc = emu.tile_emu_check_input(n, T.ctypes.data_as(C.POINTER(C.c_int)),
+                                          q.ctypes.data_as(C.POINTER(C.c_int)), tpr, C.byref(kind))
+            assert rc == 0, (it, tpr, emu.tile_emu_error().decode())
         kinds[kind.value] += 1
     assert all(k > 0 for k in kinds), kinds

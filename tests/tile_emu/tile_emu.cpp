@@ -6,7 +6,7 @@
 // tables from its own layout builder (qs_tile_layout_build), and each tile
 // goes through
 //   * the tile-order staging copies of prefetch_tile_linear (LoadMap) and
-//     convert_tile, which puts each thread's chunks at their block-0 rows and
+//     convert_load / convert_store, which put each thread's chunks at their block-0 rows and
 //     columns;
 //   * each block's contraction (in FP64 here, on the block unitaries of the
 //     plan, instead of split BF16 on the tensor cores);
@@ -90,8 +90,10 @@ extern "C" const char *tile_emu_error(void) { return g_err; }
 // Apply plan passes [0, all) to state (2^n complex128, interleaved re/im).
 // *kinds_out (may be NULL) counts the passes whose chunk pairs are adjacent
 // columns [0], other columns [1], two rows [2].
-extern "C" int tile_emu_apply(const qs_plan *P, int n, double *state, int remap, int *n_passes_out, int *kinds_out)
+extern "C" int tile_emu_apply(const qs_plan *P, int n, double *state, int remap, int tpr, int *n_passes_out,
+                              int *kinds_out)
 {
+    if (tpr != 1 && tpr != 2) return fail("threads per row must be 1 or 2");
     g_err[0] = 0;
     const size_t npass = P->passes.size();
     std::vector<qs_tiled_desc> descs;
@@ -135,29 +137,29 @@ extern "C" int tile_emu_apply(const qs_plan *P, int n, double *state, int remap,
         for (uint64_t t = 0; t < tiles; ++t) {
             const uint64_t tbase = deposit_tile(t, L);
             // ---- prefetch_tile_linear: chunk c = 128 k + thread (tile indices
-            // 2c, 2c+1) into staging slot c, then convert_tile: each thread's
+            // 2c, 2c+1) into staging slot c, then convert_load / convert_store: each thread's
             // chunks into block 0's rows and columns
             std::fill(sh.begin(), sh.end(), 0);
             std::fill(ah.begin(), ah.end(), 0);
-            for (int th = 0; th < 128; ++th) {
+            for (int th = 0; th < 128 * tpr; ++th) {
                 uint64_t g = 0;
                 uint32_t r = 0, jj = 0;
-                for (int tb = 1; tb < 8; ++tb) {
+                for (int tb = 1; tb < 7 + tpr; ++tb) {
                     if (!((th >> (tb - 1)) & 1)) continue;
                     g |= 1ull << M.tpos[tb];
                     const int mm = M.tmap0[tb];
                     if (mm >= 0) r |= 1u << mm;
                     else jj |= 1u << (~mm);
                 }
-                for (int kk = 0; kk < 16; ++kk) {
-                    const uint64_t s = tbase | g | M.gk[kk];
+                for (int kk = 0; kk < 16 / tpr; ++kk) {
+                    const uint64_t s = tbase | g | M.gk[kk * tpr];
                     if (s + 1 >= N) return fail("load out of range", (long long)s);
-                    const int c = 128 * kk + th;
+                    const int c = 128 * tpr * kk + th;
                     stage[2 * c] = src[s];
                     stage[2 * c + 1] = src[s + 1];
                     sh[2 * c]++;
                     sh[2 * c + 1]++;
-                    const uint32_t row = r ^ M.rk[kk], j = jj ^ M.jk[kk];
+                    const uint32_t row = r ^ M.rk[kk * tpr], j = jj ^ M.jk[kk * tpr];
                     const uint32_t row1 = row | M.dr, j1 = j | M.dj;
                     if (row >= 128 || j >= 32 || row1 >= 128 || j1 >= 32 || row1 * 32 + j1 == row * 32 + j)
                         return fail("A slot out of range", row, j);
@@ -233,8 +235,9 @@ extern "C" int tile_emu_apply(const qs_plan *P, int n, double *state, int remap,
 // every tile must receive exactly the amplitude at tile base | row bits |
 // column bits.  Returns 0, or 1 with tile_emu_error() set; *kind = 0 adjacent
 // column pair, 1 other column, 2 rows.
-extern "C" int tile_emu_check_input(int n, const int *T, const int *qpos0, int *kind)
+extern "C" int tile_emu_check_input(int n, const int *T, const int *qpos0, int tpr, int *kind)
 {
+    if (tpr != 1 && tpr != 2) return fail("threads per row must be 1 or 2");
     g_err[0] = 0;
     int qpos[3][5];
     for (int j = 0; j < 5; ++j) qpos[0][j] = qpos0[j];
@@ -248,19 +251,19 @@ extern "C" int tile_emu_check_input(int n, const int *T, const int *qpos0, int *
     for (uint64_t t = 0; t < tiles; t += (tiles > 64 ? tiles / 64 : 1)) {
         const uint64_t tbase = deposit_tile(t, L);
         std::fill(ah.begin(), ah.end(), 0);
-        for (int th = 0; th < 128; ++th) {
+        for (int th = 0; th < 128 * tpr; ++th) {
             uint64_t g = 0;
             uint32_t r = 0, jj = 0;
-            for (int tb = 1; tb < 8; ++tb) {
+            for (int tb = 1; tb < 7 + tpr; ++tb) {
                 if (!((th >> (tb - 1)) & 1)) continue;
                 g |= 1ull << M.tpos[tb];
                 const int mm = M.tmap0[tb];
                 if (mm >= 0) r |= 1u << mm;
                 else jj |= 1u << (~mm);
             }
-            for (int kk = 0; kk < 16; ++kk) {
-                const uint64_t s0 = tbase | g | M.gk[kk];
-                const uint32_t row = r ^ M.rk[kk], j = jj ^ M.jk[kk];
+            for (int kk = 0; kk < 16 / tpr; ++kk) {
+                const uint64_t s0 = tbase | g | M.gk[kk * tpr];
+                const uint32_t row = r ^ M.rk[kk * tpr], j = jj ^ M.jk[kk * tpr];
                 const uint32_t row1 = row | M.dr, j1 = j | M.dj;
                 if (row1 >= 128 || j1 >= 32) return fail("A slot out of range", row1, j1);
                 a[row * 32 + j] = s0;
