@@ -71,3 +71,13 @@ def test_plan_rejects_wide_gates_and_bad_width():
         FusionPlan(12, g)
     with pytest.raises(QSError):
         FusionPlan(12, circuits.qft(12), max_k=6)
+
+
+def test_plan_rejects_bad_tiled_options():
+    """remap must be 0..2 and threads_per_row 1 or 2; both valid values build."""
+    g = circuits.qft(12)
+    for kw in ({"remap": 3}, {"threads_per_row": 0}, {"threads_per_row": 3}):
+        with pytest.raises(QSError):
+            FusionPlan(12, g, **kw)
+    for kw in ({"remap": 2}, {"threads_per_row": 2}):
+        FusionPlan(12, g, **kw).close()
