@@ -293,7 +293,9 @@ class FusionPlan:
     kernel="single" one block per pass.  remap=1: tiled passes write their
     tiles as contiguous runs into a second state-size buffer kept with the
     state (twice the memory; faster passes on large states); remap=2: the
-    next pass's tiles contiguous instead (qs_plan_opts.remap)."""
+    next pass's tiles contiguous instead (qs_plan_opts.remap).
+    threads_per_row=2: tiled passes with two threads per tile row
+    (qs_plan_opts.threads_per_row; measured slightly slower than 1)."""
 
     def __init__(self, n, gates, max_k=5, kernel="tiled", max_sub=2, low_qubits=3, remap=False, threads_per_row=1):
         g = np.ascontiguousarray(gates, dtype=GATE_DTYPE)
