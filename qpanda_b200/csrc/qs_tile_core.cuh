@@ -2,7 +2,8 @@
 // (qs_fused2.cu: one circuit, many CTAs; qs_batch.cu: many circuits, one CTA
 // each).  A tile is 4096 complex64 amplitudes that differ in 12 tile qubits;
 // for a 5-qubit block it is 128 rows (7 tile bits) x 32 columns (the block's
-// 5 bits).  Thread i of 128 owns row i and TMEM lane i.
+// 5 bits).  Thread i of 128 owns row i and TMEM lane i (with two threads per
+// row, threads i and 128 + i share row i, 16 columns each).
 #pragma once
 
 #include <cuda_bf16.h>
@@ -382,24 +383,6 @@ __device__ __forceinline__ void a_store_at(uint8_t *aHi, uint8_t *aLo, uint32_t 
     split_pair(re, im, hv, lv);
     sts32(smem_u32(aHi) + off, hv);
     sts32(smem_u32(aLo) + off, lv);
-}
-
-// A whole row (32 complex = 64 floats) as 16-byte chunks: chunk c (columns
-// 4c..4c+3) at position c ^ (row & 7) of the row's 128 bytes.
-__device__ __forceinline__ void a_store_row(uint8_t *aHi, uint8_t *aLo, int row, const float (&x)[64])
-{
-    uint8_t *rh = aHi + row * 128, *rl = aLo + row * 128;
-#pragma unroll
-    for (int c = 0; c < 8; ++c) {
-        uint4 h, l;
-        split_pair(x[8 * c + 0], x[8 * c + 1], h.x, l.x);
-        split_pair(x[8 * c + 2], x[8 * c + 3], h.y, l.y);
-        split_pair(x[8 * c + 4], x[8 * c + 5], h.z, l.z);
-        split_pair(x[8 * c + 6], x[8 * c + 7], h.w, l.w);
-        const uint32_t pos = (uint32_t)(c ^ (row & 7)) << 4;
-        *reinterpret_cast<uint4 *>(rh + pos) = h;
-        *reinterpret_cast<uint4 *>(rl + pos) = l;
-    }
 }
 
 // B operands of a pass (nsub blocks, hi and lo each) into the swizzled layout.
