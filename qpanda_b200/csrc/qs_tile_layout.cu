@@ -99,9 +99,17 @@ void choose_row_orders(const int *T, int nsub, const int (*Q)[5], int (*Cp)[7], 
     auto in_cost = [&](const RowCfg &c) {
         return input_mode == 0 ? convert_cost(Q[0], c.t) : glob_cost(c.lanes, loc0, loc1, vec0);
     };
+    // Configurations of block b: 210 ordered triples for row bits 0..2, each
+    // with 6 choices of row bits 3..4 among the other four (index 6 t + u).
+    // The input and scatter costs depend on a configuration through its
+    // triple and the previous block's lane set only, so they are evaluated
+    // once per triple.
+    constexpr int kTriples = 210, kPer = 6, kCfg = kTriples * kPer;
+    static_assert(kCfg == 1260, "7 x 6 x 5 triples x C(4, 2) lane pairs");
     std::vector<RowCfg> cfg[kMaxSub];
     for (int b = 0; b < nsub; ++b) {
         const int *C = Cp[b];
+        cfg[b].reserve(kCfg);
         // configuration 0 is the ascending order
         for (int i = 0; i < 7; ++i)
             for (int j = 0; j < 7; ++j)
@@ -117,24 +125,38 @@ void choose_row_orders(const int *T, int nsub, const int (*Q)[5], int (*Cp)[7], 
                 }
     }
     std::vector<int> best[kMaxSub], from[kMaxSub];
-    best[0].resize(cfg[0].size());
-    for (size_t i = 0; i < cfg[0].size(); ++i) best[0][i] = in_cost(cfg[0][i]);
-    for (int b = 1; b < nsub; ++b) {
-        // the previous block enters only through its lane set: keep its cheapest configuration per set
-        std::vector<std::pair<unsigned, int>> sets;     // (lanes, configuration)
-        for (size_t p = 0; p < cfg[b - 1].size(); ++p) {
-            size_t s = 0;
-            while (s < sets.size() && sets[s].first != cfg[b - 1][p].lanes) ++s;
-            if (s == sets.size()) sets.push_back({cfg[b - 1][p].lanes, (int)p});
-            else if (best[b - 1][p] < best[b - 1][sets[s].second]) sets[s].second = (int)p;
+    best[0].resize(kCfg);
+    for (int t = 0; t < kTriples; ++t) {
+        if (input_mode == 0) {
+            const int c = convert_cost(Q[0], cfg[0][kPer * t].t);
+            for (int u = 0; u < kPer; ++u) best[0][kPer * t + u] = c;
+        } else {
+            for (int u = 0; u < kPer; ++u) best[0][kPer * t + u] = in_cost(cfg[0][kPer * t + u]);
         }
-        best[b].assign(cfg[b].size(), 1 << 30);
-        from[b].assign(cfg[b].size(), -1);
-        for (size_t i = 0; i < cfg[b].size(); ++i)
-            for (const auto &s : sets) {
-                const int c = best[b - 1][s.second] + scatter_cost(s.first, Q[b], cfg[b][i].t);
-                if (c < best[b][i]) { best[b][i] = c; from[b][i] = s.second; }
+    }
+    std::vector<int> set_of(1u << 12);
+    for (int b = 1; b < nsub; ++b) {
+        // the previous block enters only through its lane set: keep its
+        // cheapest configuration per set (first one on ties), sets in order of
+        // first appearance
+        std::vector<std::pair<unsigned, int>> sets;     // (lanes, configuration)
+        std::fill(set_of.begin(), set_of.end(), -1);
+        for (int p = 0; p < kCfg; ++p) {
+            const unsigned ln = cfg[b - 1][p].lanes;
+            int &s = set_of[ln];
+            if (s < 0) { s = (int)sets.size(); sets.push_back({ln, p}); }
+            else if (best[b - 1][p] < best[b - 1][sets[s].second]) sets[s].second = p;
+        }
+        best[b].assign(kCfg, 1 << 30);
+        from[b].assign(kCfg, -1);
+        for (int t = 0; t < kTriples; ++t) {
+            int bc = 1 << 30, bf = -1;
+            for (const auto &st : sets) {
+                const int c = best[b - 1][st.second] + scatter_cost(st.first, Q[b], cfg[b][kPer * t].t);
+                if (c < bc) { bc = c; bf = st.second; }
             }
+            for (int u = 0; u < kPer; ++u) { best[b][kPer * t + u] = bc; from[b][kPer * t + u] = bf; }
+        }
     }
     const int last = nsub - 1;
     int sel[kMaxSub] = {0, 0, 0}, bestc = 1 << 30;
