@@ -189,9 +189,23 @@ k_marginal(const T *__restrict__ a, MargParams P, double *__restrict__ part)
         uint64_t uidx = g * P.R + r, hu = 0;
         for (int j = 0; j < P.uhi; ++j) hu |= ((uidx >> j) & 1ull) << P.uhi_pos[j];
         const uint64_t base = (hm | hu) << P.c;
-        for (int l = t; l < C; l += kThreads) {
-            V x = pa[base + l];
-            p[l] = p2(x.x, x.y);
+        // all of the thread's loads of the chunk (up to 4096 / kThreads) go
+        // out before the first store, so that enough bytes are in flight to
+        // stream the state at HBM speed
+        constexpr int kPer = 4096 / kThreads;
+        double v[kPer];
+#pragma unroll
+        for (int i = 0; i < kPer; ++i) {
+            const int l = t + i * kThreads;
+            if (l < C) {
+                const V x = pa[base + l];
+                v[i] = p2(x.x, x.y);
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < kPer; ++i) {
+            const int l = t + i * kThreads;
+            if (l < C) p[l] = v[i];
         }
         __syncthreads();
         if (nb >= kThreads) {
