@@ -225,11 +225,14 @@ typedef struct qs_plan_opts {
                               back; 2 = as 1, but each pass writes the layout in which the next pass's
                               tiles are contiguous (loads stream, stores scatter; measured slower) */
     int threads_per_row;   /* tiled passes: 1 = each of a lane's 128 threads owns a row of the tile (default);
-                              2 = 256 threads per lane, two per row, each with 16 of its 32 columns */
+                              2 = 256 threads per lane, two per row, each with 16 of its 32 columns
+                              (measured 3-4 % slower) */
 } qs_plan_opts;
 /* Defaults: 5-qubit blocks, tiled passes of 12 qubits with up to 2 blocks
  * (a pass of 3 blocks saves a pass but runs on a kernel with fewer resident
- * CTAs, and measured slower overall), qubits 0..2 in every tile, in place. */
+ * CTAs, and measured slower overall), qubits 0..2 in every tile, in place,
+ * one thread per tile row.  Fill a qs_plan_opts with this call before
+ * changing fields: the struct may gain fields at its end. */
 int qs_plan_default_opts(qs_plan_opts *opts);
 int qs_plan_create_ex(int n_qubits, const qs_gate *gates, size_t count, const qs_plan_opts *opts,
                       qs_plan **out);
