@@ -109,6 +109,71 @@ std::vector<std::pair<uint64_t, std::vector<size_t>>> greedy_groups(const std::v
     return out;
 }
 
+typedef std::vector<std::pair<uint64_t, std::vector<size_t>>> Groups;
+
+// Closure-first fusion of the gates idx[] (in list order) into groups of at
+// most k qubits.  A group starts with the first unplaced gate, then takes
+// every available gate whose qubits it already has (available: no earlier
+// unplaced gate shares a qubit with it, so it only moves past gates it
+// commutes with), and only when none is left grows by the available gate
+// that adds the fewest new qubits (the earliest of those).  Taking gates in
+// list order instead lets a gate on new qubits in early and fills the group
+// before the gates that would have fitted: on the 32-qubit depth-16 random
+// circuit this packs the 768 gates into 72 groups instead of 89.
+Groups closure_groups(const std::vector<size_t> &idx, const std::vector<uint64_t> &mask, int k)
+{
+    Groups out;
+    const size_t N = idx.size();
+    std::vector<char> done(N, 0);
+    size_t left = N, first = 0;
+    auto take = [&](size_t t, uint64_t &Q, std::vector<size_t> &mem) {
+        done[t] = 1;
+        --left;
+        Q |= mask[idx[t]];
+        mem.push_back(idx[t]);
+    };
+    while (left) {
+        uint64_t Q = 0;
+        std::vector<size_t> mem;
+        bool seeded = false;
+        while (true) {
+            bool changed = true;
+            while (changed) {                // closure: available gates inside Q (any gate to seed)
+                changed = false;
+                uint64_t blocked = 0;
+                while (first < N && done[first]) ++first;
+                for (size_t t = first; t < N; ++t) {
+                    if (done[t]) continue;
+                    const uint64_t m = mask[idx[t]];
+                    if (!(m & blocked) && (!seeded || !(m & ~Q))) {
+                        take(t, Q, mem);
+                        seeded = true;
+                        changed = true;
+                    } else {
+                        blocked |= m;
+                    }
+                }
+            }
+            uint64_t blocked = 0;            // grow by the available gate adding the fewest qubits
+            int best_add = 65;
+            size_t best = N;
+            for (size_t t = first; t < N; ++t) {
+                if (done[t]) continue;
+                const uint64_t m = mask[idx[t]];
+                if (!(m & blocked) && __builtin_popcountll(Q | m) <= k) {
+                    const int add = __builtin_popcountll(m & ~Q);
+                    if (add < best_add) { best_add = add; best = t; }
+                }
+                blocked |= m;
+            }
+            if (best == N) break;
+            take(best, Q, mem);
+        }
+        out.push_back(std::make_pair(Q, std::move(mem)));
+    }
+    return out;
+}
+
 // Block unitary: qubits q[0..4] ascending (global), gates applied in order.
 void block_unitary(PlanBlock &B, const std::vector<qs_prim> &prim)
 {
@@ -170,7 +235,8 @@ int build_blocks(qs_plan *P)
     std::vector<size_t> all(P->gates.size());
     for (size_t i = 0; i < all.size(); ++i) all[i] = i;
     const uint64_t every = P->n >= 64 ? ~0ull : ((1ull << P->n) - 1);
-    for (auto &grp : greedy_groups(all, mask, P->max_k)) {
+    Groups ga = greedy_groups(all, mask, P->max_k), gb = closure_groups(all, mask, P->max_k);
+    for (auto &grp : gb.size() < ga.size() ? gb : ga) {
         PlanBlock B;
         B.gates = grp.second;
         mask_to_list(widen(grp.first, every, 5), B.q);
@@ -181,20 +247,28 @@ int build_blocks(qs_plan *P)
     return QS_OK;
 }
 
-// Tiled passes: a pass takes gates while its qubits stay within tile_qubits
-// (the lowest low_qubits always included, so that every row of the tile is a
-// run of at least 2^low_qubits contiguous amplitudes) and its gates still
-// fuse into at most max_sub blocks of 5 qubits.
-int build_passes(qs_plan *P)
+// Tiled passes.  A pass's tile holds the lowest low_qubits qubits (so that
+// every row of the tile is a run of at least 2^low_qubits contiguous
+// amplitudes) and the qubits of its blocks, at most tile_qubits in all; a
+// pass applies up to max_sub blocks of 5 qubits.  Two drafts are built and
+// the one with fewer passes is kept (the first on a tie):
+//   tile-first: a pass takes gates in list order while its qubits stay
+//     within the tile and its gates still fuse (greedy_groups) into at most
+//     max_sub blocks;
+//   blocks-first: all gates are fused into blocks (closure_groups), and
+//     consecutive blocks share a pass while their qubits and the low qubits
+//     fit one tile.
+// On the 32-qubit depth-16 random circuit the first gives 46 passes and the
+// second 43 (36 with low_qubits = 2); on a QFT they tie.
+struct DraftPass {
+    uint64_t T;                          // tile qubits before widening
+    Groups blocks;
+};
+
+std::vector<DraftPass> draft_tile_first(const std::vector<uint64_t> &mask, int TQ, int MS, uint64_t low)
 {
-    std::vector<qs_prim> prim;
-    std::vector<uint64_t> mask;
-    int r = lower_all(P, prim, mask);
-    if (r) return r;
-    const int TQ = P->opts.tile_qubits, MS = P->opts.max_sub;
-    const uint64_t every = P->n >= 64 ? ~0ull : ((1ull << P->n) - 1);
-    const uint64_t low = (1ull << P->opts.low_qubits) - 1;
-    const size_t G = P->gates.size();
+    std::vector<DraftPass> out;
+    const size_t G = mask.size();
     std::vector<char> done(G, 0);
     size_t left = G;
     while (left) {
@@ -222,12 +296,51 @@ int build_passes(qs_plan *P)
                 blocked |= m;
             }
         }
-        if (mem.empty()) return qs_fail(QS_ERR_UNSUPPORTED, "plan: no gate fits a %d-qubit tile", TQ);
+        if (mem.empty()) return {};
+        out.push_back(DraftPass{T, greedy_groups(mem, mask, 5)});
+    }
+    return out;
+}
+
+std::vector<DraftPass> draft_blocks_first(const std::vector<uint64_t> &mask, int TQ, int MS, uint64_t low)
+{
+    std::vector<size_t> all(mask.size());
+    for (size_t i = 0; i < all.size(); ++i) all[i] = i;
+    Groups g = closure_groups(all, mask, 5);
+    std::vector<DraftPass> out;
+    for (size_t i = 0; i < g.size();) {
+        DraftPass d{low | g[i].first, {}};
+        size_t c = 1;
+        while ((int)c < MS && i + c < g.size() && __builtin_popcountll(d.T | g[i + c].first) <= TQ) {
+            d.T |= g[i + c].first;
+            ++c;
+        }
+        for (size_t j = i; j < i + c; ++j) d.blocks.push_back(std::move(g[j]));
+        out.push_back(std::move(d));
+        i += c;
+    }
+    return out;
+}
+
+int build_passes(qs_plan *P)
+{
+    std::vector<qs_prim> prim;
+    std::vector<uint64_t> mask;
+    int r = lower_all(P, prim, mask);
+    if (r) return r;
+    const int TQ = P->opts.tile_qubits, MS = P->opts.max_sub;
+    const uint64_t every = P->n >= 64 ? ~0ull : ((1ull << P->n) - 1);
+    const uint64_t low = (1ull << P->opts.low_qubits) - 1;
+    std::vector<DraftPass> a = draft_tile_first(mask, TQ, MS, low);
+    if (a.empty() && !mask.empty()) return qs_fail(QS_ERR_UNSUPPORTED, "plan: no gate fits a %d-qubit tile", TQ);
+    std::vector<DraftPass> b = draft_blocks_first(mask, TQ, MS, low);
+    const std::vector<DraftPass> &d = b.size() < a.size() ? b : a;
+    for (const DraftPass &dp : d) {
         PlanPass pass;
-        T = widen(T, every, TQ);
+        const uint64_t T = widen(dp.T, every, TQ);
         mask_to_list(T, pass.T);
         pass.first = P->blocks.size();
-        for (auto &grp : greedy_groups(mem, mask, 5)) {
+        for (const auto &grp : dp.blocks) {
             PlanBlock B;
             B.gates = grp.second;
             mask_to_list(widen(grp.first, T, 5), B.q);
@@ -237,8 +350,8 @@ int build_passes(qs_plan *P)
         }
         pass.count = P->blocks.size() - pass.first;
         int qpos[3][5];
-        for (size_t b = 0; b < pass.count && b < 3; ++b)
-            for (int j = 0; j < 5; ++j) qpos[b][j] = P->blocks[pass.first + b].q[j];
+        for (size_t k = 0; k < pass.count && k < 3; ++k)
+            for (int j = 0; j < 5; ++j) qpos[k][j] = P->blocks[pass.first + k].q[j];
         if (P->n >= TQ && (r = qs_tile_row_orders(P->n, pass.T, (int)pass.count, qpos, pass.rows)))
             return r;                        // narrower states run the gates per gate
         P->passes.push_back(pass);
