@@ -133,3 +133,18 @@ def test_block0_input_mapping_any_column_order(emu):
             assert rc == 0, (it, tpr, emu.tile_emu_error().decode())
         kinds[kind.value] += 1
     assert all(k > 0 for k in kinds), kinds
+
+
+@pytest.mark.parametrize("seed", range(6))
+def test_planner_every_gate_kind_random_mix(emu, seed):
+    """Plans of mixed circuits - every gate kind, 3-qubit gates, control
+    lists, QFT and ansatz pieces concatenated - from both pass drafts
+    (gate-order tiles and closure-first blocks) reproduce the oracle."""
+    from tests.golden.make_golden import every_gate_circuit
+    n = 13 + seed % 4
+    g = np.concatenate([every_gate_circuit(n, 50 + seed), circuits.qft(n),
+                        circuits.random_layers(n, 3, 60 + seed, iswap_frac=0.3),
+                        circuits.vqe_ansatz(n, 2, seed=seed)])
+    for remap, low in ((0, 3), (1, 2), (2, 1)):
+        err, _ = run_emu(emu, n, g, random_state(n, seed), remap, low_qubits=low)
+        assert err < 1e-10, (seed, remap, low, err)
