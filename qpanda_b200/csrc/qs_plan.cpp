@@ -284,7 +284,7 @@ int build_blocks(qs_plan *P)
 //     consecutive blocks share a pass while their qubits and the low qubits
 //     fit one tile.
 // On the 32-qubit depth-16 random circuit the first gives 46 passes and the
-// second 43 (36 with low_qubits = 2); on a QFT they tie.
+// second 37 (33 with low_qubits = 2); on a 28-qubit QFT 51 and 37.
 struct DraftPass {
     uint64_t T;                          // tile qubits before widening
     Groups blocks;
