@@ -116,14 +116,16 @@ typedef std::vector<std::pair<uint64_t, std::vector<size_t>>> Groups;
 // every available gate whose qubits it already has (available: no earlier
 // unplaced gate shares a qubit with it, so it only moves past gates it
 // commutes with), and only when none is left grows by one available gate:
-// the one after which the next closure would take the most gates (then the
-// one adding the fewest qubits, then the earliest).  Taking gates in list
+// the one after which the next closure would take the most gates (ratio =
+// false), or the most gates per qubit added (ratio = true); then the one
+// adding the fewest qubits, then the earliest.  Taking gates in list
 // order instead lets a gate on new qubits in early and fills the group before
 // the gates that would have fitted.  Gate counts per group on the 32-qubit
 // depth-16 random circuit (768 gates): 89 groups in list order, 72 growing by
-// fewest new qubits, 65 with the look-ahead; a 24-qubit QFT 76 -> 55, a
-// 20-qubit 6-layer ansatz 30 -> 21 (fewest new qubits -> look-ahead).
-Groups closure_groups(const std::vector<size_t> &idx, const std::vector<uint64_t> &mask, int k)
+// fewest new qubits, 65 with the look-ahead (63 by ratio); a 24-qubit QFT
+// 76 -> 55, a 20-qubit 6-layer ansatz 30 -> 21 (fewest new qubits ->
+// look-ahead).
+Groups closure_groups(const std::vector<size_t> &idx, const std::vector<uint64_t> &mask, int k, bool ratio)
 {
     Groups out;
     const size_t N = idx.size();
@@ -183,7 +185,12 @@ Groups closure_groups(const std::vector<size_t> &idx, const std::vector<uint64_t
                     trial[t] = 1;
                     const int got = closure(Q | m, nullptr);
                     trial[t] = 0;
-                    if (got > best_n || (got == best_n && add < best_add)) {
+                    // by ratio: (got + 1) / max(add, 1) against the best's, cross-multiplied
+                    const long lhs = (long)(got + 1) * (best_add > 1 ? best_add : 1);
+                    const long rhs = (long)(best_n + 1) * (add > 1 ? add : 1);
+                    const bool better = best == N || (ratio ? (lhs > rhs || (lhs == rhs && add < best_add))
+                                                            : (got > best_n || (got == best_n && add < best_add)));
+                    if (better) {
                         best_n = got;
                         best_add = add;
                         best = t;
@@ -260,8 +267,10 @@ int build_blocks(qs_plan *P)
     std::vector<size_t> all(P->gates.size());
     for (size_t i = 0; i < all.size(); ++i) all[i] = i;
     const uint64_t every = P->n >= 64 ? ~0ull : ((1ull << P->n) - 1);
-    Groups ga = greedy_groups(all, mask, P->max_k), gb = closure_groups(all, mask, P->max_k);
-    for (auto &grp : gb.size() < ga.size() ? gb : ga) {
+    Groups ga = greedy_groups(all, mask, P->max_k), gb = closure_groups(all, mask, P->max_k, false),
+           gc = closure_groups(all, mask, P->max_k, true);
+    Groups &gbc = gc.size() < gb.size() ? gc : gb;
+    for (auto &grp : gbc.size() < ga.size() ? gbc : ga) {
         PlanBlock B;
         B.gates = grp.second;
         mask_to_list(widen(grp.first, every, 5), B.q);
@@ -284,7 +293,7 @@ int build_blocks(qs_plan *P)
 //     consecutive blocks share a pass while their qubits and the low qubits
 //     fit one tile.
 // On the 32-qubit depth-16 random circuit the first gives 46 passes and the
-// second 37 (33 with low_qubits = 2); on a 28-qubit QFT 51 and 37.
+// second 36 (32 with low_qubits = 2); on a 28-qubit QFT 51 and 37.
 struct DraftPass {
     uint64_t T;                          // tile qubits before widening
     Groups blocks;
@@ -331,7 +340,8 @@ std::vector<DraftPass> draft_blocks_first(const std::vector<uint64_t> &mask, int
 {
     std::vector<size_t> all(mask.size());
     for (size_t i = 0; i < all.size(); ++i) all[i] = i;
-    Groups g = closure_groups(all, mask, 5);
+    Groups g0 = closure_groups(all, mask, 5, false), g1 = closure_groups(all, mask, 5, true);
+    Groups &g = g1.size() < g0.size() ? g1 : g0;
     std::vector<DraftPass> out;
     for (size_t i = 0; i < g.size();) {
         DraftPass d{low | g[i].first, {}};
