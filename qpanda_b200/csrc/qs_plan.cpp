@@ -131,9 +131,10 @@ Groups closure_groups(const std::vector<size_t> &idx, const std::vector<uint64_t
     const size_t N = idx.size();
     std::vector<char> done(N, 0);
     size_t left = N, first = 0;
-    // Gates the closure of Q would take (marking them in `mark` when it is
-    // non-null): repeated scans in list order; a scan stops once every qubit
-    // of Q is blocked by an earlier unplaced gate.
+    // How many gates the closure of Q would take (and which, in *take when
+    // take is non-null), gates marked in `trial` counting as placed: repeated
+    // scans in list order; a scan stops once every qubit of Q is blocked by
+    // an earlier unplaced gate.
     std::vector<char> trial(N, 0);
     auto closure = [&](uint64_t Q, std::vector<size_t> *take) {
         int n = 0;
