@@ -70,12 +70,26 @@ float bf16_float(uint16_t h)
     return f;
 }
 
+// What a scan in list order has passed over without placing: a later gate
+// may be placed ahead of those earlier gates only if it commutes with each of
+// them - it shares no qubit with it, or both are diagonal in the computational
+// basis (RZ and CR with any controls: phases, which commute with each other
+// whatever their qubits).  Diagonality is decided by the gate's kind, never by
+// its angle, so that plans rebound to other angles keep a valid order.
+struct Blocker {
+    uint64_t any = 0;                    // qubits of passed non-diagonal gates
+    uint64_t diag = 0;                   // qubits of passed diagonal gates
+    bool free(uint64_t m, bool d) const { return !(m & any) && (d || !(m & diag)); }
+    void add(uint64_t m, bool d) { (d ? diag : any) |= m; }
+};
+
 // Greedy fusion of the gates idx[] (in list order) into groups of at most k
-// qubits: a gate joins the open group when no earlier unplaced gate shares a
-// qubit with it (so it only moves past gates it commutes with) and the group
-// stays within k qubits.  Returns the groups' member lists and qubit masks.
+// qubits: a gate joins the open group when every earlier unplaced gate
+// commutes with it (Blocker) and the group stays within k qubits.  Returns
+// the groups' member lists and qubit masks.
 std::vector<std::pair<uint64_t, std::vector<size_t>>> greedy_groups(const std::vector<size_t> &idx,
-                                                                    const std::vector<uint64_t> &mask, int k,
+                                                                    const std::vector<uint64_t> &mask,
+                                                                    const std::vector<char> &diag, int k,
                                                                     uint64_t seed_mask = 0, int max_groups = 0)
 {
     std::vector<std::pair<uint64_t, std::vector<size_t>>> out;
@@ -87,19 +101,20 @@ std::vector<std::pair<uint64_t, std::vector<size_t>>> greedy_groups(const std::v
         bool changed = true;
         while (changed) {
             changed = false;
-            uint64_t blocked = 0;
+            Blocker bl;
             while (first < idx.size() && done[first]) ++first;
             for (size_t t = first; t < idx.size(); ++t) {
                 if (done[t]) continue;
                 const uint64_t m = mask[idx[t]];
-                if (!(m & blocked) && __builtin_popcountll(Q | m) <= k) {
+                const bool d = diag[idx[t]];
+                if (bl.free(m, d) && __builtin_popcountll(Q | m) <= k) {
                     done[t] = 1;
                     --left;
                     Q |= m;
                     mem.push_back(idx[t]);
                     changed = true;
                 } else {
-                    blocked |= m;
+                    bl.add(m, d);
                 }
             }
         }
@@ -114,8 +129,8 @@ typedef std::vector<std::pair<uint64_t, std::vector<size_t>>> Groups;
 // Closure-first fusion of the gates idx[] (in list order) into groups of at
 // most k qubits.  A group starts with the first unplaced gate, then takes
 // every available gate whose qubits it already has (available: no earlier
-// unplaced gate shares a qubit with it, so it only moves past gates it
-// commutes with), and only when none is left grows by one available gate:
+// unplaced gate fails to commute with it - Blocker), and only when none is
+// left grows by one available gate:
 // the one after which the next closure would take the most gates (ratio =
 // false), or the most gates per qubit added (ratio = true); then the one
 // adding the fewest qubits, then the earliest.  Taking gates in list
@@ -125,7 +140,8 @@ typedef std::vector<std::pair<uint64_t, std::vector<size_t>>> Groups;
 // fewest new qubits, 65 with the look-ahead (63 by ratio); a 24-qubit QFT
 // 76 -> 55, a 20-qubit 6-layer ansatz 30 -> 21 (fewest new qubits ->
 // look-ahead).
-Groups closure_groups(const std::vector<size_t> &idx, const std::vector<uint64_t> &mask, int k, bool ratio)
+Groups closure_groups(const std::vector<size_t> &idx, const std::vector<uint64_t> &mask,
+                      const std::vector<char> &diag, int k, bool ratio)
 {
     Groups out;
     const size_t N = idx.size();
@@ -133,8 +149,8 @@ Groups closure_groups(const std::vector<size_t> &idx, const std::vector<uint64_t
     size_t left = N, first = 0;
     // How many gates the closure of Q would take (and which, in *take when
     // take is non-null), gates marked in `trial` counting as placed: repeated
-    // scans in list order; a scan stops once every qubit of Q is blocked by
-    // an earlier unplaced gate.
+    // scans in list order; a scan stops once every qubit of Q is held by an
+    // earlier unplaced non-diagonal gate.
     std::vector<char> trial(N, 0);
     auto closure = [&](uint64_t Q, std::vector<size_t> *take) {
         int n = 0;
@@ -142,17 +158,18 @@ Groups closure_groups(const std::vector<size_t> &idx, const std::vector<uint64_t
         bool changed = true;
         while (changed) {
             changed = false;
-            uint64_t blocked = 0;
-            for (size_t t = first; t < N && (Q & ~blocked); ++t) {
+            Blocker bl;
+            for (size_t t = first; t < N && (Q & ~bl.any); ++t) {
                 if (done[t] || trial[t]) continue;
                 const uint64_t m = mask[idx[t]];
-                if (!(m & blocked) && !(m & ~Q)) {
+                const bool d = diag[idx[t]];
+                if (bl.free(m, d) && !(m & ~Q)) {
                     trial[t] = 1;
                     touched.push_back(t);
                     ++n;
                     changed = true;
                 } else {
-                    blocked |= m;
+                    bl.add(m, d);
                 }
             }
         }
@@ -175,13 +192,14 @@ Groups closure_groups(const std::vector<size_t> &idx, const std::vector<uint64_t
             std::vector<size_t> take;
             closure(Q, &take);
             for (size_t t : take) place(t, Q, mem);
-            uint64_t blocked = 0;            // grow: available gates that fit
+            Blocker bl;                      // grow: available gates that fit
             int best_n = -1, best_add = 65;
             size_t best = N;
             for (size_t t = first; t < N; ++t) {
                 if (done[t]) continue;
                 const uint64_t m = mask[idx[t]];
-                if (!(m & blocked) && __builtin_popcountll(Q | m) <= k) {
+                const bool d = diag[idx[t]];
+                if (bl.free(m, d) && __builtin_popcountll(Q | m) <= k) {
                     const int add = __builtin_popcountll(m & ~Q);
                     trial[t] = 1;
                     const int got = closure(Q | m, nullptr);
@@ -197,7 +215,7 @@ Groups closure_groups(const std::vector<size_t> &idx, const std::vector<uint64_t
                         best = t;
                     }
                 }
-                blocked |= m;
+                bl.add(m, d);
             }
             if (best == N) break;
             place(best, Q, mem);
@@ -242,15 +260,26 @@ void mask_to_list(uint64_t Q, int *out)
         if ((Q >> q) & 1ull) out[k++] = q;
 }
 
-int lower_all(qs_plan *P, std::vector<qs_prim> &prim, std::vector<uint64_t> &mask)
+// Lowered primitives, qubit masks and (when diag is non-null) which gates are
+// diagonal: RZ and CR records, with or without controls - by kind, checked
+// against their lowered matrices.
+int lower_all(qs_plan *P, std::vector<qs_prim> &prim, std::vector<uint64_t> &mask, std::vector<char> *diag = nullptr)
 {
     const size_t G = P->gates.size();
     prim.resize(G);
     mask.resize(G);
+    if (diag) diag->assign(G, 0);
     for (size_t i = 0; i < G; ++i) {
         int r = qs_lower_gate(P->n, &P->gates[i], &prim[i]);
         if (r) return r;
         mask[i] = qs_gate_qubits(&P->gates[i]);
+        if (diag) {
+            const int op = P->gates[i].op;
+            const qs_prim &q = prim[i];
+            const bool diagonal_matrix = q.kind == QS_PRIM_PHASE ||
+                                         (q.m[2] == 0 && q.m[3] == 0 && q.m[4] == 0 && q.m[5] == 0);
+            (*diag)[i] = (op == QS_OP_RZ || op == QS_OP_CR) && diagonal_matrix;
+        }
         if (__builtin_popcountll(mask[i]) > P->max_k)
             return qs_fail(QS_ERR_UNSUPPORTED, "plan: gate %zu touches %d qubits (fusion width %d)", i,
                            __builtin_popcountll(mask[i]), P->max_k);
@@ -263,13 +292,14 @@ int build_blocks(qs_plan *P)
 {
     std::vector<qs_prim> prim;
     std::vector<uint64_t> mask;
-    int r = lower_all(P, prim, mask);
+    std::vector<char> diag;
+    int r = lower_all(P, prim, mask, &diag);
     if (r) return r;
     std::vector<size_t> all(P->gates.size());
     for (size_t i = 0; i < all.size(); ++i) all[i] = i;
     const uint64_t every = P->n >= 64 ? ~0ull : ((1ull << P->n) - 1);
-    Groups ga = greedy_groups(all, mask, P->max_k), gb = closure_groups(all, mask, P->max_k, false),
-           gc = closure_groups(all, mask, P->max_k, true);
+    Groups ga = greedy_groups(all, mask, diag, P->max_k), gb = closure_groups(all, mask, diag, P->max_k, false),
+           gc = closure_groups(all, mask, diag, P->max_k, true);
     Groups &gbc = gc.size() < gb.size() ? gc : gb;
     for (auto &grp : gbc.size() < ga.size() ? gbc : ga) {
         PlanBlock B;
@@ -294,13 +324,14 @@ int build_blocks(qs_plan *P)
 //     consecutive blocks share a pass while their qubits and the low qubits
 //     fit one tile.
 // On the 32-qubit depth-16 random circuit the first gives 46 passes and the
-// second 36 (32 with low_qubits = 2); on a 28-qubit QFT 51 and 37.
+// second 34 (32 with low_qubits = 2); on a 28-qubit QFT 51 and 31.
 struct DraftPass {
     uint64_t T;                          // tile qubits before widening
     Groups blocks;
 };
 
-std::vector<DraftPass> draft_tile_first(const std::vector<uint64_t> &mask, int TQ, int MS, uint64_t low)
+std::vector<DraftPass> draft_tile_first(const std::vector<uint64_t> &mask, const std::vector<char> &diag, int TQ,
+                                        int MS, uint64_t low)
 {
     std::vector<DraftPass> out;
     const size_t G = mask.size();
@@ -312,14 +343,15 @@ std::vector<DraftPass> draft_tile_first(const std::vector<uint64_t> &mask, int T
         bool changed = true;
         while (changed) {
             changed = false;
-            uint64_t blocked = 0;
+            Blocker bl;
             for (size_t i = 0; i < G; ++i) {
                 if (done[i]) continue;
                 const uint64_t m = mask[i];
-                if (!(m & blocked) && __builtin_popcountll(T | m) <= TQ) {
+                const bool d = diag[i];
+                if (bl.free(m, d) && __builtin_popcountll(T | m) <= TQ) {
                     std::vector<size_t> trial = mem;
                     trial.push_back(i);
-                    if ((int)greedy_groups(trial, mask, 5, 0, MS).size() <= MS) {
+                    if ((int)greedy_groups(trial, mask, diag, 5, 0, MS).size() <= MS) {
                         done[i] = 1;
                         --left;
                         T |= m;
@@ -328,20 +360,21 @@ std::vector<DraftPass> draft_tile_first(const std::vector<uint64_t> &mask, int T
                         continue;
                     }
                 }
-                blocked |= m;
+                bl.add(m, d);
             }
         }
         if (mem.empty()) return {};
-        out.push_back(DraftPass{T, greedy_groups(mem, mask, 5)});
+        out.push_back(DraftPass{T, greedy_groups(mem, mask, diag, 5)});
     }
     return out;
 }
 
-std::vector<DraftPass> draft_blocks_first(const std::vector<uint64_t> &mask, int TQ, int MS, uint64_t low)
+std::vector<DraftPass> draft_blocks_first(const std::vector<uint64_t> &mask, const std::vector<char> &diag, int TQ,
+                                          int MS, uint64_t low)
 {
     std::vector<size_t> all(mask.size());
     for (size_t i = 0; i < all.size(); ++i) all[i] = i;
-    Groups g0 = closure_groups(all, mask, 5, false), g1 = closure_groups(all, mask, 5, true);
+    Groups g0 = closure_groups(all, mask, diag, 5, false), g1 = closure_groups(all, mask, diag, 5, true);
     Groups &g = g1.size() < g0.size() ? g1 : g0;
     std::vector<DraftPass> out;
     for (size_t i = 0; i < g.size();) {
@@ -362,14 +395,15 @@ int build_passes(qs_plan *P)
 {
     std::vector<qs_prim> prim;
     std::vector<uint64_t> mask;
-    int r = lower_all(P, prim, mask);
+    std::vector<char> diag;
+    int r = lower_all(P, prim, mask, &diag);
     if (r) return r;
     const int TQ = P->opts.tile_qubits, MS = P->opts.max_sub;
     const uint64_t every = P->n >= 64 ? ~0ull : ((1ull << P->n) - 1);
     const uint64_t low = (1ull << P->opts.low_qubits) - 1;
-    std::vector<DraftPass> a = draft_tile_first(mask, TQ, MS, low);
+    std::vector<DraftPass> a = draft_tile_first(mask, diag, TQ, MS, low);
     if (a.empty() && !mask.empty()) return qs_fail(QS_ERR_UNSUPPORTED, "plan: no gate fits a %d-qubit tile", TQ);
-    std::vector<DraftPass> b = draft_blocks_first(mask, TQ, MS, low);
+    std::vector<DraftPass> b = draft_blocks_first(mask, diag, TQ, MS, low);
     const std::vector<DraftPass> &d = b.size() < a.size() ? b : a;
     for (const DraftPass &dp : d) {
         PlanPass pass;
