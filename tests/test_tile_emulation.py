@@ -148,3 +148,37 @@ def test_planner_every_gate_kind_random_mix(emu, seed):
     for remap, low in ((0, 3), (1, 2), (2, 1)):
         err, _ = run_emu(emu, n, g, random_state(n, seed), remap, low_qubits=low)
         assert err < 1e-10, (seed, remap, low, err)
+
+
+def test_rebound_plans_keep_a_valid_order(emu):
+    """A plan built for one set of angles, rebound to another (as the batch
+    executor shares plans between circuits of one gate pattern), applies the
+    new circuit exactly - also when the first set has zero angles, which make
+    RX / RY gates diagonal numerically: the planner lets only gates that are
+    diagonal by kind (RZ, CR) pass each other."""
+    from qpanda_b200 import lib
+    n = 14
+    base = np.concatenate([circuits.vqe_ansatz(n, 3, seed=4), circuits.qft(n),
+                           circuits.random_layers(n, 3, 8, iswap_frac=0.2)])
+    zero = base.copy()
+    zero["theta"] = 0.0
+    other = base.copy()
+    other["theta"] = np.random.default_rng(5).uniform(0, 6.28, len(base))
+    emu.tile_emu_rebind.argtypes = [C.c_void_p, C.c_void_p, C.c_size_t, C.POINTER(C.c_void_p)]
+    for proto_gates in (zero, base):
+        p = FusionPlan(n, proto_gates, remap=1, low_qubits=2)
+        g = np.ascontiguousarray(other)
+        h = C.c_void_p()
+        assert emu.tile_emu_rebind(p.handle, g.ctypes.data, len(g), C.byref(h)) == 0, emu.tile_emu_error().decode()
+        init = random_state(n, 9)
+        st = np.ascontiguousarray(init.astype(np.complex128))
+        npass = C.c_int()
+        k = (C.c_int * 3)()
+        rc = emu.tile_emu_apply(h, n, st.ctypes.data, 1, 1, C.byref(npass), k)
+        lib().qs_plan_destroy(h)
+        p.close()
+        assert rc == 0, emu.tile_emu_error().decode()
+        o = OracleState(n)
+        o.set_state(init)
+        o.apply(g)
+        assert np.abs(st - o.state()).max() < 1e-10

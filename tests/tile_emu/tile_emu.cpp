@@ -283,3 +283,13 @@ extern "C" int tile_emu_check_input(int n, const int *T, const int *qpos0, int t
     }
     return 0;
 }
+
+// The plan `proto` rebound to a gate list with the same operations on the
+// same qubits (other angles), as the batched executor does; destroy with
+// qs_plan_destroy.
+extern "C" int tile_emu_rebind(const qs_plan *proto, const qs_gate *gates, size_t count, qs_plan **out)
+{
+    g_err[0] = 0;
+    if (qs_plan_rebind(proto, gates, count, out)) return fail("rebind failed");
+    return 0;
+}
