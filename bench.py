@@ -49,9 +49,8 @@ def parse():
                     help="fused path: tiled passes (up to 3 blocks per pass) or one block per pass")
     ap.add_argument("--max-sub", type=int, default=2, choices=[1, 2, 3],
                     help="tiled passes: fused blocks per pass")
-    ap.add_argument("--low", type=int, default=None, choices=[1, 2, 3, 4, 5],
-                    help="tiled passes: qubits 0..low-1 in every tile (contiguous runs of 2^low amplitudes); "
-                         "default 2 with --remap 1 (measured fastest: 36 passes), 3 in place")
+    ap.add_argument("--low", type=int, default=3, choices=[1, 2, 3, 4, 5],
+                    help="tiled passes: qubits 0..low-1 in every tile (contiguous runs of 2^low amplitudes)")
     ap.add_argument("--remap", type=int, default=1, choices=[0, 1],
                     help="tiled passes: 1 = contiguous tile writes through a second state-size buffer")
     ap.add_argument("--tpr", type=int, default=1, choices=[1, 2],
@@ -72,10 +71,7 @@ def parse():
                     help="vqe-sweep: run with the default batch options instead of the autotuned ones")
     ap.add_argument("--requests", type=int, default=20000, help="requests workload: trace length")
     ap.add_argument("--every", type=int, default=10, help="requests workload: serve every k-th request")
-    args = ap.parse_args()
-    if args.low is None:
-        args.low = 2 if args.remap == 1 else 3
-    return args
+    return ap.parse_args()
 
 
 # ----------------------------------------------------------------- distributed
