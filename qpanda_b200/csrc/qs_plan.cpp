@@ -140,8 +140,14 @@ typedef std::vector<std::pair<uint64_t, std::vector<size_t>>> Groups;
 // fewest new qubits, 65 with the look-ahead (63 by ratio); a 24-qubit QFT
 // 76 -> 55, a 20-qubit 6-layer ansatz 30 -> 21 (fewest new qubits ->
 // look-ahead).
+//
+// With tile_q > 0 the groups are formed for passes of up to per_pass groups
+// whose qubits and tile_low must fit tile_q qubits: a group that continues a
+// pass grows only within that budget, and one whose first gate does not fit
+// starts a new pass.
 Groups closure_groups(const std::vector<size_t> &idx, const std::vector<uint64_t> &mask,
-                      const std::vector<char> &diag, int k, bool ratio)
+                      const std::vector<char> &diag, int k, bool ratio, uint64_t tile_low = 0, int tile_q = 0,
+                      int per_pass = 1)
 {
     Groups out;
     const size_t N = idx.size();
@@ -183,8 +189,15 @@ Groups closure_groups(const std::vector<size_t> &idx, const std::vector<uint64_t
         Q |= mask[idx[t]];
         mem.push_back(idx[t]);
     };
+    uint64_t pass_T = tile_low;              // tile so far of the pass being filled (tile_q > 0)
+    int in_pass = 0;
     while (left) {
         while (first < N && done[first]) ++first;
+        if (tile_q > 0 && in_pass > 0 && __builtin_popcountll(pass_T | mask[idx[first]]) > tile_q) {
+            pass_T = tile_low;               // the next gate does not fit this pass: start a new one
+            in_pass = 0;
+        }
+        const uint64_t budget_T = tile_q > 0 && in_pass > 0 ? pass_T : 0;
         uint64_t Q = 0;
         std::vector<size_t> mem;
         place(first, Q, mem);                // seed: the first unplaced gate
@@ -199,7 +212,8 @@ Groups closure_groups(const std::vector<size_t> &idx, const std::vector<uint64_t
                 if (done[t]) continue;
                 const uint64_t m = mask[idx[t]];
                 const bool d = diag[idx[t]];
-                if (bl.free(m, d) && __builtin_popcountll(Q | m) <= k) {
+                if (bl.free(m, d) && __builtin_popcountll(Q | m) <= k &&
+                    (!budget_T || __builtin_popcountll(budget_T | Q | m) <= tile_q)) {
                     const int add = __builtin_popcountll(m & ~Q);
                     trial[t] = 1;
                     const int got = closure(Q | m, nullptr);
@@ -219,6 +233,13 @@ Groups closure_groups(const std::vector<size_t> &idx, const std::vector<uint64_t
             }
             if (best == N) break;
             place(best, Q, mem);
+        }
+        if (tile_q > 0) {
+            pass_T |= Q;
+            if (++in_pass == per_pass) {
+                pass_T = tile_low;
+                in_pass = 0;
+            }
         }
         out.push_back(std::make_pair(Q, std::move(mem)));
     }
@@ -324,7 +345,7 @@ int build_blocks(qs_plan *P)
 //     consecutive blocks share a pass while their qubits and the low qubits
 //     fit one tile.
 // On the 32-qubit depth-16 random circuit the first gives 46 passes and the
-// second 34 (32 with low_qubits = 2); on a 28-qubit QFT 51 and 31.
+// second 32; on a 28-qubit QFT 51 and 31.
 struct DraftPass {
     uint64_t T;                          // tile qubits before widening
     Groups blocks;
@@ -374,21 +395,26 @@ std::vector<DraftPass> draft_blocks_first(const std::vector<uint64_t> &mask, con
 {
     std::vector<size_t> all(mask.size());
     for (size_t i = 0; i < all.size(); ++i) all[i] = i;
-    Groups g0 = closure_groups(all, mask, diag, 5, false), g1 = closure_groups(all, mask, diag, 5, true);
-    Groups &g = g1.size() < g0.size() ? g1 : g0;
-    std::vector<DraftPass> out;
-    for (size_t i = 0; i < g.size();) {
-        DraftPass d{low | g[i].first, {}};
-        size_t c = 1;
-        while ((int)c < MS && i + c < g.size() && __builtin_popcountll(d.T | g[i + c].first) <= TQ) {
-            d.T |= g[i + c].first;
-            ++c;
+    // four fusions: look-ahead by gates taken or by gates per qubit added,
+    // free or with each pass's later blocks kept within the tile
+    std::vector<DraftPass> best;
+    for (int v = 0; v < 4; ++v) {
+        Groups g = closure_groups(all, mask, diag, 5, v & 1, low, v & 2 ? TQ : 0, MS);
+        std::vector<DraftPass> out;
+        for (size_t i = 0; i < g.size();) {
+            DraftPass d{low | g[i].first, {}};
+            size_t c = 1;
+            while ((int)c < MS && i + c < g.size() && __builtin_popcountll(d.T | g[i + c].first) <= TQ) {
+                d.T |= g[i + c].first;
+                ++c;
+            }
+            for (size_t j = i; j < i + c; ++j) d.blocks.push_back(std::move(g[j]));
+            out.push_back(std::move(d));
+            i += c;
         }
-        for (size_t j = i; j < i + c; ++j) d.blocks.push_back(std::move(g[j]));
-        out.push_back(std::move(d));
-        i += c;
+        if (v == 0 || out.size() < best.size()) best = std::move(out);
     }
-    return out;
+    return best;
 }
 
 int build_passes(qs_plan *P)

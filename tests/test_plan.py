@@ -58,7 +58,7 @@ def test_plan_pass_count_32q():
     t3 = FusionPlan(32, g, kernel="tiled", max_sub=3)
     assert t3.num_launches() <= 38        # up to 3 blocks per pass within 12 tile qubits
     t2 = FusionPlan(32, g, kernel="tiled")  # default: up to 2 blocks per pass
-    assert t3.num_launches() <= t2.num_launches() <= 38
+    assert t3.num_launches() <= t2.num_launches() <= 32
     assert FusionPlan(32, g, kernel="tiled", low_qubits=2).num_launches() <= 32
     for T, blocks in t2.passes():
         assert 1 <= len(blocks) <= 2 and T[:3] == [0, 1, 2] and T == sorted(T)
