@@ -145,6 +145,12 @@ typedef std::vector<std::pair<uint64_t, std::vector<size_t>>> Groups;
 // whose qubits and tile_low must fit tile_q qubits: a group that continues a
 // pass grows only within that budget, and one whose first gate does not fit
 // starts a new pass.
+// Growth candidates whose look-ahead is evaluated per step: the first 24
+// available gates in list order.  On the circuits measured (random layers,
+// QFT, ansatz) the plans equal the unbounded search; a 32-qubit QFT plans in
+// 30 ms instead of 112 (with 12 the plans lose 1-2 passes).
+constexpr int kMaxCandidates = 24;
+
 Groups closure_groups(const std::vector<size_t> &idx, const std::vector<uint64_t> &mask,
                       const std::vector<char> &diag, int k, bool ratio, uint64_t tile_low = 0, int tile_q = 0,
                       int per_pass = 1)
@@ -189,6 +195,8 @@ Groups closure_groups(const std::vector<size_t> &idx, const std::vector<uint64_t
         Q |= mask[idx[t]];
         mem.push_back(idx[t]);
     };
+    uint64_t all_q = 0;                      // every qubit the gates touch
+    for (size_t t = 0; t < N; ++t) all_q |= mask[idx[t]];
     uint64_t pass_T = tile_low;              // tile so far of the pass being filled (tile_q > 0)
     int in_pass = 0;
     while (left) {
@@ -208,13 +216,15 @@ Groups closure_groups(const std::vector<size_t> &idx, const std::vector<uint64_t
             Blocker bl;                      // grow: available gates that fit
             int best_n = -1, best_add = 65;
             size_t best = N;
-            for (size_t t = first; t < N; ++t) {
+            int evaluated = 0;               // the first kMaxCandidates available gates are tried
+            for (size_t t = first; t < N && (all_q & ~bl.any) && evaluated < kMaxCandidates; ++t) {
                 if (done[t]) continue;
                 const uint64_t m = mask[idx[t]];
                 const bool d = diag[idx[t]];
                 if (bl.free(m, d) && __builtin_popcountll(Q | m) <= k &&
                     (!budget_T || __builtin_popcountll(budget_T | Q | m) <= tile_q)) {
                     const int add = __builtin_popcountll(m & ~Q);
+                    ++evaluated;
                     trial[t] = 1;
                     const int got = closure(Q | m, nullptr);
                     trial[t] = 0;
