@@ -58,9 +58,12 @@ def parse():
     ap.add_argument("--qubits", type=int, default=N_QUBITS)
     ap.add_argument("--depth", type=int, default=DEPTH)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-secondary", action="store_true",
+                    help="default workload: skip the short runs of the other workloads")
     ap.add_argument("--workload", default="circuit32",
-                    choices=["circuit32", "vqe-sweep", "requests", "qft28", "passes"],
-                    help="circuit32: the 32-qubit random circuit (default); vqe-sweep: 4096 "
+                    choices=["circuit32", "circuit20", "vqe-sweep", "requests", "qft28", "passes"],
+                    help="circuit32: the 32-qubit random circuit (default); circuit20: the 20-qubit complex128 "
+                         "random circuit on the per-gate path, CPU reference timed directly; vqe-sweep: 4096 "
                          "hardware-efficient-ansatz circuits of 10-22 qubits in one persistent launch; "
                          "requests: Poisson request trace against the server; qft28: 28-qubit QFT on the "
                          "plain per-gate path in complex64 and complex128; passes: the random circuit "
@@ -185,32 +188,98 @@ def peaks():
 
 
 # ----------------------------------------------------------------- reference arm
-def cpu_reference_sample(n_sample, layers_sample, omp=True):
-    """Time the reference CPU backend (compiled from its sources) on a sample of
-    the workload: the same layer structure at n_sample qubits, layers_sample
-    layers, complex128 (its only precision).  Returns seconds."""
-    from oracle.pyoracle import RefState, ref_available
-    from qpanda_b200 import circuits
-    if not ref_available(omp):
-        raise FileNotFoundError("oracle/_ref not built")
-    g = circuits.random_layers(n_sample, layers_sample, SEED, iswap_frac=ISWAP_FRAC)
-    r = RefState(n_sample, omp=omp)
-    t0 = time.perf_counter()
-    r.apply(g)
-    return time.perf_counter() - t0
+REF_QUBITS = 30          # the largest state the reference takes (QPandaAPI.cpp:87), complex128: 16 GiB
+REF_GATES_PER_STEP = 8
 
 
-def cpu_baseline_entry(n, depth, n_sample=26, layers_sample=2):
+def circuit_gate_count(n, depth):
+    """Gates of random_layers(n, depth): a rotation per qubit and a pair gate
+    per matched pair, per layer."""
+    return depth * (n + n // 2)
+
+
+class RefSampler:
+    """The reference CPU backend (CPUQuantumGates.cpp compiled from its
+    sources, oracle/_ref) on the benchmark circuit's structure at
+    min(n, 30) qubits in complex128 (its only precision): each step applies
+    the next `REF_GATES_PER_STEP` gates of that circuit (cycling) and is timed
+    on its own.  A circuit of n qubits is then  seconds per gate x its gate
+    count x 2^(n - sample qubits)  (every gate of the reference loops over the
+    whole state).  omp: the -fopenmp build on every host core, else the
+    shipped single-threaded build."""
+
+    def __init__(self, n, depth, omp):
+        from oracle.pyoracle import RefState, ref_available
+        if not ref_available(omp):
+            raise FileNotFoundError("oracle/_ref not built")
+        self.n, self.depth, self.omp = n, depth, omp
+        self.ns = min(n, REF_QUBITS)
+        self.gates = workload(self.ns, depth)
+        self.state = RefState(self.ns, omp=omp)
+        self.pos = 0
+        self.secs = 0.0
+        self.count = 0
+
+    def step(self, k=REF_GATES_PER_STEP, record=True):
+        idx = [(self.pos + i) % len(self.gates) for i in range(k)]
+        self.pos = (self.pos + k) % len(self.gates)
+        g = self.gates[idx]
+        t0 = time.perf_counter()
+        self.state.apply(g)
+        dt = time.perf_counter() - t0
+        if record:
+            self.secs += dt
+            self.count += k
+        return dt
+
+    def circuit_seconds(self):
+        return self.secs / self.count * circuit_gate_count(self.n, self.depth) * 2 ** (self.n - self.ns)
+
+    def describe(self):
+        cores = os.cpu_count() or 1
+        build = f"-O3 -fopenmp, {cores} threads" if self.omp else "-O3, 1 thread (as shipped)"
+        return (f"reference CPUQuantumGates.cpp ({build}, complex128) on the {self.n}-qubit depth-{self.depth} "
+                f"circuit's structure at {self.ns} qubits: {self.count} gates in {self.secs:.2f} s, "
+                f"{1e3 * self.secs / self.count:.0f} ms per gate; x{circuit_gate_count(self.n, self.depth)} gates"
+                + (f" x{2 ** (self.n - self.ns)} (state size)" if self.n > self.ns else "")
+                + f" = {self.circuit_seconds():.0f} s per circuit"
+                + (f" (extrapolated: a {self.n}-qubit complex128 state is {16 << self.n >> 30} GiB and the reference "
+                   f"caps programs at {REF_QUBITS} qubits)" if self.n > self.ns else ""))
+
+    def close(self):
+        self.state = None
+
+
+def cpu_baseline_entry(n, depth):
+    """The cpu_baseline of the B200 line: a bounded sample on both builds."""
     cores = os.cpu_count() or 1
-    secs = cpu_reference_sample(n_sample, layers_sample, omp=True)
-    scale = (2 ** (n - n_sample)) * (depth / layers_sample)
-    circuit_s = secs * scale
-    return {"value": 1.0 / circuit_s, "unit": "circuits/s", "cores": cores, "kind": "reference",
-            "sample": (f"reference CPUQuantumGates.cpp (-O3 -fopenmp, {cores} threads, complex128) on the "
-                       f"same layer structure at {n_sample} qubits x {layers_sample} layers: {secs:.2f} s; "
-                       f"extrapolated x{scale:.0f} (state size 2^{n - n_sample}, layers {depth}/{layers_sample}) "
-                       f"to {circuit_s:.0f} s per {n}-qubit circuit; a {n}-qubit complex128 state "
-                       f"({16 << n >> 30} GiB) does not fit the host and the reference caps programs at 30 qubits")}
+    omp = RefSampler(n, depth, omp=True)
+    omp.step(record=False)                     # first touch of the 16 GiB state
+    for _ in range(3):
+        omp.step()
+    out = {"value": 1.0 / omp.circuit_seconds(), "unit": "circuits/s", "cores": cores, "kind": "reference",
+           "sample": omp.describe()}
+    omp.close()
+    one = RefSampler(n, depth, omp=False)
+    one.step(k=4)
+    out["single_core"] = {"value": 1.0 / one.circuit_seconds(), "unit": "circuits/s", "cores": 1,
+                          "sample": one.describe()}
+    one.close()
+    out["host"] = host_cpu()
+    return out
+
+
+def host_cpu():
+    model = "unknown"
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    model = line.split(":", 1)[1].strip()
+                    break
+    except OSError:
+        pass
+    return {"nproc": os.cpu_count(), "model": model}
 
 
 def run_reference(args):
@@ -218,29 +287,30 @@ def run_reference(args):
     if rank != 0:
         return
     n, depth = args.qubits, args.depth
-    n_sample, layers_sample = 24, 2
+    if args.workload == "circuit20":
+        return run_reference_circuit20(args)
     cores = os.cpu_count() or 1
-    times = []
+    smp = RefSampler(n, depth, omp=True)
+    smp.step(record=False)                     # first touch of the state
+    steps = []
     for i in range(args.warmup + args.steps):
-        t = cpu_reference_sample(n_sample, layers_sample, omp=True)
+        dt = smp.step(record=i >= args.warmup)
         if i >= args.warmup:
-            times.append(t)
-    scale = (2 ** (n - n_sample)) * (depth / layers_sample)
-    circuit_s = statistics.median(times) * scale
+            steps.append(dt)
+    circuit_s = smp.circuit_seconds()
     value = 1.0 / circuit_s
-    sample = (f"reference CPUQuantumGates.cpp (-O3 -fopenmp, {cores} threads, complex128); each step = "
-              f"{n_sample} qubits x {layers_sample} layers of the same circuit structure, "
-              f"extrapolated x{scale:.0f} to a {n}-qubit depth-{depth} circuit")
+    sample = smp.describe() + f"; each step = {REF_GATES_PER_STEP} consecutive gates of that circuit"
+    smp.close()
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": value, "unit": "circuits/s", "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": statistics.median(times) * 1e3,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": statistics.median(steps) * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic",
         "config": {"workload": f"random-circuit-{n}q-depth{depth}", "qubits": n, "depth": depth,
-                   "iswap_frac": ISWAP_FRAC, "seed": SEED, "sample_qubits": n_sample,
-                   "sample_layers": layers_sample},
+                   "iswap_frac": ISWAP_FRAC, "seed": SEED, "sample_qubits": smp.ns,
+                   "gates_per_step": REF_GATES_PER_STEP},
         "cpu_baseline": {"value": value, "unit": "circuits/s", "cores": cores, "kind": "reference",
-                         "sample": sample},
+                         "sample": sample, "host": host_cpu()},
         "e2e": {"value": value, "unit": "circuits/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }))
 
@@ -443,6 +513,14 @@ def run_b200(args):
     torch.cuda.synchronize()
     e2e_s = max_over_ranks((time.perf_counter() - t0) / e2e_steps, ws, device=f"cuda:{local}")
 
+    sv.close()
+    plan.close()
+
+    # the other benchmark workloads, summarised, on one GPU
+    secondary = None
+    if rank == 0 and ws == 1 and not args.no_secondary:
+        secondary = secondary_summaries(args, gpu_id)
+
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         try:
@@ -481,13 +559,258 @@ def run_b200(args):
                     "phase_ms": {k: 1e3 * v / e2e_steps for k, v in phase_s.items()}},
             "gpu_launches": launches,
             "clocks": clk,
+            "secondary": secondary,
         }
         print(json.dumps(line))
-    sv.close()
-    plan.close()
     if ws > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
+
+
+# ----------------------------------------------------------------- 20-qubit circuit
+C20_QUBITS, C20_LAYERS = 20, 20
+C20_METRIC = "20q random-circuit time, complex128 per-gate path (the drop-in), L2-resident state"
+
+
+def c20_gates():
+    """20 qubits, 20 layers of a rotation on every qubit and CNOTs on a seeded
+    perfect matching: 600 gates."""
+    from qpanda_b200 import circuits
+    return circuits.random_layers(C20_QUBITS, C20_LAYERS, SEED)
+
+
+def circuit20_line(args, steps=None, warmup=None, gpu_id=None):
+    """The 20-qubit circuit on the per-gate kernels in complex128 (the
+    reference's precision): device time per circuit (reset + 600 gates), end
+    to end through the C ABI (gate list from pinned host memory, the full 2^20
+    probability vector and 1024 shots back), and the reference CPU backend
+    timed on the whole circuit (no extrapolation) with one thread and with
+    every host core.  The 16 MiB state stays in L2, so `roofline` is reported
+    against L2-resident traffic, not HBM."""
+    import ctypes as C
+
+    import torch
+    from qpanda_b200 import StateVector, circuits, lib
+    from qpanda_b200.capi import check
+    steps = args.steps if steps is None else steps
+    warmup = args.warmup if warmup is None else warmup
+    n = C20_QUBITS
+    g = c20_gates()
+    L = lib()
+    stream = torch.cuda.current_stream()
+    sv = StateVector(n, "c128")
+    h = sv.handle
+    gp = g.ctypes.data
+
+    def circuit():
+        check(L.qs_reset_zero(h))
+        check(L.qs_gates_apply(h, C.c_void_p(gp), len(g)))
+
+    for _ in range(max(3, warmup)):
+        circuit()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(gpu_id) if gpu_id is not None else None
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(steps + 1)]
+    ev[0].record(stream)
+    for k in range(steps):
+        circuit()
+        ev[k + 1].record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop() if clocks else None
+    per = [ev[k].elapsed_time(ev[k + 1]) / 1e3 for k in range(steps)]
+    circuit_s = statistics.mean(per)
+    # end to end through the C ABI
+    pin_g = torch.empty(g.nbytes, dtype=torch.uint8).pin_memory()
+    pin_g.numpy()[:] = np.frombuffer(g.tobytes(), dtype=np.uint8)
+    qs = np.arange(n, dtype=np.int32)
+    pin_u = torch.empty(SHOTS * n, dtype=torch.float64).pin_memory()
+    pin_u.numpy()[:] = np.random.default_rng(SEED).uniform(size=SHOTS * n)
+    pin_p = torch.empty(1 << n, dtype=torch.float64).pin_memory()
+    pin_o = torch.empty(SHOTS, dtype=torch.int64).pin_memory()
+
+    def e2e_step():
+        check(L.qs_reset_zero(h))
+        check(L.qs_gates_apply(h, C.c_void_p(pin_g.data_ptr()), len(g)))
+        check(L.qs_probs(h, qs.ctypes.data_as(C.POINTER(C.c_int)), n,
+                         C.cast(C.c_void_p(pin_p.data_ptr()), C.POINTER(C.c_double))))
+        check(L.qs_sample(h, qs.ctypes.data_as(C.POINTER(C.c_int)), n,
+                          C.cast(C.c_void_p(pin_u.data_ptr()), C.POINTER(C.c_double)), SHOTS,
+                          C.cast(C.c_void_p(pin_o.data_ptr()), C.POINTER(C.c_uint64))))
+
+    e2e_step()
+    torch.cuda.synchronize()
+    e2e_n = max(3, min(steps, 10))
+    t0 = time.perf_counter()
+    for _ in range(e2e_n):
+        e2e_step()
+    e2e_s = (time.perf_counter() - t0) / e2e_n
+    sv.close()
+    alg = circuits.gate_bytes(g, n, 16)
+    cpu = None
+    if not args.no_cpu_baseline:
+        try:
+            cpu = c20_cpu()
+        except Exception as ex:   # the reference build is absent
+            cpu = {"value": None, "unit": "circuits/s", "kind": "reference", "sample": f"unavailable: {ex}"}
+    return {
+        "metric": C20_METRIC, "value": 1.0 / circuit_s, "unit": "circuits/s", "n_gpus": 1, "steps": steps,
+        "warmup": max(3, warmup), "ms_per_step": circuit_s * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64 (complex128 state)", "data": "synthetic",
+        "config": {"workload": "random-circuit-20q-depth20-c128", "qubits": n, "layers": C20_LAYERS,
+                   "gates": len(g), "seed": SEED, "path": "per-gate",
+                   "l2": "16 MiB state, L2-resident by design (the configuration's size); no flush"},
+        "roofline": {"bound": "l2", "kernel": "k_pair / k_phase (per gate)", "achieved": alg / circuit_s / 1e9,
+                     "peak": None, "unit": "GB/s", "frac": None, "traffic": None,
+                     "note": "algorithmic bytes of the 600 gates per second; the state never leaves L2"},
+        "cpu_baseline": cpu,
+        "e2e": {"value": 1.0 / e2e_s, "unit": "circuits/s", "h2d_bytes_per_step": int(g.nbytes + SHOTS * n * 8),
+                "d2h_bytes_per_step": int(8 << n) + SHOTS * 8,
+                "includes": "gate list from pinned host memory, the circuit, the full probability vector and "
+                            "1024 shots to the host"},
+        "gpu_launches": steps * (1 + len(g)),
+        "clocks": clk,
+    }
+
+
+def c20_cpu():
+    """The reference CPU backend on the whole 20-qubit circuit (600 gates)
+    plus its pMeasure over all qubits, timed directly: one thread (the
+    shipped build) and every host core (-fopenmp)."""
+    from oracle.pyoracle import RefState, ref_available
+    g = c20_gates()
+    qs = list(range(C20_QUBITS))
+    out = {}
+    for omp in (True, False):
+        if not ref_available(omp):
+            raise FileNotFoundError("oracle/_ref not built")
+        times = []
+        for _ in range(2 if omp else 1):
+            r = RefState(C20_QUBITS, omp=omp)
+            t0 = time.perf_counter()
+            r.apply(g)
+            r.pmeasure(qs)
+            times.append(time.perf_counter() - t0)
+        out[omp] = min(times)
+    cores = os.cpu_count() or 1
+    return {"value": 1.0 / out[True], "unit": "circuits/s", "cores": cores, "kind": "reference",
+            "sample": (f"reference CPUQuantumGates.cpp, the whole circuit (600 gates) and pMeasure over the 20 "
+                       f"qubits, complex128: {out[True]:.3f} s with -fopenmp on {cores} threads (value), "
+                       f"{out[False]:.3f} s as shipped on 1 thread; measured, not extrapolated"),
+            "single_core": {"value": 1.0 / out[False], "unit": "circuits/s", "cores": 1},
+            "host": host_cpu()}
+
+
+def run_circuit20(args):
+    ws, rank, local = dist_setup()
+    import torch
+    torch.cuda.set_device(local)
+    dist_init(ws, "nccl")
+    props = torch.cuda.get_device_properties(local)
+    gpu_id = "GPU-" + str(props.uuid) if getattr(props, "uuid", None) else str(local)
+    barrier(ws)
+    if rank != 0 or ws > 1:
+        args.no_cpu_baseline = True
+    line = circuit20_line(args, gpu_id=gpu_id)
+    barrier(ws)
+    elapsed = max_over_ranks(line["ms_per_step"] / 1e3, ws, device=f"cuda:{local}")
+    line["value"] = ws / elapsed
+    line["n_gpus"] = ws
+    line["config"]["parallelism"] = f"replicas x{ws}"
+    if rank == 0:
+        print(json.dumps(line))
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def run_reference_circuit20(args):
+    from oracle.pyoracle import RefState
+    g = c20_gates()
+    qs = list(range(C20_QUBITS))
+    times = []
+    for i in range(args.warmup + args.steps):
+        r = RefState(C20_QUBITS, omp=True)
+        t0 = time.perf_counter()
+        r.apply(g)
+        r.pmeasure(qs)
+        if i >= args.warmup:
+            times.append(time.perf_counter() - t0)
+    value = 1.0 / statistics.median(times)
+    cores = os.cpu_count() or 1
+    print(json.dumps({
+        "impl": "reference", "metric": C20_METRIC, "value": value, "unit": "circuits/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": statistics.median(times) * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "random-circuit-20q-depth20-c128", "qubits": C20_QUBITS, "layers": C20_LAYERS,
+                   "seed": SEED},
+        "cpu_baseline": {"value": value, "unit": "circuits/s", "cores": cores, "kind": "reference",
+                         "sample": (f"reference CPUQuantumGates.cpp (-fopenmp, {cores} threads, complex128): "
+                                    "each step = the whole circuit and pMeasure over all qubits"),
+                         "host": host_cpu()},
+        "e2e": {"value": value, "unit": "circuits/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }))
+
+
+# ----------------------------------------------------------------- secondary workloads
+def secondary_summaries(args, gpu_id):
+    """Short runs of the other benchmark workloads for the default line, each
+    timed with CUDA events and its clocks sampled: the 20-qubit complex128
+    circuit (with the reference CPU backend timed on it directly), the 28-qubit
+    QFT on the per-gate kernels, the 4096-circuit batched sweep (autotuned on
+    every 64th circuit) and a slice of the request trace."""
+    import copy
+    quiet = copy.copy(args)
+    quiet.no_cpu_baseline = True
+    out = {}
+
+    def keep(name, f):
+        t0 = time.perf_counter()
+        try:
+            out[name] = f()
+        except Exception as ex:
+            out[name] = {"error": f"{type(ex).__name__}: {ex}"}
+        out[name]["wall_s"] = round(time.perf_counter() - t0, 1)
+
+    def c20():
+        ln = circuit20_line(args, steps=10, warmup=3, gpu_id=gpu_id)
+        cpu = ln["cpu_baseline"] or {}
+        return {"workload": ln["config"]["workload"], "circuits_per_s": ln["value"], "ms_per_circuit": ln["ms_per_step"],
+                "e2e_circuits_per_s": ln["e2e"]["value"], "e2e_includes": ln["e2e"]["includes"],
+                "l2_resident_gbs": ln["roofline"]["achieved"],
+                "cpu_reference_circuits_per_s": cpu.get("value"), "cpu_cores": cpu.get("cores"),
+                "cpu_reference_1core_circuits_per_s": (cpu.get("single_core") or {}).get("value"),
+                "cpu_sample": cpu.get("sample"), "clocks": ln["clocks"]}
+
+    def qft():
+        ln = qft_line(quiet, 28, steps=2, warmup=1, gpu_id=gpu_id)
+        res = {"workload": ln["config"]["workload"], "peak_gbs": ln["roofline"]["peak"],
+               "peak_source": ln["roofline"]["peak_source"], "error_c64": ln["error_c64"],
+               "fused_c64": ln["fused_c64"], "clocks": ln["clocks"]}
+        for dt in ("complex64", "complex128"):
+            res[dt] = {"circuit_ms": 1e3 * ln[dt]["circuit_s"], "hbm_gbs_effective": ln[dt]["hbm_gbs_effective"],
+                       "kernels": {k: {"gbs": v["gbs"], "frac": v["frac"], "mean_ms": v["mean_ms"]}
+                                   for k, v in ln[dt]["kernels"].items()}}
+        return res
+
+    def vqe():
+        ln = vqe_line(quiet, steps=3, warmup=3, tune_stride=64, gpu_id=gpu_id)
+        return {"workload": "vqe-sweep-4096", "circuits_per_s": ln["value"], "ms_per_sweep": ln["ms_per_step"],
+                "hbm_gbs": ln["roofline"]["achieved"], "frac": ln["roofline"]["frac"],
+                "e2e_circuits_per_s": ln["e2e"]["value"], "autotuned": ln["config"]["autotuned"],
+                "build_s": ln["config"]["build_s"], "clocks": ln["clocks"]}
+
+    def req():
+        ln = requests_line(quiet, 2000, 20, gpu_id=gpu_id, budget_gb=100)
+        return {"workload": "requests", "served": ln["config"]["served"], "failed": ln["failed"],
+                "circuits_per_s": ln["value"], "latency_s": ln["latency_s"], "service_s": ln["service_s"],
+                "subsample": "every 20th of the first 2000 requests of the trace (0.1 of its rate), real time",
+                "clocks": ln["clocks"]}
+
+    keep("circuit20_c128", c20)
+    keep("qft28", qft)
+    keep("vqe_sweep", vqe)
+    keep("requests", req)
+    return out
 
 
 # ----------------------------------------------------------------- batched sweep
@@ -508,52 +831,47 @@ def sweep_bytes(sweep):
     return tot
 
 
-def run_vqe_sweep(args):
+def vqe_line(args, steps, warmup, tune_stride=16, gpu_id=None, rank=0):
+    """The batched sweep on one GPU: autotune (every tune_stride-th circuit),
+    build, `warmup` + `steps` graph replays timed with CUDA events, then end
+    to end through the C ABI.  Returns the result line."""
     import ctypes as C
 
     import torch
-    ws, rank, local = dist_setup()
-    torch.cuda.set_device(local)
-    dist_init(ws, "nccl")
     from qpanda_b200 import Batch, autotune_batch, circuits
     from qpanda_b200.capi import _concat, _iptr, BatchOpts, check, lib
 
     sweep = circuits.vqe_sweep(args.circuits, SWEEP_SEED + rank)
     t0 = time.perf_counter()
     if args.no_autotune:
-        from qpanda_b200.capi import BatchOpts
         opts, tune_ms = BatchOpts(), None
         check(lib().qs_batch_default_opts(C.byref(opts)))
     else:
-        opts, tune_ms = autotune_batch(sweep, stride=16)
+        opts, tune_ms = autotune_batch(sweep, stride=tune_stride)
     tune_s = time.perf_counter() - t0
     t0 = time.perf_counter()
     b = Batch(sweep, opts=opts)
     build_s = time.perf_counter() - t0
     stream = torch.cuda.current_stream()
-    for _ in range(args.warmup):
+    for _ in range(max(3, warmup)):
         b.run(C.c_void_p(stream.cuda_stream))
     torch.cuda.synchronize()
-    barrier(ws)
-    props = torch.cuda.get_device_properties(local)
-    gpu_id = "GPU-" + str(props.uuid) if getattr(props, "uuid", None) else str(local)
-    clocks = ClockSampler(gpu_id)
-    ev = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+    clocks = ClockSampler(gpu_id) if gpu_id is not None else None
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(steps + 1)]
     ev[0].record(stream)
-    for k in range(args.steps):
+    for k in range(steps):
         b.run(C.c_void_p(stream.cuda_stream))
         ev[k + 1].record(stream)
     torch.cuda.synchronize()
-    clk = clocks.stop()
-    barrier(ws)
-    per = [ev[k].elapsed_time(ev[k + 1]) / 1e3 for k in range(args.steps)]
-    step_s = max_over_ranks(statistics.mean(per), ws, device=f"cuda:{local}")
+    clk = clocks.stop() if clocks else None
+    per = [ev[k].elapsed_time(ev[k + 1]) / 1e3 for k in range(steps)]
+    step_s = statistics.mean(per)
     zz = b.zz()
     alg = sweep_bytes(sweep)
     peak, peak_kind = peaks()
     # e2e: build from host gate records, run, read every <ZZ> back
     nq, gates, offs = _concat(sweep)
-    e2e_steps = max(1, min(args.steps, 2))
+    e2e_steps = max(1, min(steps, 2))
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     for _ in range(e2e_steps):
@@ -566,9 +884,10 @@ def run_vqe_sweep(args):
         out = np.empty(cnt.value)
         check(lib().qs_batch_zz(h, out.ctypes.data_as(C.POINTER(C.c_double)), C.byref(cnt)))
         lib().qs_batch_destroy(h)
-    e2e_s = max_over_ranks((time.perf_counter() - t0) / e2e_steps, ws, device=f"cuda:{local}")
+    e2e_s = (time.perf_counter() - t0) / e2e_steps
+    b.close()
     cpu = None
-    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+    if not args.no_cpu_baseline:
         try:
             from oracle.pyoracle import RefState
             sample = sweep[:: max(1, len(sweep) // 48)]
@@ -587,29 +906,47 @@ def run_vqe_sweep(args):
                               f"gate x amplitude work ({work_all / work_s:.1f}x)")}
         except Exception as ex:
             cpu = {"value": None, "unit": "circuits/s", "kind": "reference", "sample": f"unavailable: {ex}"}
+    return {
+        "metric": "batched VQE sweep throughput (circuits/s)", "value": len(sweep) / step_s,
+        "unit": "circuits/s", "n_gpus": 1, "steps": steps, "warmup": max(3, warmup),
+        "ms_per_step": step_s * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "bf16x3->f32 (complex64 states)", "data": "synthetic",
+        "config": {"workload": "vqe-sweep", "circuits": len(sweep), "qubits": "U{10..22}",
+                   "layers": "U{4..12}", "seed": SWEEP_SEED, "outputs": "all <Z_i Z_{i+1}>",
+                   "launch": "one persistent kernel, CUDA graph replay",
+                   "autotuned": {"max_sub": opts.max_sub, "low_qubits": opts.low_qubits,
+                                 "order": opts.order, "sample_ms": tune_ms, "tune_s": tune_s,
+                                 "stride": None if args.no_autotune else tune_stride},
+                   "build_s": build_s, "l2": "21 GB of states >> L2"},
+        "roofline": {"bound": "hbm", "kernel": "k_batch", "achieved": alg / step_s / 1e9, "peak": peak,
+                     "unit": "GB/s", "frac": alg / step_s / 1e9 / peak, "peak_source": peak_kind,
+                     "traffic": None, "algorithmic_bytes_per_launch": alg, "launch_s": step_s},
+        "zz_checksum": float(sum(float(np.sum(z)) for z in zz)),
+        "cpu_baseline": cpu,
+        "e2e": {"value": len(sweep) / e2e_s, "unit": "circuits/s",
+                "h2d_bytes_per_step": int(gates.nbytes), "d2h_bytes_per_step": int(8 * sum(len(z) for z in zz)),
+                "includes": "planning and upload of every circuit, the run, all <ZZ> to the host"},
+        "gpu_launches": steps, "clocks": clk,
+    }
+
+
+def run_vqe_sweep(args):
+    import torch
+    ws, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    dist_init(ws, "nccl")
+    props = torch.cuda.get_device_properties(local)
+    gpu_id = "GPU-" + str(props.uuid) if getattr(props, "uuid", None) else str(local)
+    if rank != 0 or ws > 1:
+        args.no_cpu_baseline = True
+    barrier(ws)
+    line = vqe_line(args, args.steps, args.warmup, gpu_id=gpu_id, rank=rank)
+    barrier(ws)
+    step_s = max_over_ranks(line["ms_per_step"] / 1e3, ws, device=f"cuda:{local}")
+    line["value"] = ws * args.circuits / step_s
+    line["n_gpus"] = ws
     if rank == 0:
-        print(json.dumps({
-            "metric": "batched VQE sweep throughput (circuits/s)", "value": ws * len(sweep) / step_s,
-            "unit": "circuits/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": step_s * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "bf16x3->f32 (complex64 states)", "data": "synthetic",
-            "config": {"workload": "vqe-sweep", "circuits": len(sweep), "qubits": "U{10..22}",
-                       "layers": "U{4..12}", "seed": SWEEP_SEED, "outputs": "all <Z_i Z_{i+1}>",
-                       "launch": "one persistent kernel, CUDA graph replay",
-                       "autotuned": {"max_sub": opts.max_sub, "low_qubits": opts.low_qubits,
-                                     "order": opts.order, "sample_ms": tune_ms, "tune_s": tune_s},
-                       "build_s": build_s, "l2": "21 GB of states >> L2"},
-            "roofline": {"bound": "hbm", "kernel": "k_batch", "achieved": alg / step_s / 1e9, "peak": peak,
-                         "unit": "GB/s", "frac": alg / step_s / 1e9 / peak, "peak_source": peak_kind,
-                         "traffic": None, "algorithmic_bytes_per_launch": alg, "launch_s": step_s},
-            "zz_checksum": float(sum(float(np.sum(z)) for z in zz)),
-            "cpu_baseline": cpu,
-            "e2e": {"value": ws * len(sweep) / e2e_s, "unit": "circuits/s",
-                    "h2d_bytes_per_step": int(gates.nbytes), "d2h_bytes_per_step": int(8 * sum(len(z) for z in zz)),
-                    "includes": "planning and upload of every circuit, the run, all <ZZ> to the host"},
-            "gpu_launches": args.steps, "clocks": clk,
-        }))
-    b.close()
+        print(json.dumps(line))
     if ws > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
@@ -619,20 +956,18 @@ def run_vqe_sweep(args):
 TRACE_SEED = 4242
 
 
-def run_requests(args):
-    """Replay a seeded Poisson request trace against the continuous-batching
-    server in real time; report circuits/s and latency percentiles."""
+def requests_line(args, n_requests, every, gpu_id=None, rank=0, budget_gb=120):
+    """Replay requests 0, every, 2 every, ... of the first n_requests of the
+    seeded Poisson trace against the continuous-batching server, each at its
+    original arrival time; returns the line (circuits/s, latency
+    percentiles)."""
     import threading
 
-    import torch
-    ws, rank, local = dist_setup()
-    torch.cuda.set_device(local)
-    dist_init(ws, "nccl")
     from qpanda_b200 import Server, circuits
 
-    trace = circuits.request_trace(args.requests, TRACE_SEED + rank)
-    sample = trace[:: args.every]
-    srv = Server(budget_bytes=120 << 30, slots=8)
+    trace = circuits.request_trace(n_requests, TRACE_SEED + rank)
+    sample = trace[:: every]
+    srv = Server(budget_bytes=budget_gb << 30, slots=8)
     # warm-up: one small request of each kind (module loading, pools)
     for kind in ("shots", "probs"):
         g = circuits.random_layers(14, 2, 1)
@@ -668,9 +1003,7 @@ def run_requests(args):
     done_submitting = threading.Event()
     th = threading.Thread(target=waiter)
     th.start()
-    props = torch.cuda.get_device_properties(local)
-    gpu_id = "GPU-" + str(props.uuid) if getattr(props, "uuid", None) else str(local)
-    clocks = ClockSampler(gpu_id)
+    clocks = ClockSampler(gpu_id) if gpu_id is not None else None
     t0 = time.perf_counter()
     alg_bytes = 0
     for req in sample:
@@ -686,7 +1019,7 @@ def run_requests(args):
             ids.append((rid, req, t_sub))
     done_submitting.set()
     th.join()
-    clk = clocks.stop()
+    clk = clocks.stop() if clocks else None
     ends = [t + lat for (_, t, lat, _, ok) in results.values() if ok]
     makespan = max(ends) - min(t for (_, t, _, _, _) in results.values())
     lats = np.array([lat for (_, _, lat, _, ok) in results.values() if ok])
@@ -701,17 +1034,16 @@ def run_requests(args):
             nl = FusionPlan(q, circuits.random_layers(q, req["depth"], req["seed"])).num_launches()
             alg_bytes += 2 * 8 * (1 << q) * nl
     peak, peak_kind = peaks()
-    if rank == 0:
-        print(json.dumps({
-            "metric": "request loop: circuits/s with p50/p99 latency", "value": ws * n_ok / makespan,
-            "unit": "circuits/s", "n_gpus": ws, "steps": 1, "warmup": 2, "ms_per_step": makespan * 1e3,
+    return {
+            "metric": "request loop: circuits/s with p50/p99 latency", "value": n_ok / makespan,
+            "unit": "circuits/s", "n_gpus": 1, "steps": 1, "warmup": 2, "ms_per_step": makespan * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "bf16x3->f32 (complex64 states)", "data": "synthetic",
-            "config": {"workload": "requests", "trace": args.requests, "served": len(sample), "every": args.every,
-                       "rate_per_s": 2000.0 / args.every, "qubits": "U{8..30}", "depth": "U{4..32}",
+            "config": {"workload": "requests", "trace": n_requests, "served": len(sample), "every": every,
+                       "rate_per_s": 2000.0 / every, "qubits": "U{8..30}", "depth": "U{4..32}",
                        "kinds": "1024 shots or full probability vector", "seed": TRACE_SEED,
-                       "server": {"slots": 8, "hbm_budget_gb": 120, "max_concurrent": stats["max_concurrent"]},
-                       "subsample": (f"every {args.every}th request of the {args.requests}-request trace, at its "
+                       "server": {"slots": 8, "hbm_budget_gb": budget_gb, "max_concurrent": stats["max_concurrent"]},
+                       "subsample": (f"every {every}th request of the first {n_requests} of the trace, at its "
                                      "original arrival time (the full trace is about 1.3 PB of state traffic)")},
             "latency_s": {"p50": float(np.percentile(lats, 50)), "p99": float(np.percentile(lats, 99)),
                           "mean": float(lats.mean())},
@@ -721,11 +1053,27 @@ def run_requests(args):
                          "peak": peak, "unit": "GB/s", "frac": alg_bytes / makespan / 1e9 / peak,
                          "peak_source": peak_kind, "traffic": None, "algorithmic_bytes_per_launch": alg_bytes,
                          "launch_s": makespan},
-            "e2e": {"value": ws * n_ok / makespan, "unit": "circuits/s",
+            "e2e": {"value": n_ok / makespan, "unit": "circuits/s",
                     "h2d_bytes_per_step": None, "d2h_bytes_per_step": None,
                     "includes": "host circuit generation, submission in real time, shots to the host"},
             "clocks": clk,
-        }))
+    }
+
+
+def run_requests(args):
+    import torch
+    ws, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    dist_init(ws, "nccl")
+    props = torch.cuda.get_device_properties(local)
+    gpu_id = "GPU-" + str(props.uuid) if getattr(props, "uuid", None) else str(local)
+    line = requests_line(args, args.requests, args.every, gpu_id=gpu_id, rank=rank)
+    makespan = max_over_ranks(line["ms_per_step"] / 1e3, ws, device=f"cuda:{local}")
+    served = line["config"]["served"] - line["failed"]
+    line["value"] = line["e2e"]["value"] = ws * served / makespan
+    line["n_gpus"] = ws
+    if rank == 0:
+        print(json.dumps(line))
     if ws > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
@@ -735,21 +1083,17 @@ def run_requests(args):
 QFT_SEED = 28028
 
 
-def run_qft(args):
-    """28-qubit QFT (H and CR(pi/2^k) on all pairs, then the reversal swaps) on a
+def qft_line(args, n, steps, warmup, gpu_id=None):
+    """n-qubit QFT (H and CR(pi/2^k) on all pairs, then the reversal swaps) on a
     seeded normalised complex Gaussian state, on the plain per-gate path in
     complex64 and complex128: per-kernel HBM GB/s from CUDA events after every
-    gate, and the complex64 error against the complex128 run."""
+    gate, and the complex64 error against the complex128 run.  Returns the line."""
     import ctypes as C
 
     import torch
-    ws, rank, local = dist_setup()
-    torch.cuda.set_device(local)
-    dist_init(ws, "nccl")
     from qpanda_b200 import FusionPlan, StateVector, circuits, lib
     from qpanda_b200.capi import OP, check
 
-    n = 28 if args.qubits == N_QUBITS else args.qubits
     gates = circuits.qft(n)
     rng = np.random.default_rng(QFT_SEED)
     init = rng.standard_normal(1 << n) + 1j * rng.standard_normal(1 << n)
@@ -762,14 +1106,12 @@ def run_qft(args):
     gptr = [gates[i:i + 1].ctypes.data for i in range(len(gates))]
     peak, peak_kind = peaks()
     out, states = {}, {}
-    props = torch.cuda.get_device_properties(local)
-    gpu_id = "GPU-" + str(props.uuid) if getattr(props, "uuid", None) else str(local)
-    clocks = ClockSampler(gpu_id)
+    clocks = ClockSampler(gpu_id) if gpu_id is not None else None
     for dt, amp_b, npdt in (("c64", 8, np.complex64), ("c128", 16, np.complex128)):
         sv = StateVector(n, dt)
         host = init.astype(npdt)
         kinds, circ = {}, []
-        for k in range(args.warmup + args.steps):
+        for k in range(warmup + steps):
             sv.set_state(host)
             torch.cuda.synchronize()
             ev = [torch.cuda.Event(enable_timing=True) for _ in range(len(gates) + 1)]
@@ -778,7 +1120,7 @@ def run_qft(args):
                 check(L.qs_gate_apply(sv.handle, C.c_void_p(gptr[i])))
                 ev[i + 1].record(stream)
             torch.cuda.synchronize()
-            if k < args.warmup:
+            if k < warmup:
                 continue
             circ.append(ev[0].elapsed_time(ev[-1]) / 1e3)
             for i in range(len(gates)):
@@ -788,13 +1130,13 @@ def run_qft(args):
         for op, ts in kinds.items():
             t = statistics.mean(ts)
             gbs = 2 * amp_b * frac_of[op] * (1 << n) / t / 1e9
-            table[kind_of[op]] = {"launches_per_circuit": len(ts) // args.steps, "mean_ms": t * 1e3,
+            table[kind_of[op]] = {"launches_per_circuit": len(ts) // steps, "mean_ms": t * 1e3,
                                   "gbs": gbs, "frac": gbs / peak}
         cs = statistics.mean(circ)
         out[dt] = {"circuit_s": cs, "hbm_gbs_effective": circuits.gate_bytes(gates, n, amp_b) / cs / 1e9,
                    "kernels": table}
         states[dt] = sv
-    clk = clocks.stop()
+    clk = clocks.stop() if clocks else None
     a, d = states["c64"], states["c128"]
     ip = a.inner(d)
     mx, ss = a.diff(d)
@@ -826,7 +1168,7 @@ def run_qft(args):
     check(L.qs_get_state(a.handle, C.c_void_p(pin_out.data_ptr()), 0))
     e2e_s = time.perf_counter() - t0
     cpu = None
-    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+    if not args.no_cpu_baseline:
         try:
             from oracle.pyoracle import RefState
             ns = 22
@@ -842,13 +1184,15 @@ def run_qft(args):
                               f"({secs * scale:.0f} s); value = the same algorithmic bytes per second")}
         except Exception as ex:
             cpu = {"value": None, "unit": "GB/s", "kind": "reference", "sample": f"unavailable: {ex}"}
-    if rank == 0:
-        dom = max(out["c64"]["kernels"], key=lambda k: out["c64"]["kernels"][k]["mean_ms"] *
-                  out["c64"]["kernels"][k]["launches_per_circuit"])
-        dk = out["c64"]["kernels"][dom]
-        print(json.dumps({
+    dom = max(out["c64"]["kernels"], key=lambda k: out["c64"]["kernels"][k]["mean_ms"] *
+              out["c64"]["kernels"][k]["launches_per_circuit"])
+    dk = out["c64"]["kernels"][dom]
+    a.close()
+    d.close()
+    if True:
+        return ({
             "metric": "28q QFT HBM GB/s, plain per-gate path", "value": out["c64"]["hbm_gbs_effective"],
-            "unit": "GB/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+            "unit": "GB/s", "n_gpus": 1, "steps": steps, "warmup": warmup,
             "ms_per_step": out["c64"]["circuit_s"] * 1e3, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32 (complex64 state); f64 line under complex128", "data": "synthetic",
             "config": {"workload": f"qft-{n}q", "qubits": n, "gates": len(gates), "seed": QFT_SEED,
@@ -861,10 +1205,27 @@ def run_qft(args):
             "e2e": {"value": circuits.gate_bytes(gates, n, 8) / e2e_s / 1e9, "unit": "GB/s",
                     "h2d_bytes_per_step": 8 << n, "d2h_bytes_per_step": 8 << n,
                     "includes": "host state in, the QFT per gate, host state out (complex64)"},
-            "gpu_launches": len(gates) * (args.warmup + args.steps) * 2, "clocks": clk,
-        }))
-    a.close()
-    d.close()
+            "gpu_launches": len(gates) * (warmup + steps) * 2, "clocks": clk,
+        })
+
+
+def run_qft(args):
+    import torch
+    ws, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    dist_init(ws, "nccl")
+    props = torch.cuda.get_device_properties(local)
+    gpu_id = "GPU-" + str(props.uuid) if getattr(props, "uuid", None) else str(local)
+    if rank != 0 or ws > 1:
+        args.no_cpu_baseline = True
+    n = 28 if args.qubits == N_QUBITS else args.qubits
+    line = qft_line(args, n, args.steps, args.warmup, gpu_id=gpu_id)
+    line["n_gpus"] = ws
+    if rank == 0:
+        print(json.dumps(line))
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
 
 
 # ----------------------------------------------------------------- pass profile
@@ -918,6 +1279,8 @@ def main():
         run_qft(args)
     elif args.workload == "passes":
         run_passes(args)
+    elif args.workload == "circuit20":
+        run_circuit20(args)
     else:
         run_b200(args)
 

@@ -227,6 +227,10 @@ typedef struct qs_plan_opts {
     int threads_per_row;   /* tiled passes: 1 = each of a lane's 128 threads owns a row of the tile (default);
                               2 = 256 threads per lane, two per row, each with 16 of its 32 columns
                               (measured 3-4 % slower) */
+    int tile_in_tmem;      /* tiled passes: 1 = the tile is the MMAs' A operand in tensor memory and the
+                              block matrices the B operand in shared memory (default), for every pass
+                              with two tile qubits outside all of its blocks and position 0 in its tile;
+                              other passes, and 0, keep the tile in shared memory */
 } qs_plan_opts;
 /* Defaults: 5-qubit blocks, tiled passes of 12 qubits with up to 2 blocks
  * (a pass of 3 blocks saves a pass but runs on a kernel with fewer resident

@@ -16,6 +16,11 @@
  * libstdc++ is (a+ib)(c+id) = (ac-bd) + i(ad+bc); products by a real scalar
  * scale both parts.  std::abs(complex<double>) is hypot(re, im).
  *
+ * Large states: the per-amplitude loops of the gates run on OpenMP threads
+ * (-fopenmp).  Every amplitude is still computed by the same expression from
+ * the same inputs, so results do not depend on the thread count; sums
+ * (probabilities, norms) stay serial, in the reference's order.
+ *
  * Differences from the reference, on purpose:
  *  - measurements take the uniform u as an argument instead of drawing it
  *    from the global 16807 generator (QuantumGates.cpp:46-85);
@@ -34,6 +39,7 @@
 
 #define SQ2 0.707106781186548          /* CPUQuantumGates.cpp:36 */
 #define POW2(n) (1ull << (n))
+#define PAR_MIN (1ll << 16)            /* loops shorter than this stay on one thread */
 
 typedef struct orc_state {
     int n;
@@ -113,10 +119,11 @@ static int for_each_pair(orc_state *s, int t, const int *ctrl, int nctrl,
     }
     holes[nctrl] = t;
     if (sort_unique(holes, nctrl + 1)) return -1;
-    uint64_t M = s->N >> (nctrl + 1);
+    long long M = (long long)(s->N >> (nctrl + 1));
     uint64_t st = POW2(t);
-    for (uint64_t i = 0; i < M; ++i) {
-        uint64_t idx = insert_zeros(i, holes, nctrl + 1) | block;
+#pragma omp parallel for schedule(static) if (M >= PAR_MIN)
+    for (long long i = 0; i < M; ++i) {
+        uint64_t idx = insert_zeros((uint64_t)i, holes, nctrl + 1) | block;
         fn(&s->a[2 * idx], &s->a[2 * (idx + st)], p);
     }
     return 0;
@@ -280,8 +287,10 @@ int orc_cr(orc_state *s, int q1, int q2, double theta, int dagger, const int *ct
     if (k < 0) return -1;
     double c = cos(theta), sn = dagger ? -sin(theta) : sin(theta);
     uint64_t set = cmask | POW2(q1) | POW2(q2);
-    for (uint64_t i = 0; i < (s->N >> k); ++i) {
-        uint64_t idx = insert_zeros(i, holes, k) | set;
+    long long M = (long long)(s->N >> k);
+#pragma omp parallel for schedule(static) if (M >= PAR_MIN)
+    for (long long i = 0; i < M; ++i) {
+        uint64_t idx = insert_zeros((uint64_t)i, holes, k) | set;
         double ar = s->a[2 * idx], ai = s->a[2 * idx + 1];
         s->a[2 * idx] = ar * c - ai * sn;
         s->a[2 * idx + 1] = ar * sn + ai * c;
@@ -299,8 +308,10 @@ int orc_iswap(orc_state *s, int q1, int q2, int dagger, const int *ctrl, int nct
     int k = subspace_setup(s, q, 2, ctrl, nctrl, holes, &cmask);
     if (k < 0) return -1;
     double sg = dagger ? -1.0 : 1.0;
-    for (uint64_t i = 0; i < (s->N >> k); ++i) {
-        uint64_t base = insert_zeros(i, holes, k) | cmask;
+    long long M = (long long)(s->N >> k);
+#pragma omp parallel for schedule(static) if (M >= PAR_MIN)
+    for (long long i = 0; i < M; ++i) {
+        uint64_t base = insert_zeros((uint64_t)i, holes, k) | cmask;
         uint64_t i1 = base | POW2(q1), i2 = base | POW2(q2);
         double ar = s->a[2 * i1], ai = s->a[2 * i1 + 1];
         double br = s->a[2 * i2], bi = s->a[2 * i2 + 1];
@@ -320,8 +331,10 @@ int orc_sqiswap(orc_state *s, int q1, int q2, int dagger, const int *ctrl, int n
     int k = subspace_setup(s, q, 2, ctrl, nctrl, holes, &cmask);
     if (k < 0) return -1;
     double sg = dagger ? -1.0 : 1.0;
-    for (uint64_t i = 0; i < (s->N >> k); ++i) {
-        uint64_t base = insert_zeros(i, holes, k) | cmask;
+    long long M = (long long)(s->N >> k);
+#pragma omp parallel for schedule(static) if (M >= PAR_MIN)
+    for (long long i = 0; i < M; ++i) {
+        uint64_t base = insert_zeros((uint64_t)i, holes, k) | cmask;
         uint64_t i1 = base | POW2(q1), i2 = base | POW2(q2);
         double ar = s->a[2 * i1], ai = s->a[2 * i1 + 1];
         double br = s->a[2 * i2], bi = s->a[2 * i2 + 1];
@@ -344,8 +357,10 @@ int orc_cswap(orc_state *s, int c, int qa, int qb, const int *ctrl, int nctrl)
     if (c >= 0) all[na++] = c;
     int k = subspace_setup(s, q, 2, all, na, holes, &cmask);
     if (k < 0) return -1;
-    for (uint64_t i = 0; i < (s->N >> k); ++i) {
-        uint64_t base = insert_zeros(i, holes, k) | cmask;
+    long long M = (long long)(s->N >> k);
+#pragma omp parallel for schedule(static) if (M >= PAR_MIN)
+    for (long long i = 0; i < M; ++i) {
+        uint64_t base = insert_zeros((uint64_t)i, holes, k) | cmask;
         uint64_t i1 = base | POW2(qa), i2 = base | POW2(qb);
         double t0 = s->a[2 * i1], t1 = s->a[2 * i1 + 1];
         s->a[2 * i1] = s->a[2 * i2]; s->a[2 * i1 + 1] = s->a[2 * i2 + 1];
@@ -443,20 +458,27 @@ int orc_pmeasure(orc_state *s, const int *qubits, int m, double *out)
 int orc_sample(orc_state *s, const int *qubits, int m, const double *u,
                uint64_t shots, uint64_t *out)
 {
-    orc_state *w = orc_create(s->n);
-    if (!w) return -1;
-    for (uint64_t sh = 0; sh < shots; ++sh) {
-        memcpy(w->a, s->a, 2 * s->N * sizeof(double));
-        uint64_t bits = 0;
-        for (int k = 0; k < m; ++k) {
-            int o = orc_measure(w, qubits[k], u[sh * (uint64_t)m + k]);
-            if (o < 0) { orc_destroy(w); return -1; }
-            bits |= (uint64_t)o << k;
+    int bad = 0;
+    /* shots are independent: each thread re-measures its own copy */
+#pragma omp parallel reduction(| : bad)
+    {
+        orc_state *w = orc_create(s->n);
+        if (!w) bad = 1;
+#pragma omp for schedule(dynamic, 4)
+        for (long long sh = 0; sh < (long long)shots; ++sh) {
+            if (!w) continue;
+            memcpy(w->a, s->a, 2 * s->N * sizeof(double));
+            uint64_t bits = 0;
+            for (int k = 0; k < m; ++k) {
+                int o = orc_measure(w, qubits[k], u[(uint64_t)sh * (uint64_t)m + k]);
+                if (o < 0) { bad = 1; break; }
+                bits |= (uint64_t)o << k;
+            }
+            out[sh] = bits;
         }
-        out[sh] = bits;
+        orc_destroy(w);
     }
-    orc_destroy(w);
-    return 0;
+    return bad ? -1 : 0;
 }
 
 double orc_norm2(orc_state *s)

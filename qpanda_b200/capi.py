@@ -281,7 +281,8 @@ class StateVector:
 
 class PlanOpts(C.Structure):
     _fields_ = [("block_qubits", C.c_int), ("tile_qubits", C.c_int), ("max_sub", C.c_int),
-                ("low_qubits", C.c_int), ("kernel", C.c_int), ("remap", C.c_int), ("threads_per_row", C.c_int)]
+                ("low_qubits", C.c_int), ("kernel", C.c_int), ("remap", C.c_int), ("threads_per_row", C.c_int),
+                ("tile_in_tmem", C.c_int)]
 
 
 PLAN_SINGLE, PLAN_TILED = 1, 2
@@ -295,9 +296,12 @@ class FusionPlan:
     state (twice the memory; faster passes on large states); remap=2: the
     next pass's tiles contiguous instead (qs_plan_opts.remap).
     threads_per_row=2: tiled passes with two threads per tile row
-    (qs_plan_opts.threads_per_row; measured slightly slower than 1)."""
+    (qs_plan_opts.threads_per_row; measured slightly slower than 1).
+    tile_in_tmem=0: keep every pass's tile in shared memory instead of tensor
+    memory (qs_plan_opts.tile_in_tmem)."""
 
-    def __init__(self, n, gates, max_k=5, kernel="tiled", max_sub=2, low_qubits=3, remap=False, threads_per_row=1):
+    def __init__(self, n, gates, max_k=5, kernel="tiled", max_sub=2, low_qubits=3, remap=False, threads_per_row=1,
+                 tile_in_tmem=1):
         g = np.ascontiguousarray(gates, dtype=GATE_DTYPE)
         self._keep = g
         h = C.c_void_p()
@@ -309,6 +313,7 @@ class FusionPlan:
             o.block_qubits, o.max_sub, o.low_qubits = int(max_k), int(max_sub), int(low_qubits)
             o.remap = int(remap)
             o.threads_per_row = int(threads_per_row)
+            o.tile_in_tmem = int(tile_in_tmem)
             check(lib().qs_plan_create_ex(int(n), g.ctypes.data, g.size, C.byref(o), C.byref(h)))
         self._h = h
         self.n = int(n)

@@ -63,3 +63,7 @@ int qs_tiled_grid(const qs_state *s);
 int qs_tile_row_orders(int n, const int *T, int nsub, const int (*qpos)[5], int (*rows)[7],
                        const int *wtile = nullptr, int input_mode = 0);
 int qs_launch_tiled(qs_state *s, const qs_tiled_desc *d, int *err_dev);
+// The same pass on k_tile_tmem (qs_tile_tmem.cu): the tile in tensor memory
+// as the MMAs' A operand.  QS_ERR_UNSUPPORTED, with nothing launched and no
+// error recorded, for a pass it does not take (then use qs_launch_tiled).
+int qs_launch_tiled_tmem(qs_state *s, const qs_tiled_desc *d, int *err_dev);

@@ -14,6 +14,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <type_traits>
 #include <vector>
 
 #include "qs_common.cuh"
@@ -234,6 +235,78 @@ k_marginal(const T *__restrict__ a, MargParams P, double *__restrict__ part)
         uint64_t oi = out_hi;
         for (int r = 0; r < P.mlo; ++r) oi |= (uint64_t)((b >> r) & 1) << P.mlo_out[r];
         dst[oi] = acc[b];
+    }
+}
+
+// The same marginal when every chunk bit is measured (P.ulo == 0, chunks of
+// 4096): each bin is one amplitude of each chunk, so a thread owns fixed
+// chunk positions and adds their |a|^2 in registers, chunk after chunk -
+// the order k_marginal adds them in, so the bins are bit-identical - with
+// 16-byte loads (two complex64 or one complex128 amplitude each), two
+// chunks' loads in flight before their first use, and no shared memory.
+template <typename T>
+__global__ void __launch_bounds__(kThreads)
+k_marginal_direct(const T *__restrict__ a, MargParams P, double *__restrict__ part)
+{
+    constexpr int kApl = sizeof(T) == 4 ? 2 : 1;            // amplitudes per 16-byte load
+    constexpr int kLoads = 4096 / (kThreads * kApl);          // per thread and chunk
+    typedef typename std::conditional<sizeof(T) == 4, float4, double2>::type L16;
+    const L16 *pa = reinterpret_cast<const L16 *>(a);
+    const int t = threadIdx.x;
+    const uint64_t o = blockIdx.x / P.G, g = blockIdx.x % P.G;
+    uint64_t hm = 0, out_hi = 0;
+    for (int r = 0; r < P.mhi; ++r) {
+        const uint64_t bit = (o >> r) & 1ull;
+        hm |= bit << P.mhi_pos[r];
+        out_hi |= bit << P.mhi_out[r];
+    }
+    double acc[kLoads * kApl];
+#pragma unroll
+    for (int i = 0; i < kLoads * kApl; ++i) acc[i] = 0.0;
+    auto chunk_base = [&](uint64_t r) {
+        const uint64_t uidx = g * P.R + r;
+        uint64_t hu = 0;
+        for (int j = 0; j < P.uhi; ++j) hu |= ((uidx >> j) & 1ull) << P.uhi_pos[j];
+        return ((hm | hu) << 12) / kApl;                       // in 16-byte units
+    };
+    auto add = [&](const L16 (&v)[kLoads]) {
+#pragma unroll
+        for (int i = 0; i < kLoads; ++i) {
+            if constexpr (sizeof(T) == 4) {
+                const float4 x = *reinterpret_cast<const float4 *>(&v[i]);
+                acc[2 * i] += p2(x.x, x.y);
+                acc[2 * i + 1] += p2(x.z, x.w);
+            } else {
+                const double2 x = *reinterpret_cast<const double2 *>(&v[i]);
+                acc[i] += p2(x.x, x.y);
+            }
+        }
+    };
+    uint64_t r = 0;
+    for (; r + 2 <= P.R; r += 2) {
+        const uint64_t b0 = chunk_base(r), b1 = chunk_base(r + 1);
+        L16 v0[kLoads], v1[kLoads];
+#pragma unroll
+        for (int i = 0; i < kLoads; ++i) v0[i] = __ldg(pa + b0 + t + i * kThreads);
+#pragma unroll
+        for (int i = 0; i < kLoads; ++i) v1[i] = __ldg(pa + b1 + t + i * kThreads);
+        add(v0);
+        add(v1);
+    }
+    if (r < P.R) {
+        const uint64_t b0 = chunk_base(r);
+        L16 v0[kLoads];
+#pragma unroll
+        for (int i = 0; i < kLoads; ++i) v0[i] = __ldg(pa + b0 + t + i * kThreads);
+        add(v0);
+    }
+    double *dst = part + g * (1ull << P.m);
+#pragma unroll
+    for (int i = 0; i < kLoads * kApl; ++i) {
+        const int l = (t + (i / kApl) * kThreads) * kApl + (i % kApl);   // chunk position
+        uint64_t oi = out_hi;
+        for (int b = 0; b < P.mlo; ++b) oi |= (uint64_t)((l >> P.mlo_pos[b]) & 1) << P.mlo_out[b];
+        dst[oi] = acc[i];
     }
 }
 
@@ -501,12 +574,17 @@ int marginal_launch(qs_state *s, const MargParams &P, double *dev_out, double *p
 {
     const uint64_t ohi = 1ull << P.mhi, G = P.G;
     if (G == 1) part = dev_out;
-    size_t smem = marginal_smem(P);
-    QS_CUDA_TRY(cudaFuncSetAttribute(k_marginal<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024));
     uint64_t ctas = ohi * G;
     if (ctas > 0x7fffffffull) return qs_fail(QS_ERR_UNSUPPORTED, "qs_probs: too many output bins");
-    k_marginal<T><<<(unsigned)ctas, kThreads, smem, s->stream>>>(static_cast<const T *>(s->amp), P, part);
-    QS_LAUNCH_CHECK("k_marginal");
+    if (P.ulo == 0 && P.c == 12) {
+        k_marginal_direct<T><<<(unsigned)ctas, kThreads, 0, s->stream>>>(static_cast<const T *>(s->amp), P, part);
+        QS_LAUNCH_CHECK("k_marginal_direct");
+    } else {
+        size_t smem = marginal_smem(P);
+        QS_CUDA_TRY(cudaFuncSetAttribute(k_marginal<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024));
+        k_marginal<T><<<(unsigned)ctas, kThreads, smem, s->stream>>>(static_cast<const T *>(s->amp), P, part);
+        QS_LAUNCH_CHECK("k_marginal");
+    }
     if (G > 1) {
         uint64_t nout = 1ull << P.m;
         k_marginal_combine<<<grid_for(nout, kThreads), kThreads, 0, s->stream>>>(part, G, nout, dev_out);

@@ -512,6 +512,7 @@ extern "C" int qs_plan_default_opts(qs_plan_opts *o)
     o->kernel = QS_PLAN_TILED;
     o->remap = 0;
     o->threads_per_row = 1;
+    o->tile_in_tmem = 1;
     return QS_OK;
 }
 
@@ -854,7 +855,10 @@ extern "C" int qs_plan_apply_range(qs_state *s, qs_plan *P, size_t first, size_t
             d.prev_out = u ? norm + GT * (1 + (u - 1) % 2) : nullptr;
             d.in_parts = u ? nullptr : norm;
             d.out_parts = norm + GT * (1 + u % 2);
-            if ((r = qs_launch_tiled(s, &d, flag))) return r;
+            r = QS_ERR_UNSUPPORTED;
+            if (P->opts.tile_in_tmem && d.threads_per_row == 1) r = qs_launch_tiled_tmem(s, &d, flag);
+            if (r == QS_ERR_UNSUPPORTED) r = qs_launch_tiled(s, &d, flag);
+            if (r) return r;
         }
         return QS_OK;
     }

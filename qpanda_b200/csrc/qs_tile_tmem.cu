@@ -1,0 +1,681 @@
+// qs_tile_tmem.cu - tiled fused passes with the tile held in tensor memory
+// (complex64).  Layout and rationale: qs_tile_tmem.cuh.
+//
+// One CTA per SM with four lane groups of 128 threads (4 warps); each group
+// owns a 32 KB staging buffer, an mbarrier, a named barrier and 128 TMEM
+// columns (two 64-column regions that alternate between a block's A operand
+// - BF16 hi in 32 columns, lo in 32 - and its FP32 accumulator).  A group
+// walks tiles  blockIdx.x * 4 + group  in steps of  gridDim.x * 4;  per tile:
+//   1. wait for the tile's copies (issued one tile earlier) and gather each
+//      thread's block-0 row from the swizzled staging buffer;
+//   2. split the row into BF16 hi/lo and write it to the group's TMEM lanes
+//      (tcgen05.st); barrier; one thread issues the block's 12 MMAs
+//      (kind::f16, A from TMEM, B = the block matrix in shared memory,
+//      D = x_hi R_hi + x_hi R_lo + x_lo R_hi in the other region) and commits
+//      to the group's mbarrier; every thread issues its copies of the next tile
+//      into the staging buffer it has finished reading;
+//   3. per block: wait, load the row's 64 results (tcgen05.ld); before the
+//      next block swap the leaving column bits with the entering lane bits by
+//      warp shuffles, split, write them as the next A and issue the next MMAs;
+//      after the last block store the row to HBM (in place, or at the
+//      positions of a remapping pass's StoreMap).
+// The four groups' chains overlap each other on the SM.
+//
+// The previous pass's norm correction (a scalar) is folded into block 0's
+// matrix when the CTA loads it; the input norm is summed on the plan's first
+// pass only; every wait on an mbarrier is bounded (qs_tile::mbar_wait), and an
+// expired wait is reported through the plan's error word.
+#include <algorithm>
+#include <cstring>
+
+#include "qs_fused.h"
+#include "qs_tile_core.cuh"
+#include "qs_tile_tmem.cuh"
+
+using qs_tmem::TLayout;
+
+// ------------------------------------------------------------------ host layout
+namespace {
+
+// 128-byte lines one warp-wide store of the last block touches, times the
+// stores per thread: lanes whose tile bits are written at positions 1..3
+// (0..3 without column pairs) share lines.
+int tmem_store_cost(uint32_t lanes, const int *WT, bool vec)
+{
+    int k = 0;
+    for (int t = 0; t < 12; ++t)
+        if (((lanes >> t) & 1) && WT[t] <= 3 && (WT[t] >= 1 || !vec)) ++k;
+    return (vec ? 16 : 32) * (32 >> (k > 5 ? 5 : k));
+}
+
+}  // namespace
+
+int qs_tmem_layout_build(int n, const qs_tiled_desc *d, TLayout *L)
+{
+    memset(L, 0, sizeof(*L));
+    const int nsub = d->nsub;
+    if (nsub < 1 || nsub > qs_tmem::kMaxSub) return qs_fail(QS_ERR_ARG, "tiled pass: %d blocks", nsub);
+    int local[64];
+    for (int i = 0; i < 64; ++i) local[i] = -1;
+    for (int t = 0; t < 12; ++t) {
+        const int q = d->T[t];
+        if (q < 0 || q >= n || (t && q <= d->T[t - 1]))
+            return qs_fail(QS_ERR_ARG, "tiled pass: tile qubits must be ascending and in range");
+        local[q] = t;
+        L->tmask |= 1ull << q;
+        L->tpos[t] = (int8_t)q;
+    }
+    if (d->T[0] != 0) return QS_ERR_UNSUPPORTED;       // 16-byte copies need tile bit 0 at position 0
+    uint32_t qm[qs_tmem::kMaxSub] = {0, 0, 0};
+    int mbit[qs_tmem::kMaxSub][12];
+    for (int b = 0; b < nsub; ++b) {
+        for (int t = 0; t < 12; ++t) mbit[b][t] = -1;
+        for (int m = 0; m < 5; ++m) {
+            const int q = d->qpos[b][m];
+            const int t = (q >= 0 && q < n) ? local[q] : -1;
+            if (t < 0 || ((qm[b] >> t) & 1))
+                return qs_fail(QS_ERR_ARG, "tiled pass: block qubits must be distinct tile qubits");
+            qm[b] |= 1u << t;
+            mbit[b][t] = m;
+        }
+    }
+    int WT[12];
+    uint64_t wseen = 0;
+    for (int t = 0; t < 12; ++t) {
+        WT[t] = d->has_write ? d->wtile[t] : d->T[t];
+        if (WT[t] < 0 || WT[t] >= n || ((wseen >> WT[t]) & 1))
+            return qs_fail(QS_ERR_ARG, "tiled pass: write positions must be distinct and in range");
+        wseen |= 1ull << WT[t];
+    }
+    uint32_t uni = 0;
+    for (int b = 0; b < nsub; ++b) uni |= qm[b];
+    const uint32_t cand = ~uni & 0xfffu;
+    if (__builtin_popcount(cand) < 2) return QS_ERR_UNSUPPORTED;
+    const int last = nsub - 1;
+    int z = -1;                                  // tile bit written at position 0
+    for (int t = 0; t < 12; ++t)
+        if (WT[t] == 0) z = t;
+    const bool zlast = z >= 0 && ((qm[last] >> z) & 1);
+
+    // warp bits: two tile bits outside every block; the last block's lanes are
+    // the rest of its row bits, so pick the pair that leaves the lanes with the
+    // cheapest stores, then one that keeps tile bit 0 out (a lane there gives
+    // the 8-byte gather its bank bit 0), then the higher write positions
+    int wa = -1, wb = -1;
+    long best = 1L << 40;
+    for (int a = 0; a < 12; ++a)
+        for (int b = a + 1; b < 12; ++b) {
+            if (!((cand >> a) & 1) || !((cand >> b) & 1)) continue;
+            const uint32_t lanes = 0xfffu & ~qm[last] & ~(1u << a) & ~(1u << b);
+            long c = (long)tmem_store_cost(lanes, WT, zlast) * 4096;
+            if (a == 0 || b == 0) c += 2048;
+            c -= WT[a] + WT[b];
+            if (c < best) { best = c; wa = a; wb = b; }
+        }
+    const int W[2] = {wa, wb};
+    const uint32_t wmask = (1u << wa) | (1u << wb);
+
+    // block 0's lanes: tile bit 0 first when it is one, then ascending
+    int lanes0[5], nl = 0;
+    if (!((qm[0] | wmask) & 1u)) lanes0[nl++] = 0;
+    for (int t = 1; t < 12; ++t)
+        if (!(((qm[0] | wmask) >> t) & 1)) lanes0[nl++] = t;
+    if (nl != 5) return qs_fail(QS_ERR_ARG, "tiled pass: row bits");
+
+    // block 0's register order: search the 120 orders of its column bits;
+    // transitions pair leaving and entering bits in order, except that the
+    // bit written at position 0 takes register bit 0 when it enters and
+    // register bit 0 leaves.  Keep the order that gives the last block 16-byte
+    // stores (register bit 0 written at position 0), then 16-byte gathers
+    // (register bit 0 of block 0 = tile bit 0).
+    int cols0[5], nc = 0;
+    for (int t = 0; t < 12; ++t)
+        if ((qm[0] >> t) & 1) cols0[nc++] = t;
+    int best_regs[qs_tmem::kMaxSub][5], best_lanes[qs_tmem::kMaxSub][5];
+    int best_sr[qs_tmem::kMaxSub][5], best_sl[qs_tmem::kMaxSub][5], best_ns[qs_tmem::kMaxSub];
+    int best_score = -1;
+    int perm[5] = {0, 1, 2, 3, 4};
+    do {
+        int regs[qs_tmem::kMaxSub][5], lanes[qs_tmem::kMaxSub][5];
+        int sr[qs_tmem::kMaxSub][5], sl[qs_tmem::kMaxSub][5], ns[qs_tmem::kMaxSub] = {0, 0, 0};
+        for (int p = 0; p < 5; ++p) { regs[0][p] = cols0[perm[p]]; lanes[0][p] = lanes0[p]; }
+        for (int b = 0; b + 1 < nsub; ++b) {
+            int lp[5], ln = 0, ei[5], en = 0;
+            for (int p = 0; p < 5; ++p)
+                if (!((qm[b + 1] >> regs[b][p]) & 1)) lp[ln++] = p;
+            for (int i = 0; i < 5; ++i)
+                if ((qm[b + 1] >> lanes[b][i]) & 1) ei[en++] = i;
+            // z enters now and register 0 leaves: pair them first
+            int zi = -1;
+            for (int k = 0; k < en; ++k)
+                if (lanes[b][ei[k]] == z) zi = k;
+            if (zi > 0 && ln > 0 && lp[0] == 0) std::swap(ei[0], ei[zi]);
+            for (int p = 0; p < 5; ++p) { regs[b + 1][p] = regs[b][p]; lanes[b + 1][p] = lanes[b][p]; }
+            for (int k = 0; k < ln; ++k) {
+                sr[b][k] = lp[k];
+                sl[b][k] = ei[k];
+                regs[b + 1][lp[k]] = lanes[b][ei[k]];
+                lanes[b + 1][ei[k]] = regs[b][lp[k]];
+            }
+            ns[b] = ln;
+        }
+        const int score = (zlast && regs[last][0] == z ? 2 : 0) + (regs[0][0] == 0 ? 1 : 0);
+        if (score > best_score) {
+            best_score = score;
+            memcpy(best_regs, regs, sizeof(regs));
+            memcpy(best_lanes, lanes, sizeof(lanes));
+            memcpy(best_sr, sr, sizeof(sr));
+            memcpy(best_sl, sl, sizeof(sl));
+            memcpy(best_ns, ns, sizeof(ns));
+        }
+    } while (best_score < 3 && std::next_permutation(perm, perm + 5));
+
+    L->nsub = nsub;
+    L->pair_in = best_regs[0][0] == 0;
+    L->vec_out = WT[best_regs[last][0]] == 0;
+    for (int b = 0; b + 1 < nsub; ++b) {
+        L->nswap[b] = (int8_t)best_ns[b];
+        for (int k = 0; k < best_ns[b]; ++k) {
+            L->swap_r[b][k] = (int8_t)best_sr[b][k];
+            L->swap_l[b][k] = (int8_t)best_sl[b][k];
+        }
+    }
+    for (int b = 0; b < nsub; ++b)
+        for (int p = 0; p < 5; ++p) L->mperm[b][p] = (int8_t)mbit[b][best_regs[b][p]];
+
+    // staging swizzle: the lanes of one shared-memory phase (lane bits 0..2 for
+    // 16-byte gathers, 0..3 for 8-byte ones) must read distinct bank slots
+    // (stage-slot bits 1..3, and bit 0 for 8-byte reads); tile bits >= 4 get
+    // the free ones through f
+    uint16_t fbit[12] = {0};
+    {
+        const int phase = L->pair_in ? 3 : 4;
+        uint32_t used = 0;
+        for (int i = 0; i < phase; ++i)
+            if (best_lanes[0][i] <= 3) used |= 1u << best_lanes[0][i];
+        for (int i = 0; i < phase; ++i) {
+            const int t = best_lanes[0][i];
+            if (t <= 3) continue;
+            for (int s = 1; s <= 3; ++s)
+                if (!((used >> s) & 1)) { used |= 1u << s; fbit[t] = (uint16_t)(1u << s); break; }
+        }
+    }
+    auto slot = [&](int t) { return (uint16_t)((1u << t) ^ fbit[t]); };
+    for (int i = 0; i < 5; ++i) L->s_lane[i] = slot(best_lanes[0][i]);
+    for (int v = 0; v < 2; ++v) L->s_warp[v] = slot(W[v]);
+    for (int j = 0; j < 32; ++j) {
+        uint16_t s = 0;
+        for (int p = 0; p < 5; ++p)
+            if ((j >> p) & 1) s ^= slot(best_regs[0][p]);
+        L->s_col[j] = s;
+    }
+    for (int b = 0; b < 7; ++b) {
+        L->g_bit[b] = 1ull << d->T[b + 1];
+        L->cf_bit[b] = (uint16_t)(fbit[b + 1] >> 1);
+    }
+    for (int k = 0; k < 16; ++k) {
+        uint64_t g = 0;
+        uint16_t c = 0;
+        for (int i = 0; i < 4; ++i)
+            if ((k >> i) & 1) { g |= 1ull << d->T[8 + i]; c ^= (uint16_t)(fbit[8 + i] >> 1); }
+        L->gk[k] = g;
+        L->cf_k[k] = c;
+    }
+    for (int i = 0; i < 5; ++i) L->o_lane[i] = 1ull << WT[best_lanes[last][i]];
+    for (int v = 0; v < 2; ++v) L->o_warp[v] = 1ull << WT[W[v]];
+    for (int j = 0; j < 32; ++j) {
+        uint64_t o = 0;
+        for (int p = 0; p < 5; ++p)
+            if ((j >> p) & 1) o |= 1ull << WT[best_regs[last][p]];
+        L->o_col[j] = o;
+    }
+    return QS_OK;
+}
+
+// ------------------------------------------------------------------ device
+namespace {
+
+using namespace qs_tile;
+
+constexpr int kGroups = 4;                       // lane groups (tiles in flight) per CTA
+constexpr int kGroupThreads = 128;
+constexpr int kCtaThreads = kGroups * kGroupThreads;
+constexpr uint32_t kOffB = 0;                    // 3 blocks x (hi, lo) x 8 KB
+constexpr uint32_t kOffStage = qs_tmem::kMaxSub * 2 * kB;
+constexpr uint32_t kOffMisc = kOffStage + kGroups * kStage;
+constexpr uint32_t kSmemUsed = kOffMisc + 64;
+// Ask for more than half of the SM's shared memory, so that no other CTA that
+// allocates tensor memory can share the SM (this one takes all 512 columns).
+constexpr uint32_t kSmemBytes = kSmemUsed > 200 * 1024 ? kSmemUsed : 200 * 1024;
+constexpr uint32_t kCols = 512;
+static_assert(kSmemBytes + 1024 <= 228 * 1024, "one CTA per SM");
+static_assert((kOffStage & 1023) == 0, "operands 1024-byte aligned");
+static_assert(kGroups * 128 <= kCols, "TMEM columns per group");
+
+struct TParams {
+    TLayout L;
+    StoreMap W;
+    uint64_t tiles;
+    const uint16_t *mat;         // nsub x [2][64][64] BF16 bits (hi, lo), the plan's column order
+    int *err;
+    int nparts;                  // norm partials per pass (>= gridDim.x; the tail is written as zeros)
+    const double *norm0;
+    const double *prev_out;
+    double *in_parts;
+    double *out_parts;
+};
+
+__device__ __forceinline__ void group_bar(int id)
+{
+    asm volatile("bar.sync %0, %1;" :: "r"(id), "r"(kGroupThreads) : "memory");
+}
+
+__device__ __forceinline__ bool group_bar_or(int id, bool v)
+{
+    uint32_t r;
+    asm volatile(
+        "{\n\t.reg .pred p, q;\n\t"
+        "setp.ne.u32 p, %1, 0;\n\t"
+        "bar.red.or.pred q, %2, %3, p;\n\t"
+        "selp.u32 %0, 1, 0, q;\n\t}\n"
+        : "=r"(r) : "r"((uint32_t)v), "r"(id), "r"(kGroupThreads) : "memory");
+    return r != 0;
+}
+
+// tile_base / tile_base_advance on the TLayout's positions
+__device__ __forceinline__ uint64_t tbase_of(uint64_t tile, const TLayout &L)
+{
+#pragma unroll 4
+    for (int j = 0; j < 12; ++j) {
+        const uint64_t low = (1ull << L.tpos[j]) - 1;
+        tile = ((tile & ~low) << 1) | (tile & low);
+    }
+    return tile;
+}
+
+// Block matrices into the swizzled B layout, each permuted to this kernel's
+// column order (register bit p = matrix bit mperm[b][p], for rows and
+// columns alike); block 0's scaled by `scale` (hi + lo recombined, scaled,
+// split again).
+__device__ void load_b_perm(uint8_t *dst, const uint16_t *mat, const TLayout &L, float scale)
+{
+    const int total = L.nsub * 64 * 32;
+    for (int it = threadIdx.x; it < total; it += kCtaThreads) {
+        const int b = it >> 11, np = (it >> 5) & 63, cp = it & 31;
+        const uint32_t n = 2 * qs_tmem::tmem_matrix_index((uint32_t)np >> 1, L.mperm[b]) + (np & 1);
+        const uint32_t k = 2 * qs_tmem::tmem_matrix_index((uint32_t)cp, L.mperm[b]);
+        const uint16_t *src = mat + (size_t)b * 2 * 4096;
+        uint32_t hi = *reinterpret_cast<const uint32_t *>(src + n * 64 + k);
+        uint32_t lo = *reinterpret_cast<const uint32_t *>(src + 4096 + n * 64 + k);
+        if (b == 0 && scale != 1.0f) {
+            const float a = (__uint_as_float(hi << 16) + __uint_as_float(lo << 16)) * scale;
+            const float c = (__uint_as_float(hi & 0xffff0000u) + __uint_as_float(lo & 0xffff0000u)) * scale;
+            split_pair(a, c, hi, lo);
+        }
+        const uint32_t off = qs_tmem::tmem_b_offset((uint32_t)np, 2u * cp);
+        *reinterpret_cast<uint32_t *>(dst + (2 * b) * kB + off) = hi;
+        *reinterpret_cast<uint32_t *>(dst + (2 * b + 1) * kB + off) = lo;
+    }
+}
+
+// D (TMEM) = A_hi B_hi + A_hi B_lo + A_lo B_hi with A in TMEM (hi at a_tmem,
+// lo 32 columns further), B in shared memory; 12 MMAs of K = 16, then commit.
+__device__ __forceinline__ void issue_ts(uint32_t d_tmem, uint32_t a_tmem, uint32_t b_hi, uint32_t b_lo,
+                                         uint32_t mbar)
+{
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint64_t dBh = umma_desc(b_hi), dBl = umma_desc(b_lo);
+#pragma unroll
+    for (int pr = 0; pr < 3; ++pr) {
+        const uint32_t a = a_tmem + (pr == 2 ? 32u : 0u);
+        const uint64_t db = pr == 1 ? dBl : dBh;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const uint32_t acc = (pr | k) ? 1u : 0u;
+            asm volatile(
+                "{\n\t.reg .pred p;\n\t"
+                "setp.ne.b32 p, %3, 0;\n\t"
+                "tcgen05.mma.cta_group::1.kind::f16 [%0], [%1], %2, %4, p;\n\t}\n"
+                :
+                : "r"(d_tmem), "r"(a + 8u * k), "l"(db + 2ull * k), "r"(acc), "r"(kIdesc));
+        }
+    }
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                 :: "r"(mbar) : "memory");
+}
+
+__device__ __forceinline__ void tmem_st32(uint32_t taddr, const uint32_t (&v)[32])
+{
+    asm volatile(
+        "tcgen05.st.sync.aligned.32x32b.x32.b32 [%0], "
+        "{%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16,"
+        "%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31,%32};"
+        :: "r"(taddr), "r"(v[0]), "r"(v[1]), "r"(v[2]), "r"(v[3]), "r"(v[4]), "r"(v[5]), "r"(v[6]),
+           "r"(v[7]), "r"(v[8]), "r"(v[9]), "r"(v[10]), "r"(v[11]), "r"(v[12]), "r"(v[13]), "r"(v[14]),
+           "r"(v[15]), "r"(v[16]), "r"(v[17]), "r"(v[18]), "r"(v[19]), "r"(v[20]), "r"(v[21]), "r"(v[22]),
+           "r"(v[23]), "r"(v[24]), "r"(v[25]), "r"(v[26]), "r"(v[27]), "r"(v[28]), "r"(v[29]), "r"(v[30]),
+           "r"(v[31])
+        : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float *y)
+{
+    uint32_t r[32];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+        "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),
+          "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]),
+          "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]),
+          "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        : "r"(taddr));
+#pragma unroll
+    for (int i = 0; i < 32; ++i) y[i] = __uint_as_float(r[i]);
+}
+
+// Row values (32 complex = 64 floats, y[2j] real, y[2j+1] imaginary) as BF16
+// hi/lo pairs into the thread's TMEM lane: hi at columns a..a+31, lo at
+// a+32..a+63.
+__device__ __forceinline__ void split_store(uint32_t taddr, const float (&y)[64])
+{
+    uint32_t hv[32], lv[32];
+#pragma unroll
+    for (int j = 0; j < 32; ++j) split_pair(y[2 * j], y[2 * j + 1], hv[j], lv[j]);
+    tmem_st32(taddr, hv);
+    tmem_st32(taddr + 32, lv);
+}
+
+// Swap register bit R of the row's complex index with the lane bit `lm`
+// (a mask): afterwards the value at (lane bit a, register bit c) is the one
+// that was at (lane bit c, register bit a).
+template <int R>
+__device__ __forceinline__ void swap_bit(float (&y)[64], bool up, int lm)
+{
+#pragma unroll
+    for (int j = 0; j < 32; ++j) {
+        if (j & (1 << R)) continue;
+        const int j1 = j | (1 << R);
+        const float s0 = up ? y[2 * j] : y[2 * j1];
+        const float s1 = up ? y[2 * j + 1] : y[2 * j1 + 1];
+        const float r0 = __shfl_xor_sync(0xffffffffu, s0, lm);
+        const float r1 = __shfl_xor_sync(0xffffffffu, s1, lm);
+        if (up) { y[2 * j] = r0; y[2 * j + 1] = r1; }
+        else { y[2 * j1] = r0; y[2 * j1 + 1] = r1; }
+    }
+}
+
+__device__ __forceinline__ void exchange(float (&y)[64], const TLayout &L, int b, int lane)
+{
+    for (int k = 0; k < L.nswap[b]; ++k) {
+        const int lm = 1 << L.swap_l[b][k];
+        const bool up = (lane & lm) != 0;
+        switch (L.swap_r[b][k]) {
+        case 0: swap_bit<0>(y, up, lm); break;
+        case 1: swap_bit<1>(y, up, lm); break;
+        case 2: swap_bit<2>(y, up, lm); break;
+        case 3: swap_bit<3>(y, up, lm); break;
+        default: swap_bit<4>(y, up, lm); break;
+        }
+    }
+}
+
+// The group's copies of a tile: chunk c = 128 k + t (tile indices 2c, 2c+1,
+// adjacent in memory) to stage chunk c ^ cf_t ^ cf_k[k].
+__device__ __forceinline__ void copy_tile(const float *amp, uint64_t base, const TLayout &L, uint32_t stage,
+                                          uint64_t g_t, uint32_t cs_t)
+{
+#pragma unroll
+    for (int k = 0; k < 16; ++k) {
+        const float *src = amp + 2 * (base | g_t | L.gk[k]);
+        const uint32_t dst = stage + ((cs_t ^ ((uint32_t)k << 7) ^ L.cf_k[k]) << 4);
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" :: "r"(dst), "l"(src) : "memory");
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+}
+
+__global__ void __launch_bounds__(kCtaThreads, 1) k_tile_tmem(const float *amp, float *out, TParams P)
+{
+    extern __shared__ __align__(1024) uint8_t smem[];
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int grp = tid >> 7, ltid = tid & 127, wq = ltid >> 5;
+    if (smem_u32(smem) & 1023u) {
+        if (tid == 0) atomicExch(P.err, 2);
+        return;
+    }
+    const TLayout &L = P.L;
+    const uint32_t stage = smem_u32(smem + kOffStage + grp * kStage);
+    uint64_t *mbar = reinterpret_cast<uint64_t *>(smem + kOffMisc) + grp;
+    uint32_t *tmem_holder = reinterpret_cast<uint32_t *>(smem + kOffMisc + 32);
+    float *s_scale = reinterpret_cast<float *>(smem + kOffMisc + 36);
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                     :: "r"(smem_u32(tmem_holder)), "r"(kCols));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    if (ltid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(smem_u32(mbar)), "r"(1));
+        asm volatile("fence.mbarrier_init.release.cluster;");
+    }
+    if (warp == 1) {
+        double n0 = 0, np = 0;
+        if (P.norm0 && P.prev_out)
+            for (int i = lane; i < P.nparts; i += 32) { n0 += P.norm0[i]; np += P.prev_out[i]; }
+        for (int o = 16; o > 0; o >>= 1) {
+            n0 += __shfl_xor_sync(0xffffffffu, n0, o);
+            np += __shfl_xor_sync(0xffffffffu, np, o);
+        }
+        if (lane == 0) *s_scale = (P.norm0 && P.prev_out && np > 0) ? (float)sqrt(n0 / np) : 1.0f;
+    }
+    __syncthreads();
+    load_b_perm(smem + kOffB, P.mat, L, *s_scale);
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem_base = *tmem_holder;
+    const uint32_t tgrp = tmem_base + (uint32_t)(grp * 128);          // the group's 128 columns
+    const uint32_t tlane = tgrp + ((uint32_t)(wq * 32) << 16);        // this warp's 32 lanes
+    const uint32_t mb = smem_u32(mbar);
+    const int bar_id = 1 + grp;
+
+    // per-thread parts of the gather, copy and store addresses
+    uint32_t xrow = 0;
+#pragma unroll
+    for (int i = 0; i < 5; ++i)
+        if ((lane >> i) & 1) xrow ^= L.s_lane[i];
+#pragma unroll
+    for (int v = 0; v < 2; ++v)
+        if ((wq >> v) & 1) xrow ^= L.s_warp[v];
+    uint64_t orow = 0;
+#pragma unroll
+    for (int i = 0; i < 5; ++i)
+        if ((lane >> i) & 1) orow |= L.o_lane[i];
+#pragma unroll
+    for (int v = 0; v < 2; ++v)
+        if ((wq >> v) & 1) orow |= L.o_warp[v];
+    uint64_t g_t = 0;
+    uint32_t cs_t = (uint32_t)ltid;
+#pragma unroll
+    for (int b = 0; b < 7; ++b)
+        if ((ltid >> b) & 1) { g_t |= L.g_bit[b]; cs_t ^= L.cf_bit[b]; }
+
+    const bool want_in = P.in_parts != nullptr;
+    uint32_t phase = 0;
+    bool failed = false;
+    double acc_in = 0, acc_out = 0;
+    const uint64_t stride = (uint64_t)gridDim.x * kGroups;
+    uint64_t tile = (uint64_t)blockIdx.x * kGroups + grp;
+    const uint64_t step = tbase_of(stride, L);
+    uint64_t tbase = tbase_of(tile, L);
+    if (tile < P.tiles) copy_tile(amp, tbase, L, stage, g_t, cs_t);
+    for (; tile < P.tiles; tile += stride) {
+        const uint64_t tnext = tile_base_advance(tbase, step, L.tmask);
+        asm volatile("cp.async.wait_group 0;" ::: "memory");
+        group_bar(bar_id);
+        float y[64];
+        {
+            // gather the thread's block-0 row
+            if (L.pair_in) {
+#pragma unroll
+                for (int j = 0; j < 16; ++j) {
+                    const uint32_t a = stage + ((xrow ^ L.s_col[2 * j]) << 3);
+                    asm volatile("ld.shared.v4.f32 {%0,%1,%2,%3}, [%4];"
+                                 : "=f"(y[4 * j]), "=f"(y[4 * j + 1]), "=f"(y[4 * j + 2]), "=f"(y[4 * j + 3])
+                                 : "r"(a));
+                }
+            } else {
+#pragma unroll
+                for (int j = 0; j < 32; ++j) {
+                    const uint32_t a = stage + ((xrow ^ L.s_col[j]) << 3);
+                    asm volatile("ld.shared.v2.f32 {%0,%1}, [%2];" : "=f"(y[2 * j]), "=f"(y[2 * j + 1]) : "r"(a));
+                }
+            }
+            if (want_in) {
+                float ss = 0.f;
+#pragma unroll
+                for (int i = 0; i < 64; ++i) ss = fmaf(y[i], y[i], ss);
+                acc_in += (double)ss;
+            }
+            split_store(tlane, y);
+        }
+        asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        group_bar(bar_id);
+        if (ltid == 0) issue_ts(tgrp + 64, tgrp, smem_u32(smem + kOffB), smem_u32(smem + kOffB + kB), mb);
+        // every thread of the group has read the staging buffer: next tile's copies
+        if (tile + stride < P.tiles) copy_tile(amp, tnext, L, stage, g_t, cs_t);
+
+        for (int b = 0; b < L.nsub; ++b) {
+            const bool ok = mbar_wait(mb, phase);
+            phase ^= 1;
+            if (group_bar_or(bar_id, !ok)) { failed = true; break; }
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const uint32_t dreg = (b & 1) ? 0u : 64u;                    // this block's accumulator
+            tmem_ld32(tlane + dreg, y);
+            tmem_ld32(tlane + dreg + 32, y + 32);
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            if (b + 1 < L.nsub) {
+                exchange(y, L, b, lane);
+                split_store(tlane + dreg, y);                            // the next block's A
+                asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+                asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+                group_bar(bar_id);
+                if (ltid == 0)
+                    issue_ts(tgrp + (dreg ^ 64u), tgrp + dreg, smem_u32(smem + kOffB + (2 * (b + 1)) * kB),
+                             smem_u32(smem + kOffB + (2 * (b + 1) + 1) * kB), mb);
+            } else {
+                const uint64_t obase = store_base(tile, tbase, P.W) | orow;
+                float t = 0.f;
+#pragma unroll
+                for (int i = 0; i < 64; ++i) t = fmaf(y[i], y[i], t);
+                acc_out += (double)t;
+                if (L.vec_out) {
+#pragma unroll
+                    for (int j = 0; j < 16; ++j)
+                        *reinterpret_cast<float4 *>(out + 2 * (obase | L.o_col[2 * j])) =
+                            make_float4(y[4 * j], y[4 * j + 1], y[4 * j + 2], y[4 * j + 3]);
+                } else {
+#pragma unroll
+                    for (int j = 0; j < 32; ++j)
+                        *reinterpret_cast<float2 *>(out + 2 * (obase | L.o_col[j])) = make_float2(y[2 * j], y[2 * j + 1]);
+                }
+            }
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        }
+        if (failed) break;
+        tbase = tnext;
+    }
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
+    {
+        double ai = acc_in, ao = acc_out;
+        for (int o = 16; o > 0; o >>= 1) {
+            ai += __shfl_xor_sync(0xffffffffu, ai, o);
+            ao += __shfl_xor_sync(0xffffffffu, ao, o);
+        }
+        constexpr int kWarps = kCtaThreads / 32;
+        double *red = reinterpret_cast<double *>(smem + kOffStage);      // group 0's staging buffer
+        __syncthreads();                     // every copy of every group has landed
+        if (lane == 0) { red[warp] = ai; red[kWarps + warp] = ao; }
+        __syncthreads();
+        if (tid == 0) {
+            double a = 0, b = 0;
+            for (int w = 0; w < kWarps; ++w) { a += red[w]; b += red[kWarps + w]; }
+            if (P.in_parts) P.in_parts[blockIdx.x] = a;
+            if (P.out_parts) P.out_parts[blockIdx.x] = b;
+        }
+        if (blockIdx.x == 0)                 // partials past this grid read as zero
+            for (int i = (int)gridDim.x + tid; i < P.nparts; i += kCtaThreads) {
+                if (P.in_parts) P.in_parts[i] = 0.0;
+                if (P.out_parts) P.out_parts[i] = 0.0;
+            }
+    }
+    if (failed) {
+        if (ltid == 0) atomicExch(P.err, 1);
+        mbar_wait(mb, phase ^ 1);            // bounded: the MMAs in flight, if any
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" :: "r"(tmem_base), "r"(kCols));
+    }
+}
+
+}  // namespace
+
+int qs_tmem_grid(const qs_state *s)
+{
+    const uint64_t tiles = s->N >> 12, need = (tiles + kGroups - 1) / kGroups;
+    return (int)(need < QS_SM_COUNT ? need : QS_SM_COUNT);
+}
+
+// Launch one tiled pass on k_tile_tmem.  QS_ERR_UNSUPPORTED (nothing
+// launched, no error recorded) when the pass does not fit this kernel.
+int qs_launch_tiled_tmem(qs_state *s, const qs_tiled_desc *d, int *err_dev)
+{
+    if (s->dtype != QS_C64 || s->n < 12) return QS_ERR_UNSUPPORTED;
+    TParams P;
+    memset(&P, 0, sizeof(P));
+    int r = qs_tmem_layout_build(s->n, d, &P.L);
+    if (r) return r;
+    P.W.mode = d->has_write ? d->wmode : 0;
+    P.W.ntb = s->n - 12;
+    if (d->has_write && P.W.mode != 1 && P.W.mode != 2)
+        return qs_fail(QS_ERR_ARG, "tiled pass: write mode %d", P.W.mode);
+    if (P.W.mode == 2) {
+        uint64_t seen = 0;
+        for (int l = 0; l < 12; ++l) seen |= 1ull << d->wtile[l];
+        for (int i = 0; i < P.W.ntb; ++i) {
+            const int w = d->wpos[i];
+            if (w < 0 || w >= s->n || ((seen >> w) & 1))
+                return qs_fail(QS_ERR_ARG, "tiled pass: write positions must form a permutation");
+            seen |= 1ull << w;
+            P.W.wpos[i] = (int8_t)w;
+        }
+    } else if (P.W.mode == 1) {
+        for (int l = 0; l < 12; ++l)
+            if (d->wtile[l] >= 12) return qs_fail(QS_ERR_ARG, "tiled pass: contiguous writes need tile bits at 0..11");
+    }
+    P.tiles = s->N >> 12;
+    P.mat = static_cast<const uint16_t *>(d->mat_dev);
+    P.err = err_dev;
+    P.nparts = qs_tiled_grid(s);
+    P.norm0 = d->norm0;
+    P.prev_out = d->prev_out;
+    P.in_parts = d->in_parts;
+    P.out_parts = d->out_parts;
+    const float *in = static_cast<const float *>(d->amp_in ? d->amp_in : s->amp);
+    float *out = static_cast<float *>(d->amp_out ? d->amp_out : s->amp);
+    if ((d->amp_in != nullptr) != (d->amp_out != nullptr) || (d->amp_in && (const void *)in == (const void *)out))
+        return qs_fail(QS_ERR_ARG, "tiled pass: set both buffers, and distinct, or neither");
+    if (d->has_write && !d->amp_out)
+        return qs_fail(QS_ERR_ARG, "tiled pass: remapped results need a separate output buffer");
+    QS_CUDA_TRY(cudaFuncSetAttribute(k_tile_tmem, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes));
+    const unsigned grid = (unsigned)qs_tmem_grid(s);
+    k_tile_tmem<<<grid, kCtaThreads, kSmemBytes, s->stream>>>(in, out, P);
+    QS_LAUNCH_CHECK("k_tile_tmem");
+    return QS_OK;
+}

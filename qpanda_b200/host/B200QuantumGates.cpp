@@ -33,7 +33,13 @@ QError B200QuantumGates::apply(int op, const size_t *q, int nq, double theta, in
                                const Qnum &controls, double error_rate)
 {
     if (!mState) return undefineError;
-    if (!(randGenerator() > error_rate)) return qErrorNone;
+    if (mMode != kNormal) {
+        uint64_t m = 0;
+        for (int j = 0; j < nq; ++j) m |= 1ull << q[j];
+        for (size_t c : controls) m |= 1ull << c;
+        touch(m);
+    }
+    if (!(draw() > error_rate) || mMode == kProbe) return qErrorNone;
     qs_gate g;
     memset(&g, 0, sizeof(g));
     g.op = op;
@@ -61,6 +67,7 @@ size_t B200QuantumGates::getQStateSize()
 bool B200QuantumGates::getQState(string &sState, QuantumGateParam *)
 {
     if (!mState) return false;
+    if (mMode != kNormal && mMeasured) mTerminal = false;
     vector<complex<double>> v((size_t)1 << mQubits);
     if (qs_get_state(mState, v.data(), QS_C128) != QS_OK) return false;
     std::stringstream ss;
@@ -86,6 +93,8 @@ QError B200QuantumGates::Hadamard(size_t qn, double error_rate, Qnum vControlBit
 // CPUQuantumGates.cpp:126-136: measure, then flip if the outcome was 1.
 QError B200QuantumGates::Reset(size_t qn)
 {
+    if (mMode != kNormal) mTerminal = false;     // its flip depends on the outcome
+    if (mMode == kProbe) return qErrorNone;
     int o = qubitMeasure(qn);
     if (o < 0) return undefineError;
     if (o) return NOT(qn, 0);
@@ -95,6 +104,8 @@ QError B200QuantumGates::Reset(size_t qn)
 QError B200QuantumGates::pMeasure(Qnum &qnum, vector<pair<size_t, double>> &mResult)
 {
     if (!mState) return undefineError;
+    if (mMode != kNormal && mMeasured) mTerminal = false;
+    if (mMode == kProbe) return mResult.clear(), qErrorNone;
     vector<int> qs(qnum.begin(), qnum.end());
     uint64_t idx[10];
     double p[10];
@@ -183,7 +194,7 @@ QError B200QuantumGates::sqiSWAP(size_t qn_1, size_t qn_2, double error_rate, Qn
 
 QError B200QuantumGates::controlSwap(size_t qn_1, size_t qn_2, size_t qn_3, double error_rate)
 {
-    if (qn_2 == qn_3) return randGenerator(), qErrorNone;     // the reference's loop is a no-op then
+    if (qn_2 == qn_3) return draw(), qErrorNone;              // the reference's loop is a no-op then
     size_t q[3] = {qn_1, qn_2, qn_3};
     return apply(QS_OP_CSWAP, q, 3, 0, 0, Qnum(), error_rate);
 }
@@ -192,6 +203,13 @@ QError B200QuantumGates::controlSwap(size_t qn_1, size_t qn_2, size_t qn_3, doub
 int B200QuantumGates::qubitMeasure(size_t qn)
 {
     if (!mState) return -1;
+    if (mMode != kNormal) {
+        if (qn >= (size_t)mQubits) return -1;
+        const size_t pos = mDraws;
+        mRec.push_back(Recorded{(int)qn, pos, draw()});
+        mMeasured |= 1ull << qn;
+        return 0;
+    }
     double u = randGenerator();
     int out = 0;
     if (qs_measure(mState, (int)qn, u, &out) != QS_OK) return -1;
@@ -205,7 +223,8 @@ QError B200QuantumGates::unitarySingleQubitGate(size_t qn, void *matrix, double 
     if (!mState || !matrix) return undefineError;
     const QStat &M = *static_cast<QStat *>(matrix);
     if (M.size() < 4) return qParameterError;
-    if (!(randGenerator() > error_rate)) return qErrorNone;
+    if (mMode != kNormal) touch(1ull << qn);
+    if (!(draw() > error_rate) || mMode == kProbe) return qErrorNone;
     double m[8];
     for (int j = 0; j < 4; ++j) { m[2 * j] = M[j].real(); m[2 * j + 1] = M[j].imag(); }
     return fromStatus(qs_apply_unitary_1q(mState, (int)qn, m));
@@ -265,6 +284,7 @@ QError B200QuantumGates::destroyState(size_t)
 QError B200QuantumGates::endGate(QuantumGateParam *, QuantumGates *)
 {
     if (!mState) return undefineError;
+    if (mMode == kProbe) return qErrorNone;
     return fromStatus(qs_reset_zero(mState));
 }
 
@@ -274,5 +294,89 @@ QError B200QuantumGates::matReverse(COMPLEX (*mat)[4], COMPLEX (*mat_rev)[4])
     static const int perm[4] = {0, 2, 1, 3};
     for (int r = 0; r < 4; ++r)
         for (int c = 0; c < 4; ++c) mat_rev[r][c] = mat[perm[r]][perm[c]];
+    return qErrorNone;
+}
+
+// A uniform from the generator, counted in a deferred pass; a probe pass
+// counts without drawing (and reports 1, so that every gate "applies").
+double B200QuantumGates::draw()
+{
+    if (mMode == kNormal) return randGenerator();
+    ++mDraws;
+    return mMode == kProbe ? 1.0 : randGenerator();
+}
+
+void B200QuantumGates::touch(uint64_t qubit_mask)
+{
+    if (qubit_mask & mMeasured) mTerminal = false;
+}
+
+void B200QuantumGates::beginProbe()
+{
+    mMode = kProbe;
+    mTerminal = true;
+    mDraws = 0;
+    mMeasured = 0;
+    mRec.clear();
+}
+
+bool B200QuantumGates::endProbe()
+{
+    mMode = kNormal;
+    return mTerminal && !mRec.empty();
+}
+
+void B200QuantumGates::beginDeferredMeasure()
+{
+    mMode = kDeferred;
+    mTerminal = true;
+    mDraws = 0;
+    mMeasured = 0;
+    mRec.clear();
+}
+
+QError B200QuantumGates::sampleDeferred(size_t shots, vector<uint64_t> &out)
+{
+    mMode = kNormal;
+    out.assign(shots, 0);
+    if (!mState || !mTerminal) return undefineError;
+    const size_t m = mRec.size();
+    if (shots == 0 || m == 0) return qErrorNone;
+    // distinct qubits in the order first measured: slot[k] = the distinct qubit
+    // of measurement k, lead[j] = the measurement that first measures qubit j
+    vector<int> qubits;
+    vector<size_t> slot(m), lead;
+    for (size_t k = 0; k < m; ++k) {
+        size_t j = 0;
+        while (j < qubits.size() && qubits[j] != mRec[k].qubit) ++j;
+        if (j == qubits.size()) {
+            qubits.push_back(mRec[k].qubit);
+            lead.push_back(k);
+        }
+        slot[k] = j;
+    }
+    const size_t mu = qubits.size();
+    vector<double> u(shots * mu), pass(mDraws);
+    for (size_t j = 0; j < mu; ++j) u[j] = mRec[lead[j]].u;         // shot 0: the pass's own draws
+    for (size_t s = 1; s < shots; ++s) {                             // then a pass's worth per shot
+        for (size_t d = 0; d < mDraws; ++d) pass[d] = randGenerator();
+        for (size_t j = 0; j < mu; ++j) u[s * mu + j] = pass[mRec[lead[j]].draw];
+    }
+    vector<uint64_t> raw(shots);
+    int rc = qs_sample(mState, qubits.data(), (int)mu, u.data(), shots, raw.data());
+    if (rc) return fromStatus(rc);
+    // the state the loop leaves: the last shot's measurements, in order
+    uint64_t last = 0;
+    for (size_t j = 0; j < mu; ++j) {
+        int o = 0;
+        if ((rc = qs_measure(mState, qubits[j], u[(shots - 1) * mu + j], &o))) return fromStatus(rc);
+        last |= (uint64_t)o << j;
+    }
+    raw[shots - 1] = last;
+    for (size_t s = 0; s < shots; ++s) {
+        uint64_t bits = 0;
+        for (size_t k = 0; k < m; ++k) bits |= ((raw[s] >> slot[k]) & 1ull) << k;
+        out[s] = bits;
+    }
     return qErrorNone;
 }

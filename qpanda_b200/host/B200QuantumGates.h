@@ -72,6 +72,37 @@ public:
     QError destroyState(size_t stQNum);
     QError endGate(QuantumGateParam *pQuantumProParam, QuantumGates *pQGate);
 
+    // ---- shots of a program whose measurements are terminal --------------
+    // QPandaSDK::run re-runs a MEASURE program once per shot, resetting the
+    // state each time (QPandaAPI.cpp:169-182).  When no gate, Reset or
+    // pMeasure touches the state after a measurement, one run plus sampling
+    // gives the same outcomes from the same generator stream.  Use:
+    //   beginProbe(); one pass of the program; endProbe() - a dry pass that
+    //     launches nothing and draws nothing, and tells whether every
+    //     measurement is terminal (false: run the per-shot loop as before);
+    //   beginDeferredMeasure(); one pass of the program (endGate, then every
+    //     node), in which qubitMeasure draws its uniform and records it with
+    //     the qubit and its position in the pass's draws, returns 0 and leaves
+    //     the state alone;  then sampleDeferred(shots, out).
+    void beginProbe();
+    bool endProbe();
+    void beginDeferredMeasure();
+    // True after a pass unless something touched the state after a
+    // measurement.
+    bool deferredTerminal() const { return mTerminal; }
+    // Measurements recorded in the pass, in program order.
+    size_t deferredCount() const { return mRec.size(); }
+    // out[s] bit k = outcome of the k-th recorded measurement in shot s.  Shot
+    // 0 uses the uniforms drawn in the pass; shot s > 0 draws a whole pass's
+    // worth (one per gate and per measurement, in program order) from
+    // randGenerator() and uses the draws at the measurements' positions - the
+    // draws the per-shot loop would give them.  Outcomes follow qubitMeasure's
+    // rule with sequential collapse (qs_sample); a qubit measured again gets
+    // its first outcome.  Afterwards the state is collapsed as the last shot
+    // left it and the generator stands where the loop would leave it.  Ends
+    // deferred mode.
+    QError sampleDeferred(size_t shots, vector<uint64_t> &out);
+
     // Direct access for callers that want the C ABI's extra entry points
     // (fused plans, shot sampling) on the same state.
     qs_state *state() { return mState; }
@@ -86,9 +117,25 @@ private:
                  double error_rate);
     QError fromStatus(int rc) const;
 
+    // draw one uniform, counting the pass's draws in deferred mode
+    double draw();
+    void touch(uint64_t qubit_mask);
+
     qs_state *mState = nullptr;
     int mQubits = 0;
     int mDtype;
+    // deferred measurements
+    struct Recorded {
+        int qubit;
+        size_t draw;                     // position among the pass's draws
+        double u;
+    };
+    enum Mode { kNormal, kProbe, kDeferred };
+    Mode mMode = kNormal;
+    bool mTerminal = true;
+    size_t mDraws = 0;
+    uint64_t mMeasured = 0;              // qubits measured so far in the pass
+    vector<Recorded> mRec;
 };
 
 #endif

@@ -16,6 +16,12 @@
 // to |0...0>, QuantumInstructionHandleAPI.cpp:96-100) followed by every node -
 // and count the classical registers (countState, :264-285); a program with
 // PMEASURE runs once and reports the top-10 outcomes as bitstrings.
+// qr_run_ex with `sample` set runs that loop the way a B200 integration of
+// QPandaSDK::run would: a dry probe pass (B200QuantumGates::beginProbe)
+// tells whether every MEASURE is terminal; if so the program runs once in
+// deferred-measurement mode and the shots come from
+// B200QuantumGates::sampleDeferred, with the same generator stream; else the
+// per-shot loop runs as before.  *runs receives the number of simulations.
 #include <algorithm>
 #include <cstdio>
 #include <cstring>
@@ -23,6 +29,7 @@
 #include <memory>
 #include <sstream>
 #include <string>
+#include <vector>
 
 #include <dlfcn.h>
 
@@ -59,7 +66,8 @@ static std::string to_binary(size_t v, size_t len)
 // 3 = the reference's GPUQuantumGates over libGPUEmulator.so.
 // Writes "MEASURE bits:freq,..." or "PMEASURE bits:prob,..." into out.
 // Returns the qubit count, or a negative value on failure.
-extern "C" int qr_run(const char *path, int backend, int seed, int repeat, char *out, size_t out_len)
+extern "C" int qr_run_ex(const char *path, int backend, int seed, int repeat, int sample, char *out,
+                         size_t out_len, int *runs)
 {
     std::string file(path);
     QList list;
@@ -90,8 +98,41 @@ extern "C" int qr_run(const char *path, int backend, int seed, int repeat, char 
     ref_rng_seed(seed);
     std::map<std::string, double> res;
     std::string kind;
-    if (!transmit(list, &param, g.get())) return -3;
-    if (param.mPMeasureSize == 0) {
+    B200QuantumGates *b = (backend == 1 || backend == 2) ? static_cast<B200QuantumGates *>(g.get()) : nullptr;
+    bool deferred = false;
+    if (sample && b) {
+        QuantumGateParam probe;
+        probe.mQuantumBitNumber = n;
+        b->beginProbe();
+        const bool ok = transmit(list, &probe, g.get());
+        deferred = b->endProbe() && ok && probe.mPMeasureSize == 0;
+    }
+    if (runs) *runs = 1;
+    if (deferred) {
+        // the classical register of each MEASURE node, in program order
+        std::vector<int> creg;
+        for (QNode *p = list.qList.head->next; p; p = p->next)
+            if (p->gateSpecifier == MEASURE_GATE) creg.push_back(static_cast<MeasureNode *>(p)->creg);
+        b->beginDeferredMeasure();
+        if (!transmit(list, &param, g.get())) return -3;
+        if (!b->deferredTerminal() || b->deferredCount() != creg.size()) return -6;
+        std::vector<uint64_t> shots;
+        if (b->sampleDeferred((size_t)repeat, shots) != qErrorNone) return -6;
+        kind = "MEASURE";
+        for (uint64_t bits : shots) {
+            std::map<size_t, int> regs;                  // as the dispatcher fills mReturnValue
+            for (size_t k = 0; k < creg.size(); ++k) regs[(size_t)creg[k]] = (int)((bits >> k) & 1);
+            std::stringstream ss;
+            for (auto &kv : regs) ss << kv.second;
+            std::string bs = ss.str();
+            std::reverse(bs.begin(), bs.end());
+            res[bs] += 1.0;
+        }
+        for (auto &kv : res) kv.second /= repeat;
+    } else if (!transmit(list, &param, g.get())) {
+        return -3;
+    } else if (param.mPMeasureSize == 0) {
+        if (runs) *runs = repeat;
         kind = "MEASURE";
         for (int shot = 0; shot < repeat; ++shot) {
             if (shot && !transmit(list, &param, g.get())) return -3;
@@ -125,4 +166,34 @@ extern "C" int qr_run(const char *path, int backend, int seed, int repeat, char 
     if (s.size() + 1 > out_len) return -4;
     memcpy(out, s.c_str(), s.size() + 1);
     return n;
+}
+
+extern "C" int qr_run(const char *path, int backend, int seed, int repeat, char *out, size_t out_len)
+{
+    return qr_run_ex(path, backend, seed, repeat, 0, out, out_len, nullptr);
+}
+
+// The program run once (no shot loop) and the backend's getQState text
+// (CPUQuantumGates.cpp:64-82 for the reference CPU backend): backend 0 or
+// 1/2 as in qr_run.  Returns the text length, or a negative value.
+extern "C" long qr_qstate(const char *path, int backend, int seed, char *out, size_t out_len)
+{
+    std::string file(path);
+    QList list;
+    int n = QRunesParser(file, list);
+    if (n <= 0 || n > 30) return -1;
+    std::unique_ptr<QuantumGates> g;
+    if (backend == 0) g.reset(new CPUQuantumGates());
+    else if (backend == 1 || backend == 2) g.reset(new B200QuantumGates(backend == 2 ? QS_C64 : QS_C128));
+    else return -5;
+    QuantumGateParam param;
+    param.mQuantumBitNumber = n;
+    if (g->initState(&param) != qErrorNone) return -2;
+    ref_rng_seed(seed);
+    if (!transmit(list, &param, g.get())) return -3;
+    std::string s;
+    if (!g->getQState(s, &param)) return -3;
+    if (s.size() + 1 > out_len) return -(long)(s.size() + 1);
+    memcpy(out, s.c_str(), s.size() + 1);
+    return (long)s.size();
 }

@@ -27,15 +27,26 @@ def runner():
         _lib = C.CDLL(RUNNER_SO)
         _lib.qr_run.restype = C.c_int
         _lib.qr_run.argtypes = [C.c_char_p, C.c_int, C.c_int, C.c_int, C.c_char_p, C.c_size_t]
+        _lib.qr_run_ex.restype = C.c_int
+        _lib.qr_run_ex.argtypes = [C.c_char_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_char_p, C.c_size_t,
+                                   C.POINTER(C.c_int)]
+        _lib.qr_qstate.restype = C.c_long
+        _lib.qr_qstate.argtypes = [C.c_char_p, C.c_int, C.c_int, C.c_char_p, C.c_size_t]
     return _lib
 
 
-def run(path, backend, seed=12345, repeat=1):
-    """Returns (kind, {bitstring: value}, n_qubits)."""
+def run(path, backend, seed=12345, repeat=1, sample=False, runs_out=None):
+    """Returns (kind, {bitstring: value}, n_qubits).  sample: a B200 backend
+    runs a program whose measurements are all terminal once and samples the
+    shots (B200QuantumGates deferred measurement); runs_out (a list) receives
+    the number of simulations."""
     buf = C.create_string_buffer(1 << 20)
-    n = runner().qr_run(path.encode(), backend, seed, repeat, buf, len(buf))
+    runs = C.c_int(0)
+    n = runner().qr_run_ex(path.encode(), backend, seed, repeat, int(sample), buf, len(buf), C.byref(runs))
     if n < 0:
         raise RuntimeError(f"qr_run({path}, backend={backend}) failed: {n}")
+    if runs_out is not None:
+        runs_out.append(runs.value)
     text = buf.value.decode()
     kind, _, rest = text.partition(" ")
     res = {}
@@ -43,3 +54,17 @@ def run(path, backend, seed=12345, repeat=1):
         k, v = item.split(":")
         res[k] = float(v)
     return kind, res, n
+
+
+def qstate_text(path, backend, seed=12345):
+    """The backend's getQState text after one run of the program."""
+    need = 1 << 16
+    while True:
+        buf = C.create_string_buffer(need)
+        r = runner().qr_qstate(path.encode(), backend, seed, buf, len(buf))
+        if r >= 0:
+            return buf.value.decode()
+        if r < -5 and -r > need:
+            need = -r
+            continue
+        raise RuntimeError(f"qr_qstate({path}, backend={backend}) failed: {r}")

@@ -19,7 +19,15 @@ def random_state(n, seed):
     return v / np.linalg.norm(v)
 
 
-KERNELS = ["single", "tiled"]
+# "tiled": the default tiled passes (the tile in tensor memory, k_tile_tmem,
+# where a pass fits it); "tiled-smem": every pass on k_fused_tile.
+KERNELS = ["single", "tiled", "tiled-smem"]
+
+
+def make_plan(n, g, kernel="tiled", **kw):
+    if kernel == "tiled-smem":
+        return FusionPlan(n, g, kernel="tiled", tile_in_tmem=0, **kw)
+    return FusionPlan(n, g, kernel=kernel, **kw)
 
 
 def check_fused(n, g, init=None, kernel="tiled", **kw):
@@ -28,7 +36,7 @@ def check_fused(n, g, init=None, kernel="tiled", **kw):
     if init is not None:
         sv.set_state(init.astype(np.complex64))
         o.set_state(init.astype(np.complex64).astype(np.complex128))
-    p = FusionPlan(n, g, kernel=kernel, **kw)
+    p = make_plan(n, g, kernel=kernel, **kw)
     p.apply(sv)
     p.status(sv)
     o.apply(g)
@@ -82,7 +90,7 @@ def test_fused_block_positions(need_gpu):
             spec.append(("SQISWAP", (b, a)))
         g = circuits.make_gates(spec)
         for kernel in KERNELS:
-            p = FusionPlan(n, g, kernel=kernel)
+            p = make_plan(n, g, kernel=kernel)
             assert p.num_blocks() == 1 and p.block(0)[0] == sorted(qs)
             check_fused(n, g, init=random_state(n, qs[0] + 7), kernel=kernel)
 
@@ -91,7 +99,7 @@ def test_fused_block_positions(need_gpu):
 def test_fused_vqe_and_reuse(need_gpu, kernel):
     n = 16
     g = circuits.vqe_ansatz(n, 4, seed=5)
-    p = FusionPlan(n, g, kernel=kernel)
+    p = make_plan(n, g, kernel=kernel)
     a = StateVector(n, "c64")
     p.apply(a)
     p.apply(a)               # a plan applies repeatedly
@@ -101,20 +109,21 @@ def test_fused_vqe_and_reuse(need_gpu, kernel):
     assert np.abs(a.get_state() - o.state()).max() < AMP_TOL
 
 
+@pytest.mark.parametrize("tmem", [1, 0])
 @pytest.mark.parametrize("remap", [1, 2])
 @pytest.mark.parametrize("max_sub", [1, 2, 3])
 @pytest.mark.parametrize("n", [20, 21])
-def test_tiled_remap(need_gpu, n, max_sub, remap):
+def test_tiled_remap(need_gpu, n, max_sub, remap, tmem):
     """Remapped passes (ping-pong through a second buffer, contiguous tile
     writes, natural order back at the end) at an even and an odd count of
     passes; a second application reuses the spare buffer, and releasing it
     leaves the state intact."""
     g = circuits.random_layers(n, 6, 90 + n + max_sub, iswap_frac=0.2)
     init = random_state(n, n + max_sub)
-    check_fused(n, g, init=init, kernel="tiled", max_sub=max_sub, remap=remap)
+    check_fused(n, g, init=init, kernel="tiled", max_sub=max_sub, remap=remap, tile_in_tmem=tmem)
     sv = StateVector(n, "c64")
     sv.set_state(init.astype(np.complex64))
-    p = FusionPlan(n, g, max_sub=max_sub, remap=remap)
+    p = FusionPlan(n, g, max_sub=max_sub, remap=remap, tile_in_tmem=tmem)
     p.apply(sv)
     p.apply(sv)
     p.status(sv)
@@ -138,14 +147,14 @@ def test_tiled_two_threads_per_row(need_gpu, n, max_sub, remap):
 
 
 @pytest.mark.parametrize("kernel,remap,tpr", [("single", 0, 1), ("tiled", 0, 1), ("tiled", 1, 1), ("tiled", 2, 1),
-                                              ("tiled", 1, 2)])
+                                              ("tiled", 1, 2), ("tiled-smem", 1, 1)])
 def test_fused_fidelity_26q_vs_fp64_gpu(need_gpu, kernel, remap, tpr):
     """26 qubits, 12 layers: fused complex64 against the complex128 per-gate
     path (itself pinned to the oracle by the other tests)."""
     n = 26
     g = circuits.random_layers(n, 12, 7, iswap_frac=0.1)
     f = StateVector(n, "c64")
-    p = FusionPlan(n, g, kernel=kernel, remap=remap, threads_per_row=tpr)
+    p = make_plan(n, g, kernel=kernel, remap=remap, threads_per_row=tpr)
     p.apply(f)
     p.status(f)
     d = StateVector(n, "c128")
@@ -163,7 +172,7 @@ def test_fused_range_with_interleaved_probs(need_gpu, kernel):
     the same state as the whole plan (norm partials survive other calls)."""
     n = 20
     g = circuits.random_layers(n, 6, 11, iswap_frac=0.1)
-    p = FusionPlan(n, g, kernel=kernel)
+    p = make_plan(n, g, kernel=kernel)
     a, b = StateVector(n, "c64"), StateVector(n, "c64")
     p.apply(a)
     for i in range(p.num_launches()):
@@ -181,3 +190,23 @@ def test_small_state_plan_runs_per_gate(need_gpu):
     o = OracleState(n)
     o.apply(g)
     assert np.abs(sv.get_state() - o.state()).max() < 1e-12
+
+
+@pytest.mark.parametrize("remap", [0, 1])
+def test_tile_in_tmem_matches_shared_memory_kernel(need_gpu, remap):
+    """The two tiled kernels apply the same passes with the same split-BF16
+    products: their results agree to FP32 accumulation-order differences,
+    and each is within the bar of the oracle (checked above)."""
+    n = 22
+    g = circuits.random_layers(n, 10, 4242, iswap_frac=0.1)
+    init = random_state(n, 5).astype(np.complex64)
+    out = []
+    for tmem in (1, 0):
+        sv = StateVector(n, "c64")
+        sv.set_state(init)
+        p = FusionPlan(n, g, remap=remap, tile_in_tmem=tmem)
+        p.apply(sv)
+        p.status(sv)
+        out.append(sv)
+    mx, _ = out[0].diff(out[1])
+    assert mx < 1e-6, mx

@@ -16,7 +16,20 @@ from qpanda_b200.qrunes import to_qrunes
 from tests import qrunes_harness as H
 
 needs_runner = pytest.mark.skipif(not H.available(), reason="tests/qrunes not built (needs the reference tree)")
-REF_SDK = os.path.join(os.environ.get("QPANDA_REF", "/root/reference"), "QPandaSDK")
+
+
+def _ref_sdk():
+    """The reference's QPandaSDK directory: QPANDA_REF, or where build()
+    found the reference tree ("" when neither is there)."""
+    ref = os.environ.get("QPANDA_REF", "")
+    rec = os.path.join(os.path.dirname(os.path.abspath(__file__)), "qrunes", "_build", "qpanda_ref.txt")
+    if not ref and os.path.exists(rec):
+        with open(rec) as f:
+            ref = f.read().strip()
+    return os.path.join(ref, "QPandaSDK") if ref else ""
+
+
+REF_SDK = _ref_sdk()
 
 
 def programs(tmp_path):
@@ -63,7 +76,7 @@ def test_cpu_harness_matches_oracle(tmp_path):
 
 
 @needs_runner
-@pytest.mark.skipif(not os.path.isdir(REF_SDK), reason="reference fixture programs not present")
+@pytest.mark.skipif(not REF_SDK or not os.path.isdir(REF_SDK), reason="reference fixture programs not present")
 def test_cpu_harness_reference_fixtures():
     kind, res, _ = H.run(os.path.join(REF_SDK, "shor.txt"), H.CPU)
     assert kind == "PMEASURE"
@@ -166,3 +179,79 @@ def test_cpu_harness_every_gate_program_matches_oracle(tmp_path):
     top = sorted(range(128), key=lambda i: (-p[i], i))[:10]
     for i in top:
         assert abs(res[format(i, "07b")] - p[i]) < 1e-12
+
+
+# ------------------------------------------------ shots, RESET, getQState text
+def _write(tmp_path, name, text):
+    p = tmp_path / name
+    p.write_text(text)
+    return str(p)
+
+
+@needs_runner
+@pytest.mark.gpu
+def test_terminal_measures_one_run_plus_sampling(need_gpu, tmp_path):
+    """QPandaSDK::run re-simulates a MEASURE program once per shot
+    (QPandaAPI.cpp:169-182).  With every MEASURE terminal, the B200 backend
+    runs it once and samples the shots, drawing each shot's uniforms from the
+    same 16807 stream at the positions the loop would: the counts equal the
+    reference CPU backend's per-shot loop, shot for shot; classical registers
+    in scrambled order, one qubit measured twice."""
+    n = 10
+    g = circuits.random_layers(n, 5, 31)
+    order = (3, 0, 9, 5, 1, 8, 2, 7, 4, 6)
+    measure = [(q, (7 * q + 3) % n) for q in order] + [(order[0], n)]
+    path = _write(tmp_path, "terminal.txt", to_qrunes(n, g, measure=measure))
+    k0, r0, _ = H.run(path, H.CPU, seed=4242, repeat=300)
+    runs = []
+    k1, r1, _ = H.run(path, H.B200_C128, seed=4242, repeat=300, sample=True, runs_out=runs)
+    assert k0 == k1 == "MEASURE" and runs == [1]
+    assert r0 == r1
+
+
+@needs_runner
+@pytest.mark.gpu
+def test_measure_followed_by_a_gate_runs_the_loop(need_gpu, tmp_path):
+    """A gate after a MEASURE on the measured qubit: the probe pass sees it,
+    and the shots come from the per-shot loop (one run per shot)."""
+    text = "\n".join(["QINIT 4", "CREG 3", "H 0", "CNOT 0,1", 'RY 2,"0.9"', "MEASURE 0,$0", "H 0",
+                      'RX 1,"0.3"', "MEASURE 0,$1", "MEASURE 1,$2"]) + "\n"
+    path = _write(tmp_path, "nonterminal.txt", text)
+    k0, r0, _ = H.run(path, H.CPU, seed=11, repeat=120)
+    runs = []
+    k1, r1, _ = H.run(path, H.B200_C128, seed=11, repeat=120, sample=True, runs_out=runs)
+    assert runs == [120]
+    assert r0 == r1
+
+
+@needs_runner
+@pytest.mark.gpu
+def test_reset_matches_cpu_backend(need_gpu, tmp_path):
+    """RESET (CPUQuantumGates.cpp:126-136: a measurement, then NOT when it gave
+    1; its draws shift the generator stream by one or two): the per-shot
+    counts of a program with two RESETs equal the CPU backend's; with
+    sampling asked for, RESET keeps the loop."""
+    text = "\n".join(["QINIT 5", "CREG 5", "H 0", "CNOT 0,1", 'RY 2,"1.1"', "RESET 1", "CNOT 2,1", "H 3",
+                      "RESET 3", 'RX 3,"0.7"'] + [f"MEASURE {q},${q}" for q in range(5)]) + "\n"
+    path = _write(tmp_path, "reset.txt", text)
+    k0, r0, _ = H.run(path, H.CPU, seed=5, repeat=200)
+    for backend in (H.B200_C128, H.B200_C64):
+        runs = []
+        k1, r1, _ = H.run(path, backend, seed=5, repeat=200, sample=True, runs_out=runs)
+        assert runs == [200]
+        assert r0 == r1, backend
+
+
+@needs_runner
+@pytest.mark.gpu
+def test_getqstate_text_matches_cpu_backend(need_gpu, tmp_path):
+    """B200QuantumGates::getQState prints the state as CPUQuantumGates::getQState
+    does (CPUQuantumGates.cpp:64-82), byte for byte, for a program whose
+    amplitudes sit well inside their printed digits."""
+    text = "\n".join(["QINIT 4", "CREG 1", "H 0", "H 1", "CNOT 1,2", 'RZ 2,"0.5"', 'RX 3,"1.25"',
+                      'CR 0,3,"0.75"']) + "\n"
+    path = _write(tmp_path, "qstate.txt", text)
+    t0 = H.qstate_text(path, H.CPU)
+    t1 = H.qstate_text(path, H.B200_C128)
+    assert t0.count("\n") == 16
+    assert t0 == t1

@@ -33,6 +33,7 @@
 #include "qs_fused.h"
 #include "qs_plan_internal.h"
 #include "qs_tile_core.cuh"
+#include "qs_tile_tmem.cuh"
 
 using qs_tile::Layout;
 using qs_tile::LoadMap;
@@ -90,22 +91,15 @@ extern "C" const char *tile_emu_error(void) { return g_err; }
 // Apply plan passes [0, all) to state (2^n complex128, interleaved re/im).
 // *kinds_out (may be NULL) counts the passes whose chunk pairs are adjacent
 // columns [0], other columns [1], two rows [2].
-extern "C" int tile_emu_apply(const qs_plan *P, int n, double *state, int remap, int tpr, int *n_passes_out,
-                              int *kinds_out)
+// Pass k (descriptor d, destination dst_k as qs_plan_tiled_schedule gives it)
+// the way k_fused_tile moves data.
+static int smem_pass(const qs_plan *P, int n, const qs_tiled_desc &d, int dst_k, size_t k, int tpr,
+                     std::vector<cd> *bufs[2], std::vector<int> &hits, int *kinds_out)
 {
-    if (tpr != 1 && tpr != 2) return fail("threads per row must be 1 or 2");
-    g_err[0] = 0;
-    const size_t npass = P->passes.size();
-    std::vector<qs_tiled_desc> descs;
-    std::vector<int> dst;
-    if (qs_plan_tiled_schedule(P, n, 0, npass, remap, descs, dst)) return fail("schedule failed");
-    if (n_passes_out) *n_passes_out = (int)npass;
     const uint64_t N = 1ull << n, tiles = N >> 12;
-    std::vector<cd> buf0(reinterpret_cast<cd *>(state), reinterpret_cast<cd *>(state) + N), buf1(N, cd(0, 0));
-    std::vector<cd> *bufs[2] = {&buf0, &buf1};
-    std::vector<int> hits(N);
-    for (size_t k = 0; k < npass; ++k) {
-        const qs_tiled_desc &d = descs[k];
+    std::vector<cd> &buf0 = *bufs[0];
+    {
+        const int dst[1] = {dst_k};
         Layout L;
         LoadMap M;
         if (qs_tile_layout_build(n, d.T, d.nsub, d.qpos, d.has_rows ? d.rows : nullptr, &L, &M,
@@ -117,12 +111,12 @@ extern "C" int tile_emu_apply(const qs_plan *P, int n, double *state, int remap,
         W.mode = d.has_write ? d.wmode : 0;
         W.ntb = n - 12;
         for (int i = 0; i < W.ntb && i < 52; ++i) W.wpos[i] = (int8_t)d.wpos[i];
-        if (d.has_write && dst[k] < 0) return fail("remapped pass scheduled in place", (long long)k);
-        const std::vector<cd> &in = dst[k] < 0 ? buf0 : *bufs[dst[k] ^ 1];
+        if (d.has_write && dst[0] < 0) return fail("remapped pass scheduled in place", (long long)k);
+        const std::vector<cd> &in = dst[0] < 0 ? buf0 : *bufs[dst[0] ^ 1];
         std::vector<cd> in_copy;
-        if (dst[k] < 0) in_copy = buf0;            // in place: tiles read and write the same set
-        const std::vector<cd> &src = dst[k] < 0 ? in_copy : in;
-        std::vector<cd> &out = dst[k] < 0 ? buf0 : *bufs[dst[k]];
+        if (dst[0] < 0) in_copy = buf0;            // in place: tiles read and write the same set
+        const std::vector<cd> &src = dst[0] < 0 ? in_copy : in;
+        std::vector<cd> &out = dst[0] < 0 ? buf0 : *bufs[dst[0]];
         // block unitaries (row = output basis index, column = input)
         std::vector<std::vector<cd>> U(d.nsub, std::vector<cd>(32 * 32));
         for (int b = 0; b < d.nsub; ++b) {
@@ -225,6 +219,25 @@ extern "C" int tile_emu_apply(const qs_plan *P, int n, double *state, int remap,
         for (uint64_t i = 0; i < N; ++i)
             if (hits[i] != 1) return fail("output amplitude not written exactly once", (long long)k, (long long)i);
     }
+    return 0;
+}
+
+extern "C" int tile_emu_apply(const qs_plan *P, int n, double *state, int remap, int tpr, int *n_passes_out,
+                              int *kinds_out)
+{
+    if (tpr != 1 && tpr != 2) return fail("threads per row must be 1 or 2");
+    g_err[0] = 0;
+    const size_t npass = P->passes.size();
+    std::vector<qs_tiled_desc> descs;
+    std::vector<int> dst;
+    if (qs_plan_tiled_schedule(P, n, 0, npass, remap, descs, dst)) return fail("schedule failed");
+    if (n_passes_out) *n_passes_out = (int)npass;
+    const uint64_t N = 1ull << n;
+    std::vector<cd> buf0(reinterpret_cast<cd *>(state), reinterpret_cast<cd *>(state) + N), buf1(N, cd(0, 0));
+    std::vector<cd> *bufs[2] = {&buf0, &buf1};
+    std::vector<int> hits(N);
+    for (size_t k = 0; k < npass; ++k)
+        if (smem_pass(P, n, descs[k], dst[k], k, tpr, bufs, hits, kinds_out)) return 1;
     memcpy(state, buf0.data(), N * sizeof(cd));
     return 0;
 }
@@ -291,5 +304,212 @@ extern "C" int tile_emu_rebind(const qs_plan *proto, const qs_gate *gates, size_
 {
     g_err[0] = 0;
     if (qs_plan_rebind(proto, gates, count, out)) return fail("rebind failed");
+    return 0;
+}
+
+// ---------------------------------------------------------------- k_tile_tmem
+// The same plans the way k_tile_tmem (qpanda_b200/csrc/qs_tile_tmem.cu) moves
+// data, pass by pass where its layout builder takes the pass (the others as
+// k_fused_tile above would, through the same tables):
+//   * copy_tile: chunk c = 128 k + t of the tile, from g_t | gk[k], into stage
+//     chunk  (t ^ cf_t) ^ (k << 7) ^ cf_k[k];
+//   * the gather: thread (warp w, lane l) reads column j of its block-0 row at
+//     stage slot  xrow(w, l) ^ s_col[j];
+//   * each block's product with its matrix permuted to the kernel's column
+//     order (tmem_matrix_index over mperm[b]) in FP64;
+//   * the exchanges between blocks as the warp shuffles of swap_bit do them;
+//   * the last block's stores at store_base | o_lane / o_warp | o_col.
+// Every staging slot must be written once and read once per tile, every output
+// amplitude written once per pass.  conflicts[0] counts shared-memory phases
+// of the gather whose lanes share a bank slot, conflicts[1] those of the
+// copies; passes[0] / [1] count the passes the kernel took / left.
+extern "C" int tmem_emu_apply(const qs_plan *P, int n, double *state, int remap, int *passes, long long *conflicts)
+{
+    g_err[0] = 0;
+    const size_t npass = P->passes.size();
+    std::vector<qs_tiled_desc> descs;
+    std::vector<int> dst;
+    if (qs_plan_tiled_schedule(P, n, 0, npass, remap, descs, dst)) return fail("schedule failed");
+    const uint64_t N = 1ull << n, tiles = N >> 12;
+    std::vector<cd> buf0(reinterpret_cast<cd *>(state), reinterpret_cast<cd *>(state) + N), buf1(N, cd(0, 0));
+    std::vector<cd> *bufs[2] = {&buf0, &buf1};
+    std::vector<int> hits(N);
+    for (size_t k = 0; k < npass; ++k) {
+        const qs_tiled_desc &d = descs[k];
+        qs_tmem::TLayout T;
+        const int rb = qs_tmem_layout_build(n, &d, &T);
+        if (rb == QS_ERR_UNSUPPORTED) {             // the product runs it on k_fused_tile
+            passes[1]++;
+            if (smem_pass(P, n, d, dst[k], k, 1, bufs, hits, nullptr)) return 1;
+            continue;
+        }
+        if (rb) return fail("tmem layout build failed", (long long)k);
+        passes[0]++;
+        StoreMap W;
+        memset(&W, 0, sizeof(W));
+        W.mode = d.has_write ? d.wmode : 0;
+        W.ntb = n - 12;
+        for (int i = 0; i < W.ntb && i < 52; ++i) W.wpos[i] = (int8_t)d.wpos[i];
+        const std::vector<cd> &in = dst[k] < 0 ? buf0 : *bufs[dst[k] ^ 1];
+        std::vector<cd> in_copy;
+        if (dst[k] < 0) in_copy = buf0;
+        const std::vector<cd> &src = dst[k] < 0 ? in_copy : in;
+        std::vector<cd> &out = dst[k] < 0 ? buf0 : *bufs[dst[k]];
+        // block matrices in the kernel's column order
+        std::vector<std::vector<cd>> U(d.nsub, std::vector<cd>(32 * 32));
+        for (int b = 0; b < d.nsub; ++b) {
+            int kq = 0, qs[5];
+            std::vector<double> m(2048);
+            if (qs_plan_block(P, d.first_block + b, &kq, qs, m.data())) return fail("block", b);
+            for (uint32_t i = 0; i < 32; ++i)
+                for (uint32_t j = 0; j < 32; ++j) {
+                    const uint32_t si = qs_tmem::tmem_matrix_index(i, T.mperm[b]);
+                    const uint32_t sj = qs_tmem::tmem_matrix_index(j, T.mperm[b]);
+                    U[b][i * 32 + j] = cd(m[2 * (si * 32 + sj)], m[2 * (si * 32 + sj) + 1]);
+                }
+        }
+        // the tile base as tbase_of computes it
+        Layout TL;
+        memset(&TL, 0, sizeof(TL));
+        for (int j = 0; j < 12; ++j) TL.tpos[j] = T.tpos[j];
+        std::fill(hits.begin(), hits.end(), 0);
+        std::vector<cd> stage(4096);
+        std::vector<int> wr(4096), rd(4096);
+        std::vector<cd> y(128 * 32), y2(128 * 32);
+        for (uint64_t t = 0; t < tiles; ++t) {
+            const uint64_t tbase = deposit_tile(t, TL);
+            std::fill(wr.begin(), wr.end(), 0);
+            std::fill(rd.begin(), rd.end(), 0);
+            for (int lt = 0; lt < 128; ++lt) {
+                uint64_t g_t = 0;
+                uint32_t cs_t = (uint32_t)lt;
+                for (int b = 0; b < 7; ++b)
+                    if ((lt >> b) & 1) { g_t |= T.g_bit[b]; cs_t ^= T.cf_bit[b]; }
+                for (int kk = 0; kk < 16; ++kk) {
+                    const uint64_t s = tbase | g_t | T.gk[kk];
+                    if (s + 1 >= N) return fail("load out of range", (long long)s);
+                    const uint32_t c = cs_t ^ ((uint32_t)kk << 7) ^ T.cf_k[kk];
+                    if (c >= 2048) return fail("stage chunk out of range", lt, kk);
+                    stage[2 * c] = src[s];
+                    stage[2 * c + 1] = src[s + 1];
+                    wr[2 * c]++;
+                    wr[2 * c + 1]++;
+                }
+            }
+            // copies: the 8 lanes of a quarter warp must write 8 distinct 16-byte bank slots
+            if (t == 0)
+                for (int kk = 0; kk < 16; ++kk)
+                    for (int q = 0; q < 16; ++q) {
+                        unsigned seen = 0;
+                        bool clash = false;
+                        for (int l = 0; l < 8; ++l) {
+                            const int lt = 8 * q + l;
+                            uint32_t cs_t = (uint32_t)lt;
+                            for (int b = 0; b < 7; ++b)
+                                if ((lt >> b) & 1) cs_t ^= T.cf_bit[b];
+                            const uint32_t c = cs_t ^ ((uint32_t)kk << 7) ^ T.cf_k[kk];
+                            const unsigned bit = 1u << (c & 7);
+                            if (seen & bit) clash = true;
+                            seen |= bit;
+                        }
+                        if (clash) conflicts[1]++;
+                    }
+            for (int o = 0; o < 4096; ++o)
+                if (wr[o] != 1) return fail("staging slot not written exactly once", (long long)t, o);
+            // gather
+            for (int w = 0; w < 4; ++w)
+                for (int l = 0; l < 32; ++l) {
+                    uint32_t x = 0;
+                    for (int i = 0; i < 5; ++i)
+                        if ((l >> i) & 1) x ^= T.s_lane[i];
+                    for (int v = 0; v < 2; ++v)
+                        if ((w >> v) & 1) x ^= T.s_warp[v];
+                    for (int j = 0; j < 32; ++j) {
+                        const uint32_t sl = x ^ T.s_col[j];
+                        if (sl >= 4096) return fail("gather slot out of range", l, j);
+                        if (T.pair_in && (j & 1) && sl != (x ^ T.s_col[j - 1]) + 1)
+                            return fail("gathered column pair not adjacent", l, j);
+                        y[(32 * w + l) * 32 + j] = stage[sl];
+                        rd[sl]++;
+                    }
+                }
+            for (int o = 0; o < 4096; ++o)
+                if (rd[o] != 1) return fail("staging slot not gathered exactly once", (long long)t, o);
+            if (t == 0) {
+                // gather phases: 8 lanes (16-byte reads of column pairs) or 16
+                // lanes (8-byte reads) must hit distinct bank slots
+                const int ph = T.pair_in ? 8 : 16;
+                for (int w = 0; w < 4; ++w)
+                    for (int j = 0; j < 32; j += T.pair_in ? 2 : 1)
+                        for (int p0 = 0; p0 < 32; p0 += ph) {
+                            unsigned seen = 0;
+                            bool clash = false;
+                            for (int l = p0; l < p0 + ph; ++l) {
+                                uint32_t x = 0;
+                                for (int i = 0; i < 5; ++i)
+                                    if ((l >> i) & 1) x ^= T.s_lane[i];
+                                for (int v = 0; v < 2; ++v)
+                                    if ((w >> v) & 1) x ^= T.s_warp[v];
+                                const uint32_t sl = x ^ T.s_col[j];
+                                const unsigned bit = T.pair_in ? 1u << ((sl >> 1) & 7) : 1u << (sl & 15);
+                                if (seen & bit) clash = true;
+                                seen |= bit;
+                            }
+                            if (clash) conflicts[0]++;
+                        }
+            }
+            for (int b = 0; b < d.nsub; ++b) {
+                for (int r = 0; r < 128; ++r)
+                    for (int i = 0; i < 32; ++i) {
+                        cd acc(0, 0);
+                        for (int j = 0; j < 32; ++j) acc += U[b][i * 32 + j] * y[r * 32 + j];
+                        y2[r * 32 + i] = acc;
+                    }
+                y.swap(y2);
+                if (b + 1 < d.nsub) {
+                    for (int s = 0; s < T.nswap[b]; ++s) {
+                        const int R = T.swap_r[b][s], lm = 1 << T.swap_l[b][s];
+                        if (R < 0 || R > 4 || lm > 16 || lm < 1) return fail("swap out of range", b, s);
+                        y2 = y;
+                        for (int w = 0; w < 4; ++w)
+                            for (int l = 0; l < 32; ++l) {
+                                const bool up = (l & lm) != 0;
+                                const int pl = l ^ lm;
+                                for (int j = 0; j < 32; ++j) {
+                                    if (j & (1 << R)) continue;
+                                    const int j1 = j | (1 << R);
+                                    // partner's send: its up ? y[j] : y[j1]
+                                    const bool pup = !up;
+                                    const cd recv = y2[(32 * w + pl) * 32 + (pup ? j : j1)];
+                                    if (up) y[(32 * w + l) * 32 + j] = recv;
+                                    else y[(32 * w + l) * 32 + j1] = recv;
+                                }
+                            }
+                    }
+                } else {
+                    const uint64_t ob = emu_store_base(t, tbase, W);
+                    for (int w = 0; w < 4; ++w)
+                        for (int l = 0; l < 32; ++l) {
+                            uint64_t orow = 0;
+                            for (int i = 0; i < 5; ++i)
+                                if ((l >> i) & 1) orow |= T.o_lane[i];
+                            for (int v = 0; v < 2; ++v)
+                                if ((w >> v) & 1) orow |= T.o_warp[v];
+                            for (int j = 0; j < 32; ++j) {
+                                const uint64_t o = ob | orow | T.o_col[j];
+                                if (o >= N) return fail("store out of range", (long long)o);
+                                if (T.vec_out && (j & 1) && o != (ob | orow | T.o_col[j - 1]) + 1)
+                                    return fail("stored column pair not adjacent", l, j);
+                                out[o] = y[(32 * w + l) * 32 + j];
+                                hits[o]++;
+                            }
+                        }
+                }
+            }
+        }
+        for (uint64_t i = 0; i < N; ++i)
+            if (hits[i] != 1) return fail("output amplitude not written exactly once", (long long)k, (long long)i);
+    }
+    memcpy(state, buf0.data(), N * sizeof(cd));
     return 0;
 }
