@@ -178,22 +178,26 @@ int qs_inner(qs_state *a, qs_state *b, double *re, double *im);
 /* max_i |a_i - b_i| and sum_i |a_i - b_i|^2 on the device (dtypes may differ). */
 int qs_diff(qs_state *a, qs_state *b, double *max_abs, double *sum_sq);
 
-/* qubitMeasure for callers that cannot allocate memory when they measure.
- * No counterpart in the reference.  qs_measure keeps its reduction partials in
- * scratch that qs_create allocated; this entry point allocates nothing (no
- * cudaMalloc, cudaFree or allocating library call) and needs no qs_state, for
- * a serving loop that reserved all device memory up front, a framework whose
- * own allocator owns the device memory, or a caller that holds the amplitudes
- * in a buffer of its own.  amp: 2^n_qubits amplitudes of dtype on the current
- * device, collapsed in place; u: the uniform of qubitMeasure's rule;
- * outcome_dev / p0_dev: device words that receive the outcome (-1 if the
- * selected outcome has probability 0, state left unchanged) and P(qubit q ==
- * 0).  Asynchronous on `stream`.  Its partial sums live in a fixed 512 KB
- * device array compiled into the library (held on every GPU that loads it
- * until exit), which limits states to at most 32 qubits; larger ones are
- * rejected with QS_ERR_ARG.  The first call on a device looks up that
- * array's address (cudaGetSymbolAddress): make it before any stream capture
- * on the device.  All calls share the array, so calls that overlap on the GPU
+/* Measurement of qubit q for callers that cannot allocate memory when they
+ * measure.  No counterpart in the reference.  qs_measure keeps its reduction
+ * partials in scratch that qs_create allocated; this entry point allocates
+ * nothing (no cudaMalloc, cudaFree or allocating library call) and needs no
+ * qs_state, for a serving loop that reserved all device memory up front, a
+ * framework whose own allocator owns the device memory, or a caller that holds
+ * the amplitudes in a buffer of its own.  amp: 2^n_qubits amplitudes of dtype
+ * on the current device (8-byte aligned for complex64, 16-byte for
+ * complex128), collapsed in place: with p0 = P(qubit q == 0) summed in FP64,
+ * the outcome is 1 when (float)u > p0, else 0; the half of the state with the
+ * outcome is scaled by 1/sqrt(p) (p = p0 or 1 - p0) and the other half set to
+ * zero.  outcome_dev / p0_dev: device words that receive the outcome (-1 if
+ * the selected outcome has probability 0, state left unchanged) and p0.
+ * Asynchronous on `stream`.  Its partial sums live in a fixed 512 KB device
+ * array compiled into the library (held on every GPU that loads it until
+ * exit), which limits states to at most 32 qubits; larger ones are rejected
+ * with QS_ERR_ARG.  The first call on a device looks up that array's address
+ * (cudaGetSymbolAddress) and keeps it: make that call before any stream
+ * capture on the device, and do not reset the device (cudaDeviceReset)
+ * between calls.  All calls share the array, so calls that overlap on the GPU
  * (unordered streams) race; calls ordered on one stream do not. */
 int qs_measure_noalloc(void *amp, int n_qubits, int dtype, int q, double u,
                        int *outcome_dev, double *p0_dev, void *stream);
@@ -261,6 +265,13 @@ int qs_plan_apply_range(qs_state *s, qs_plan *plan, size_t first, size_t count);
 /* Synchronize and report whether a bounded wait inside a fused pass expired
  * since the last qs_plan_apply (QS_ERR_STATE) - a watchdog, not expected. */
 int qs_plan_status(qs_state *s);
+/* Self-test of the bounded waits above: one kernel waits wait_us
+ * microseconds (1 us .. 2 s) on an mbarrier that nothing arrives on, gives up,
+ * and sets the word that qs_plan_status reads, which then returns
+ * QS_ERR_STATE; the context stays usable.  Asynchronous on the state's
+ * stream.  No reference counterpart (the reference's kernels have no
+ * waits). */
+int qs_watchdog_selftest(qs_state *s, unsigned wait_us);
 /* Free the second state-size buffer that plans with remap = 1 keep with the
  * state (no-op when there is none).  No reference counterpart. */
 int qs_release_spare(qs_state *s);
@@ -316,7 +327,12 @@ typedef struct qs_batch_opts {
     int low_qubits;        /* qubits 0..low_qubits-1 in every tile, 1..5 */
     int order;             /* QS_BATCH_LONGEST_FIRST or QS_BATCH_INPUT_ORDER */
     int use_graph;         /* capture the launch in a CUDA graph and replay it */
+    int block_qubits;      /* fusion width: gates are grouped into blocks of at most 4 or 5 qubits
+                              (default 5; applied as 5-qubit blocks either way) */
 } qs_batch_opts;
+/* Defaults (2 blocks per pass, 3 low qubits, longest first, graph, 5-qubit
+ * fusion).  Fill a qs_batch_opts with this call before changing fields: the
+ * struct may gain fields at its end. */
 int qs_batch_default_opts(qs_batch_opts *opts);
 /* Circuit c has n_qubits[c] qubits and gates[offsets[c] .. offsets[c+1]). */
 int qs_batch_create(int n_circuits, const int *n_qubits, const qs_gate *gates, const size_t *offsets,
@@ -332,11 +348,20 @@ int qs_batch_zz_offsets(const qs_batch *b, size_t *offsets);
 int qs_batch_state(qs_batch *b, int circuit, void *host_out, int host_dtype);
 int qs_batch_info(const qs_batch *b, size_t *state_bytes, size_t *passes_total);
 int qs_batch_destroy(qs_batch *b);
-/* Autotuner: build and time candidate options (blocks per pass 1..3, lowest
- * tile qubits 3 or 5, queue order) on every stride-th circuit and write the
- * fastest to *best (with use_graph set) and its time per run to *best_ms. */
+/* Autotuner: build and time candidate options (fusion width 4 or 5 qubits,
+ * blocks per pass 1..3, lowest tile qubits 3 or 5, queue order) on every
+ * stride-th circuit and write the fastest to *best (with use_graph set) and
+ * its time per run to *best_ms. */
 int qs_batch_autotune(int n_circuits, const int *n_qubits, const qs_gate *gates, const size_t *offsets,
                       int stride, qs_batch_opts *best, double *best_ms);
+/* The same, with the result kept in a text file: cache_path holds one line
+ * per tuning, keyed by the device (name, SM count) and the sampled circuits'
+ * gate pattern (operations and qubits; angles do not change the timing).  A
+ * key found there is returned without timing anything (*from_cache = 1); a
+ * new one is tuned and appended (*from_cache = 0).  No reference counterpart. */
+int qs_batch_autotune_cached(int n_circuits, const int *n_qubits, const qs_gate *gates, const size_t *offsets,
+                             int stride, const char *cache_path, qs_batch_opts *best, double *best_ms,
+                             int *from_cache);
 
 /* ---- request loop: continuous batching on one GPU ----------------------- */
 /* Requests (a circuit, plus 1024-style shots or the full probability vector)

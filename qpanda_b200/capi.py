@@ -94,6 +94,7 @@ def lib():
         "qs_batch_info": (i, [vp, C.POINTER(sz), C.POINTER(sz)]),
         "qs_batch_destroy": (i, [vp]),
         "qs_batch_autotune": (i, [i, ip, vp, C.POINTER(sz), i, vp, dp]),
+        "qs_batch_autotune_cached": (i, [i, ip, vp, C.POINTER(sz), i, C.c_char_p, vp, dp, ip]),
         "qs_plan_create_ex": (i, [i, vp, sz, vp, C.POINTER(vp)]),
         "qs_plan_default_opts": (i, [vp]),
         "qs_plan_launches": (i, [vp, C.POINTER(sz)]),
@@ -106,6 +107,7 @@ def lib():
         "qs_diff": (i, [vp, vp, dp, dp]),
         "qs_measure_noalloc": (i, [vp, i, i, i, d, vp, vp, vp]),
         "qs_plan_status": (i, [vp]),
+        "qs_watchdog_selftest": (i, [vp, C.c_uint]),
         "qs_release_spare": (i, [vp]),
         "qs_write_fullstate": (i, [vp, C.c_char_p, i]),
         "qs_format_outcomes": (i, [C.POINTER(C.c_uint64), dp, sz, i, C.c_char_p, sz, C.POINTER(sz)]),
@@ -373,7 +375,8 @@ class FusionPlan:
 
 
 class BatchOpts(C.Structure):
-    _fields_ = [("max_sub", C.c_int), ("low_qubits", C.c_int), ("order", C.c_int), ("use_graph", C.c_int)]
+    _fields_ = [("max_sub", C.c_int), ("low_qubits", C.c_int), ("order", C.c_int), ("use_graph", C.c_int),
+                ("block_qubits", C.c_int)]
 
 
 def _concat(circuits_list):
@@ -386,15 +389,22 @@ def _concat(circuits_list):
     return nq, gates, offs
 
 
-def autotune_batch(circuits_list, stride=8):
+def autotune_batch(circuits_list, stride=8, cache=None):
     """Fastest BatchOpts for these circuits (timed on every stride-th one) and
-    its time per run in ms."""
+    its time per run in ms.  cache: a file that keeps tunings by device and
+    gate pattern (qs_batch_autotune_cached); then returns (opts, ms, hit)."""
     nq, gates, offs = _concat(circuits_list)
     best, ms = BatchOpts(), C.c_double()
-    check(lib().qs_batch_autotune(len(nq), _iptr(nq), gates.ctypes.data,
-                                  offs.ctypes.data_as(C.POINTER(C.c_size_t)), int(stride), C.byref(best),
-                                  C.byref(ms)))
-    return best, ms.value
+    if cache is None:
+        check(lib().qs_batch_autotune(len(nq), _iptr(nq), gates.ctypes.data,
+                                      offs.ctypes.data_as(C.POINTER(C.c_size_t)), int(stride), C.byref(best),
+                                      C.byref(ms)))
+        return best, ms.value
+    hit = C.c_int()
+    check(lib().qs_batch_autotune_cached(len(nq), _iptr(nq), gates.ctypes.data,
+                                         offs.ctypes.data_as(C.POINTER(C.c_size_t)), int(stride),
+                                         str(cache).encode(), C.byref(best), C.byref(ms), C.byref(hit)))
+    return best, ms.value, bool(hit.value)
 
 
 class Batch:

@@ -296,13 +296,47 @@ extern "C" int qs_gate_apply(qs_state *s, const qs_gate *g)
     return qs_launch_prim(s, p);
 }
 
+// qs_lowstage.cu
+int qs_lowstage_bits(int n);
+bool qs_lowstage_fits(const qs_prim &p, int n);
+int qs_lowstage_max_run();
+double qs_lowstage_traffic(const qs_prim &p, int dtype);
+int qs_launch_lowstage(qs_state *s, const std::vector<qs_prim> &run);
+
+// Gate by gate, except that runs of consecutive gates whose target bits lie
+// in the lowest qubits go through shared memory in one pass each
+// (qs_lowstage.cu) when that moves fewer bytes than the gates would one by
+// one: same arithmetic per amplitude, fewer passes over HBM.
 extern "C" int qs_gates_apply(qs_state *s, const qs_gate *g, size_t count)
 {
+    int r = qs_check_state(s);
+    if (r) return r;
+    if (count && !g) return qs_fail(QS_ERR_ARG, "qs_gates_apply: null gate list");
+    std::vector<qs_prim> run;
+    auto flush = [&]() -> int {
+        int rc = QS_OK;
+        double per_gate = 0;
+        for (const qs_prim &p : run) per_gate += qs_lowstage_traffic(p, s->dtype);
+        if (run.size() > 1 && per_gate > 1.0) {
+            rc = qs_launch_lowstage(s, run);
+        } else {
+            for (size_t k = 0; k < run.size() && !rc; ++k) rc = qs_launch_prim(s, run[k]);
+        }
+        run.clear();
+        return rc;
+    };
     for (size_t i = 0; i < count; ++i) {
-        int r = qs_gate_apply(s, &g[i]);
-        if (r) return r;
+        qs_prim p;
+        if ((r = qs_lower_gate(s->n, &g[i], &p))) return r;
+        if (qs_lowstage_fits(p, s->n)) {
+            run.push_back(p);
+            if ((int)run.size() == qs_lowstage_max_run() && (r = flush())) return r;
+        } else {
+            if ((r = flush())) return r;
+            if ((r = qs_launch_prim(s, p))) return r;
+        }
     }
-    return QS_OK;
+    return flush();
 }
 
 extern "C" int qs_pmeasure(qs_state *s, const int *qubits, int m, uint64_t *idx_out, double *p_out, int *count)

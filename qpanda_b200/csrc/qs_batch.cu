@@ -15,6 +15,7 @@
 // Circuits with the same gate pattern (same operations on the same qubits)
 // share one plan structure; only their block matrices are rebuilt.
 #include <algorithm>
+#include <cstdio>
 #include <cstring>
 #include <map>
 #include <string>
@@ -377,6 +378,7 @@ extern "C" int qs_batch_default_opts(qs_batch_opts *o)
     o->low_qubits = 3;
     o->order = QS_BATCH_LONGEST_FIRST;
     o->use_graph = 1;
+    o->block_qubits = 5;
     return QS_OK;
 }
 
@@ -390,8 +392,9 @@ extern "C" int qs_batch_create(int n_circ, const int *n_qubits, const qs_gate *g
     qs_batch_opts o;
     if (opts) o = *opts;
     else qs_batch_default_opts(&o);
-    if (o.max_sub < 1 || o.max_sub > 3 || o.low_qubits < 1 || o.low_qubits > 5)
-        return qs_fail(QS_ERR_ARG, "qs_batch_create: max_sub 1..3, low_qubits 1..5");
+    if (o.max_sub < 1 || o.max_sub > 3 || o.low_qubits < 1 || o.low_qubits > 5 || o.block_qubits < 4 ||
+        o.block_qubits > 5)
+        return qs_fail(QS_ERR_ARG, "qs_batch_create: max_sub 1..3, low_qubits 1..5, block_qubits 4..5");
     for (int c = 0; c < n_circ; ++c) {
         if (n_qubits[c] < 1 || n_qubits[c] > kMaxZZ + 1)
             return qs_fail(QS_ERR_UNSUPPORTED, "qs_batch_create: circuit %d has %d qubits (batched circuits: 1..%d)",
@@ -410,6 +413,7 @@ extern "C" int qs_batch_create(int n_circ, const int *n_qubits, const qs_gate *g
     qs_plan_default_opts(&po);
     po.max_sub = o.max_sub;
     po.low_qubits = o.low_qubits;
+    po.block_qubits = o.block_qubits;
     std::map<std::string, int> proto_of;              // signature -> index in protos
     std::vector<qs_plan *> protos, plans(n_circ, nullptr);
     std::vector<int> proto_id(n_circ);
@@ -663,11 +667,13 @@ extern "C" int qs_batch_autotune(int n_circ, const int *n_qubits, const qs_gate 
     cudaEventCreate(&e1);
     double bt = 1e300;
     int r = QS_OK;
+    for (int bq : {5, 4})
     for (int ms : {1, 2, 3})
         for (int lq : {3, 5})
             for (int order : {QS_BATCH_LONGEST_FIRST, QS_BATCH_INPUT_ORDER}) {
                 qs_batch_opts o;
                 qs_batch_default_opts(&o);
+                o.block_qubits = bq;
                 o.max_sub = ms;
                 o.low_qubits = lq;
                 o.order = order;
@@ -697,5 +703,81 @@ done:
     if (r) return r;
     best->use_graph = 1;
     if (best_ms) *best_ms = bt;
+    return QS_OK;
+}
+
+// ---------------------------------------------------------------- tuning cache
+namespace {
+
+// FNV-1a over the device and the sampled circuits' gate pattern.
+uint64_t tune_key(int n_circ, const int *n_qubits, const qs_gate *gates, const size_t *offsets, int stride,
+                  int dev)
+{
+    uint64_t h = 1469598103934665603ull;
+    auto mix = [&](const void *p, size_t n) {
+        const unsigned char *c = static_cast<const unsigned char *>(p);
+        for (size_t i = 0; i < n; ++i) { h ^= c[i]; h *= 1099511628211ull; }
+    };
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, dev) == cudaSuccess) {
+        mix(prop.name, strlen(prop.name));
+        mix(&prop.multiProcessorCount, sizeof(int));
+    }
+    mix(&stride, sizeof(int));
+    for (int c = 0; c < n_circ; c += stride) {
+        mix(&n_qubits[c], sizeof(int));
+        for (size_t i = offsets[c]; i < offsets[c + 1]; ++i) {
+            const qs_gate &g = gates[i];
+            mix(&g.op, sizeof(int32_t));
+            mix(&g.dagger, sizeof(int32_t));
+            mix(g.q, sizeof(g.q));
+            mix(&g.nctrl, sizeof(int32_t));
+            mix(g.ctrl, sizeof(int32_t) * (size_t)std::max(0, std::min(g.nctrl, QS_MAX_CTRL)));
+        }
+    }
+    return h;
+}
+
+}  // namespace
+
+extern "C" int qs_batch_autotune_cached(int n_circ, const int *n_qubits, const qs_gate *gates,
+                                        const size_t *offsets, int stride, const char *cache_path,
+                                        qs_batch_opts *best, double *best_ms, int *from_cache)
+{
+    if (!best || !cache_path || n_circ < 1 || stride < 1 || !n_qubits || !offsets)
+        return qs_fail(QS_ERR_ARG, "qs_batch_autotune_cached: bad arguments");
+    int dev = 0;
+    QS_CUDA_TRY(cudaGetDevice(&dev));
+    const uint64_t key = tune_key(n_circ, n_qubits, gates, offsets, stride, dev);
+    if (from_cache) *from_cache = 0;
+    if (FILE *f = fopen(cache_path, "r")) {
+        char line[256];
+        while (fgets(line, sizeof(line), f)) {
+            unsigned long long k = 0;
+            int ms, lq, order, bq;
+            double t;
+            if (sscanf(line, "%llx %d %d %d %d %lf", &k, &ms, &lq, &order, &bq, &t) == 6 && k == key) {
+                qs_batch_default_opts(best);
+                best->max_sub = ms;
+                best->low_qubits = lq;
+                best->order = order;
+                best->block_qubits = bq;
+                if (best_ms) *best_ms = t;
+                if (from_cache) *from_cache = 1;
+                fclose(f);
+                return QS_OK;
+            }
+        }
+        fclose(f);
+    }
+    double t = 0;
+    int r = qs_batch_autotune(n_circ, n_qubits, gates, offsets, stride, best, &t);
+    if (r) return r;
+    if (best_ms) *best_ms = t;
+    FILE *f = fopen(cache_path, "a");
+    if (!f) return qs_fail(QS_ERR_IO, "qs_batch_autotune_cached: cannot write %s", cache_path);
+    fprintf(f, "%016llx %d %d %d %d %.6f\n", (unsigned long long)key, best->max_sub, best->low_qubits, best->order,
+            best->block_qubits, t);
+    fclose(f);
     return QS_OK;
 }

@@ -62,21 +62,50 @@ __device__ double na_block_sum(double v)
 }
 
 // CTA b sums |a_i|^2 over the amplitudes of chunk b (2^16 consecutive
-// indices, or the whole state if smaller) whose bit q is 0.
+// indices, or the whole state if smaller) whose bit q is 0, in a fixed order.
+// When bit q lies above the chunk, the chunk is all in or all out (a chunk
+// all out writes 0 at once).  Loads are 16 bytes: two complex64 amplitudes
+// (the pair 2k, 2k+1 shares bit q for q >= 1; for q = 0 the first of each
+// pair counts) when the buffer is 16-byte aligned (vec), else one amplitude.
 template <typename T>
 __global__ void __launch_bounds__(kThreads)
-k_na_chunk_sum(const T *__restrict__ a, uint64_t N, int q, double *partials)
+k_na_chunk_sum(const T *__restrict__ a, uint64_t N, int q, int vec, double *partials)
 {
     typedef typename vec2<T>::type V;
-    const V *pa = reinterpret_cast<const V *>(a);
     const uint64_t chunk = N < (1ull << kChunkBits) ? N : (1ull << kChunkBits);
     const uint64_t base = (uint64_t)blockIdx.x * chunk;
     double acc = 0;
-    for (uint64_t i = threadIdx.x; i < chunk; i += kThreads) {
-        const uint64_t idx = base + i;
-        if ((idx >> q) & 1ull) continue;
-        V x = pa[idx];
-        acc += fma((double)x.x, (double)x.x, (double)x.y * (double)x.y);
+    const bool whole = (1ull << q) >= chunk;             // bit q is constant on the chunk
+    if (!(whole && ((base >> q) & 1ull))) {
+        if (sizeof(T) == 4 && vec) {
+            const float4 *p4 = reinterpret_cast<const float4 *>(a + 2 * base);
+            const uint64_t pairs = chunk >> 1;
+            if (whole || q == 0) {
+#pragma unroll 4
+                for (uint64_t w = threadIdx.x; w < pairs; w += kThreads) {
+                    const float4 x = p4[w];
+                    acc += fma((double)x.x, (double)x.x, (double)x.y * (double)x.y);
+                    if (q) acc += fma((double)x.z, (double)x.z, (double)x.w * (double)x.w);
+                }
+            } else {
+                // pairs with bit q - 1 of the pair index clear
+                const uint64_t lo = (1ull << (q - 1)) - 1;
+#pragma unroll 4
+                for (uint64_t w = threadIdx.x; w < (pairs >> 1); w += kThreads) {
+                    const float4 x = p4[((w & ~lo) << 1) | (w & lo)];
+                    acc += fma((double)x.x, (double)x.x, (double)x.y * (double)x.y);
+                    acc += fma((double)x.z, (double)x.z, (double)x.w * (double)x.w);
+                }
+            }
+        } else {
+            const V *pa = reinterpret_cast<const V *>(a) + base;
+            const uint64_t lo = (1ull << q) - 1, items = whole ? chunk : chunk >> 1;
+#pragma unroll 4
+            for (uint64_t w = threadIdx.x; w < items; w += kThreads) {
+                const V x = pa[whole ? w : (((w & ~lo) << 1) | (w & lo))];
+                acc += fma((double)x.x, (double)x.x, (double)x.y * (double)x.y);
+            }
+        }
     }
     double s = na_block_sum(acc);
     if (threadIdx.x == 0) partials[blockIdx.x] = s;
@@ -123,7 +152,9 @@ k_na_collapse(T *__restrict__ a, uint64_t pairs, int q, const NaResult *res)
     }
 }
 
-// Device address of g_noalloc_scratch, looked up once per device.
+// Device address of g_noalloc_scratch, looked up once per device (the first
+// call on it) and kept: a cudaDeviceReset between calls would leave it stale,
+// and is not supported.
 constexpr int kMaxDevices = 64;
 std::mutex g_na_mutex;
 double *g_na_addr[kMaxDevices] = {nullptr};
@@ -154,7 +185,8 @@ int measure_noalloc_t(void *amp, int n, int q, double u, int *outcome_dev, doubl
     const uint64_t chunks = N >> kChunkBits ? N >> kChunkBits : 1;
     double *partials = scratch;
     NaResult *res = reinterpret_cast<NaResult *>(scratch + kMaxPartials);
-    k_na_chunk_sum<T><<<(unsigned)chunks, kThreads, 0, st>>>(static_cast<const T *>(amp), N, q, partials);
+    const int vec = ((uintptr_t)amp & 15u) == 0;
+    k_na_chunk_sum<T><<<(unsigned)chunks, kThreads, 0, st>>>(static_cast<const T *>(amp), N, q, vec, partials);
     QS_LAUNCH_CHECK("k_na_chunk_sum");
     k_na_decide<<<1, kThreads, 0, st>>>(partials, (int)chunks, res, u, outcome_dev, p0_dev);
     QS_LAUNCH_CHECK("k_na_decide");
@@ -177,6 +209,9 @@ extern "C" int qs_measure_noalloc(void *amp, int n_qubits, int dtype, int q, dou
                        "amplitudes, so states of 1..%d qubits only (use qs_measure for larger ones)",
                        n_qubits, kMaxPartials, kChunkBits, kMaxQubits);
     if (q < 0 || q >= n_qubits) return qs_fail(QS_ERR_ARG, "qs_measure_noalloc: qubit %d out of range", q);
+    const uintptr_t align = dtype == QS_C64 ? 8 : 16;
+    if ((uintptr_t)amp % align)
+        return qs_fail(QS_ERR_ARG, "qs_measure_noalloc: amplitudes must be %u-byte aligned", (unsigned)align);
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     return dtype == QS_C64 ? measure_noalloc_t<float>(amp, n_qubits, q, u, outcome_dev, p0_dev, st)
                            : measure_noalloc_t<double>(amp, n_qubits, q, u, outcome_dev, p0_dev, st);

@@ -132,8 +132,8 @@ __device__ __forceinline__ unsigned long long globaltimer()
     return t;
 }
 
-// Bounded wait on an mbarrier phase: false after kWaitNs.
-__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity)
+// Bounded wait on an mbarrier phase: false after limit_ns (kWaitNs).
+__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity, unsigned long long limit_ns = kWaitNs)
 {
     const unsigned long long t0 = globaltimer();
     while (true) {
@@ -146,7 +146,7 @@ __device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity)
             : "r"(mbar), "r"(parity)
             : "memory");
         if (done) return true;
-        if (globaltimer() - t0 > kWaitNs) return false;
+        if (globaltimer() - t0 > limit_ns) return false;
     }
 }
 

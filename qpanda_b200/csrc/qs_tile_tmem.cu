@@ -344,17 +344,14 @@ __device__ __forceinline__ void issue_ts(uint32_t d_tmem, uint32_t a_tmem, uint3
                  :: "r"(mbar) : "memory");
 }
 
-__device__ __forceinline__ void tmem_st32(uint32_t taddr, const uint32_t (&v)[32])
+__device__ __forceinline__ void tmem_st16(uint32_t taddr, const uint32_t (&v)[16])
 {
     asm volatile(
-        "tcgen05.st.sync.aligned.32x32b.x32.b32 [%0], "
-        "{%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16,"
-        "%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31,%32};"
+        "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], "
+        "{%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16};"
         :: "r"(taddr), "r"(v[0]), "r"(v[1]), "r"(v[2]), "r"(v[3]), "r"(v[4]), "r"(v[5]), "r"(v[6]),
            "r"(v[7]), "r"(v[8]), "r"(v[9]), "r"(v[10]), "r"(v[11]), "r"(v[12]), "r"(v[13]), "r"(v[14]),
-           "r"(v[15]), "r"(v[16]), "r"(v[17]), "r"(v[18]), "r"(v[19]), "r"(v[20]), "r"(v[21]), "r"(v[22]),
-           "r"(v[23]), "r"(v[24]), "r"(v[25]), "r"(v[26]), "r"(v[27]), "r"(v[28]), "r"(v[29]), "r"(v[30]),
-           "r"(v[31])
+           "r"(v[15])
         : "memory");
 }
 
@@ -377,14 +374,17 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float *y)
 
 // Row values (32 complex = 64 floats, y[2j] real, y[2j+1] imaginary) as BF16
 // hi/lo pairs into the thread's TMEM lane: hi at columns a..a+31, lo at
-// a+32..a+63.
+// a+32..a+63, in two halves of 16 columns (fewer values live at once).
 __device__ __forceinline__ void split_store(uint32_t taddr, const float (&y)[64])
 {
-    uint32_t hv[32], lv[32];
 #pragma unroll
-    for (int j = 0; j < 32; ++j) split_pair(y[2 * j], y[2 * j + 1], hv[j], lv[j]);
-    tmem_st32(taddr, hv);
-    tmem_st32(taddr + 32, lv);
+    for (int h = 0; h < 2; ++h) {
+        uint32_t hv[16], lv[16];
+#pragma unroll
+        for (int j = 0; j < 16; ++j) split_pair(y[32 * h + 2 * j], y[32 * h + 2 * j + 1], hv[j], lv[j]);
+        tmem_st16(taddr + 16 * h, hv);
+        tmem_st16(taddr + 32 + 16 * h, lv);
+    }
 }
 
 // Swap register bit R of the row's complex index with the lane bit `lm`

@@ -104,32 +104,53 @@ def half_view(t, L, p, value):
 
 class NcclExchanger:
     """One shard per process: rank r holds rank bits r.  The half exchange of
-    a swap is one torch.distributed send/receive pair with the partner rank
-    (NCCL between GPUs, gloo for CPU tensors)."""
+    a swap is a series of torch.distributed send/receive pairs with the
+    partner rank (NCCL between GPUs, gloo for CPU tensors), chunk by chunk:
+    each chunk of the outgoing half is sent from where it lies while the
+    partner's matching chunk lands in a staging buffer, which is then copied
+    into the chunk just sent.  The staging buffer (at most `chunk_amps`
+    amplitudes) is allocated once and reused by every swap."""
 
-    def __init__(self, group=None):
+    def __init__(self, group=None, chunk_amps=1 << 26):
         import torch.distributed as dist
         self.dist = dist
         self.group = group
         self.rank = dist.get_rank(group)
         self.world = dist.get_world_size(group)
+        self.chunk_amps = int(chunk_amps)
+        self.stage = None
 
     def shards(self):
         return [self.rank]
+
+    def _staging(self, like, amps):
+        import torch
+        if (self.stage is None or self.stage.device != like.device or self.stage.dtype != like.dtype
+                or self.stage.numel() < amps):
+            self.stage = torch.empty(amps, dtype=like.dtype, device=like.device)
+        return self.stage[:amps]
 
     def swap(self, tensors, L, j, p):
         import torch
         (t,) = tensors
         partner = self.rank ^ (1 << j)
         b = (self.rank >> j) & 1
-        out = half_view(t, L, p, 1 - b)
-        send = torch.view_as_real(out.contiguous())      # real pairs: every backend moves them
-        recv = torch.empty_like(send)
-        ops = [self.dist.P2POp(self.dist.isend, send, partner, self.group),
-               self.dist.P2POp(self.dist.irecv, recv, partner, self.group)]
-        for r in self.dist.batch_isend_irecv(ops):
-            r.wait()
-        out.copy_(torch.view_as_complex(recv))
+        out = half_view(t, L, p, 1 - b)                   # (2^(L-1-p), 2^p)
+        rows, cols = out.shape
+        # chunks of whole rows (contiguous runs of 2^p amplitudes), or of one row
+        per = max(1, min(rows, self.chunk_amps // cols)) if cols <= self.chunk_amps else 1
+        width = cols if cols <= self.chunk_amps else self.chunk_amps
+        for r0 in range(0, rows, per):
+            r1 = min(rows, r0 + per)
+            for c0 in range(0, cols, width):
+                blk = out[r0:r1, c0:c0 + width]
+                send = blk if blk.is_contiguous() else blk.contiguous()
+                recv = self._staging(send, send.numel()).view(send.shape)
+                ops = [self.dist.P2POp(self.dist.isend, torch.view_as_real(send), partner, self.group),
+                       self.dist.P2POp(self.dist.irecv, torch.view_as_real(recv), partner, self.group)]
+                for req in self.dist.batch_isend_irecv(ops):
+                    req.wait()
+                blk.copy_(recv)
 
 
 class LocalExchanger:

@@ -86,3 +86,30 @@ def test_batch_autotune_and_limits(need_gpu):
     assert len(b.zz()) == 16
     with pytest.raises(QSError):
         Batch([(25, circuits.vqe_ansatz(25, 1, seed=0))])
+
+
+def test_fusion_width_4_and_tuning_cache(need_gpu, tmp_path):
+    """Blocks of at most 4 qubits (one of the autotuner's fusion widths) give
+    the same <ZZ> as the oracle; the cached autotuner tunes once, then
+    returns the same options from its file without timing."""
+    import ctypes as C
+
+    from qpanda_b200.capi import BatchOpts, check, lib
+    sweep = small_sweep(3, count=10)
+    o = BatchOpts()
+    check(lib().qs_batch_default_opts(C.byref(o)))
+    o.block_qubits = 4
+    b = Batch(sweep, opts=o)
+    b.run()
+    for zz, (q, g) in zip(b.zz(), sweep):
+        ref, _ = oracle_zz(q, g)
+        assert np.abs(zz - ref).max() < TOL, q
+    b.close()
+    cache = tmp_path / "tune.txt"
+    o1, ms1, hit1 = autotune_batch(sweep, stride=2, cache=cache)
+    o2, ms2, hit2 = autotune_batch(sweep, stride=2, cache=cache)
+    assert not hit1 and hit2
+    assert (o1.block_qubits, o1.max_sub, o1.low_qubits, o1.order) == (o2.block_qubits, o2.max_sub, o2.low_qubits,
+                                                                      o2.order)
+    assert o1.block_qubits in (4, 5)
+    assert len(cache.read_text().splitlines()) == 1

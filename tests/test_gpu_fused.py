@@ -210,3 +210,29 @@ def test_tile_in_tmem_matches_shared_memory_kernel(need_gpu, remap):
         out.append(sv)
     mx, _ = out[0].diff(out[1])
     assert mx < 1e-6, mx
+
+
+def test_bounded_wait_expires_and_reports(need_gpu):
+    """The waits of the tensor-core kernels give up after a limit: a kernel
+    that waits on an mbarrier nothing arrives on (qs_watchdog_selftest, 50 ms)
+    returns, qs_plan_status reports it, and the context stays usable - a fused
+    plan runs correctly right after."""
+    import time
+
+    from qpanda_b200 import lib
+    from qpanda_b200.capi import QSError, check
+    n = 14
+    sv = StateVector(n, "c64")
+    t0 = time.perf_counter()
+    check(lib().qs_watchdog_selftest(sv.handle, 50000))
+    with pytest.raises(QSError) as e:
+        check(lib().qs_plan_status(sv.handle))
+    assert "bounded wait" in str(e.value)
+    assert time.perf_counter() - t0 < 5.0
+    g = circuits.random_layers(n, 4, 3, iswap_frac=0.1)
+    p = FusionPlan(n, g)
+    p.apply(sv)
+    p.status(sv)                               # cleared by the next application
+    o = OracleState(n)
+    o.apply(g)
+    assert np.abs(sv.get_state() - o.state()).max() < AMP_TOL

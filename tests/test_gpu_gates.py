@@ -205,3 +205,40 @@ def test_round_trip_28q(need_gpu, dt):
     p0 = sv.probs([0, 1, 2, n - 1])
     assert abs(p0[0] - 1) < (1e-5 if dt == "c64" else 1e-12)
     assert abs(sv.norm2() - 1) < (1e-5 if dt == "c64" else 1e-12)
+
+
+def _one_by_one(sv, gates):
+    import ctypes as C
+
+    from qpanda_b200 import lib
+    from qpanda_b200.capi import check
+    g = np.ascontiguousarray(gates)
+    for i in range(len(g)):
+        check(lib().qs_gate_apply(sv.handle, C.c_void_p(g[i:i + 1].ctypes.data)))
+
+
+@pytest.mark.parametrize("dt", ["c128", "c64"])
+@pytest.mark.parametrize("n", [9, 12, 18])
+def test_staged_low_qubit_runs_match_gate_by_gate(need_gpu, dt, n):
+    """qs_gates_apply runs consecutive gates on the lowest qubits through
+    shared memory in one pass (qs_lowstage.cu): the same state as the gates
+    one by one on the streaming kernels, and the oracle's within the usual
+    bar.  Random layers (rotations on qubits 0.. in order), the QFT (long runs
+    of controlled phases) and every gate kind with control lists."""
+    from tests.golden.make_golden import every_gate_circuit
+    for g in (circuits.random_layers(n, 4, 70 + n, iswap_frac=0.3), circuits.qft(n),
+              every_gate_circuit(n, 5 + n)):
+        init = random_state(n, n)
+        a, b = StateVector(n, dt), StateVector(n, dt)
+        a.set_state(init)
+        b.set_state(init)
+        a.apply(g)
+        _one_by_one(b, g)
+        mx, _ = a.diff(b)
+        assert mx <= (1e-15 if dt == "c128" else 1e-7), mx
+        o = OracleState(n)
+        o.set_state(init)
+        o.apply(g)
+        assert np.abs(a.get_state() - o.state()).max() < TOL[dt]
+        a.close()
+        b.close()

@@ -112,7 +112,7 @@ class OracleShard:
         return torch.from_numpy(self.o.view())
 
 
-def _rank_main(rank, world, port, n, out_dir):
+def _rank_main(rank, world, port, n, out_dir, chunk_amps=1 << 26):
     import datetime
 
     import torch.distributed as dist
@@ -123,8 +123,11 @@ def _rank_main(rank, world, port, n, out_dir):
     L = n - g_bits
     gates = circuits.random_layers(n, 4, 123 + world, iswap_frac=0.3)
     eng = OracleShard(L, rank)
-    s = ShardedState(n, g_bits, [eng], NcclExchanger())
+    x = NcclExchanger(chunk_amps=chunk_amps)
+    s = ShardedState(n, g_bits, [eng], x)
     s.run(gates)
+    if x.stage is not None:                   # one staging buffer, bounded, for every swap
+        assert x.stage.numel() <= chunk_amps
     np.save(os.path.join(out_dir, f"shard{rank}.npy"), eng.o.state())
     if rank == 0:
         np.save(os.path.join(out_dir, "pos.npy"), np.array(s.pos))
@@ -132,15 +135,18 @@ def _rank_main(rank, world, port, n, out_dir):
     dist.destroy_process_group()
 
 
-@pytest.mark.parametrize("world", [2, 4])
-def test_gloo_ranks_exchange_halves(world):
+@pytest.mark.parametrize("world,chunk", [(2, 1 << 26), (4, 1 << 26), (2, 32), (4, 8)])
+def test_gloo_ranks_exchange_halves(world, chunk):
+    """Swaps in one piece, and in many chunks through a small staging buffer
+    (down to pieces of one row of a strided half)."""
     import socket
     n = 10
     with socket.socket() as sk:
         sk.bind(("127.0.0.1", 0))
         port = sk.getsockname()[1]
     with tempfile.TemporaryDirectory() as d:
-        mp.start_processes(_rank_main, args=(world, port, n, d), nprocs=world, join=True, start_method="spawn")
+        mp.start_processes(_rank_main, args=(world, port, n, d, chunk), nprocs=world, join=True,
+                           start_method="spawn")
         shards = [np.load(os.path.join(d, f"shard{r}.npy")) for r in range(world)]
         pos = list(np.load(os.path.join(d, "pos.npy")))
     g_bits = world.bit_length() - 1
