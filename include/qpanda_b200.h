@@ -363,6 +363,38 @@ int qs_batch_autotune_cached(int n_circuits, const int *n_qubits, const qs_gate 
                              int stride, const char *cache_path, qs_batch_opts *best, double *best_ms,
                              int *from_cache);
 
+/* ---- sharded states: 2^g shards of 2^(n-g) amplitudes ------------------- */
+/* For states beyond one GPU (33 qubits and up in complex64).  The top g
+ * physical positions of the amplitude index select the shard; logical qubit
+ * q sits at physical position pos[q] (qs_sharded_positions).  Gates on local
+ * positions run on every shard without communication; a gate on a global
+ * qubit first swaps it with a local position the gate does not use - the two
+ * shards that differ in that rank bit exchange half of their slices.  The
+ * reference has no counterpart (it caps programs at 30 qubits,
+ * QPandaAPI.cpp:87).
+ * A process holds some of the shards (ranks[0..n_ranks), on the current
+ * device): two local shards swap with device copies; a shard whose partner is
+ * elsewhere calls `exchange` for each piece (at most 256 MB) of its half:
+ * send `bytes` of device memory at `send` to shard `partner`, receive as many
+ * from it into `recv` (distinct device buffers of the library), and return 0
+ * once `recv` holds them - e.g. an NCCL send/receive pair on `stream`
+ * followed by a stream synchronization.  Shard 0 starts in |0...0>, the
+ * others at zero. */
+typedef struct qs_sharded qs_sharded;
+typedef int (*qs_exchange_fn)(void *ctx, int shard, int partner, const void *send, void *recv, size_t bytes,
+                              void *stream);
+int qs_sharded_create(int n_qubits, int n_global, int dtype, const int *ranks, int n_ranks,
+                      qs_exchange_fn exchange, void *ctx, qs_sharded **out);
+/* Apply gate records (logical qubits); synchronous at every swap. */
+int qs_sharded_apply(qs_sharded *s, const qs_gate *gates, size_t count);
+/* The local shard with these rank bits (a qs_state of n - g qubits). */
+int qs_sharded_shard(qs_sharded *s, int rank, qs_state **shard);
+/* pos[q] = physical position of logical qubit q (n entries). */
+int qs_sharded_positions(const qs_sharded *s, int *pos);
+/* Swaps so far, and bytes this process's shards sent plus received. */
+int qs_sharded_info(const qs_sharded *s, size_t *swaps, size_t *bytes_moved);
+int qs_sharded_destroy(qs_sharded *s);
+
 /* ---- request loop: continuous batching on one GPU ----------------------- */
 /* Requests (a circuit, plus 1024-style shots or the full probability vector)
  * are submitted at any time; `slots` worker threads with their own streams

@@ -108,6 +108,12 @@ def lib():
         "qs_measure_noalloc": (i, [vp, i, i, i, d, vp, vp, vp]),
         "qs_plan_status": (i, [vp]),
         "qs_watchdog_selftest": (i, [vp, C.c_uint]),
+        "qs_sharded_create": (i, [i, i, i, ip, i, vp, vp, C.POINTER(vp)]),
+        "qs_sharded_apply": (i, [vp, vp, sz]),
+        "qs_sharded_shard": (i, [vp, i, C.POINTER(vp)]),
+        "qs_sharded_positions": (i, [vp, ip]),
+        "qs_sharded_info": (i, [vp, C.POINTER(sz), C.POINTER(sz)]),
+        "qs_sharded_destroy": (i, [vp]),
         "qs_release_spare": (i, [vp]),
         "qs_write_fullstate": (i, [vp, C.c_char_p, i]),
         "qs_format_outcomes": (i, [C.POINTER(C.c_uint64), dp, sz, i, C.c_char_p, sz, C.POINTER(sz)]),

@@ -47,3 +47,100 @@ def test_sharded_runs_continue_from_the_layout(need_gpu):
     assert np.abs(got - o.state()).max() < 1e-12
     for e in engines:
         e.close()
+
+
+# ------------------------------------------------ the C ABI's sharded driver
+def _sharded_reference(n, gates):
+    o = OracleState(n)
+    o.apply(gates)
+    return o.state()
+
+
+def _circuit(n, seed):
+    return np.concatenate([circuits.random_layers(n, 5, seed, iswap_frac=0.3), circuits.qft(n)])
+
+
+@pytest.mark.parametrize("dt,tol", [("c128", 1e-12), ("c64", 1e-5)])
+@pytest.mark.parametrize("n,g_bits", [(14, 1), (15, 2)])
+def test_c_abi_sharded_all_shards_local(need_gpu, n, g_bits, dt, tol):
+    """qs_sharded_* with every shard in this process: the C++ schedule (the
+    same swaps and final layout as qpanda_b200.sharded.schedule) and the
+    device-copy swaps of strided and contiguous halves, against the oracle."""
+    import ctypes as C
+
+    from qpanda_b200 import lib
+    from qpanda_b200.capi import QS_C64, QS_C128, check
+    from qpanda_b200.sharded import schedule
+    gates = _circuit(n, 40 + n)
+    code = QS_C64 if dt == "c64" else QS_C128
+    ranks = np.arange(1 << g_bits, dtype=np.int32)
+    h = C.c_void_p()
+    check(lib().qs_sharded_create(n, g_bits, code, ranks.ctypes.data_as(C.POINTER(C.c_int)), len(ranks), None,
+                                  None, C.byref(h)))
+    g = np.ascontiguousarray(gates)
+    check(lib().qs_sharded_apply(h, g.ctypes.data, len(g)))
+    shards = []
+    for r in ranks:
+        s = C.c_void_p()
+        check(lib().qs_sharded_shard(h, int(r), C.byref(s)))
+        out = np.empty(1 << (n - g_bits), dtype=np.complex128)
+        check(lib().qs_get_state(s, out.ctypes.data, QS_C128))
+        shards.append(out)
+    pos = np.empty(n, dtype=np.int32)
+    check(lib().qs_sharded_positions(h, pos.ctypes.data_as(C.POINTER(C.c_int))))
+    swaps, moved = C.c_size_t(), C.c_size_t()
+    check(lib().qs_sharded_info(h, C.byref(swaps), C.byref(moved)))
+    lib().qs_sharded_destroy(h)
+    steps, pos_py = schedule(n, g_bits, gates)
+    assert list(pos) == list(pos_py)
+    assert swaps.value == sum(1 for st in steps if st[0] == "swap") > 0
+    got = gather_logical(shards, n, g_bits, list(pos))
+    assert np.abs(got - _sharded_reference(n, gates)).max() < tol
+
+
+@pytest.fixture(scope="module")
+def mailbox(tmp_path_factory):
+    import ctypes as C
+    import os
+    import subprocess
+
+    from qpanda_b200 import lib
+    lib()
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    libdir = os.path.join(root, "qpanda_b200", "_lib")
+    out = str(tmp_path_factory.mktemp("mailbox") / "libmailbox.so")
+    cmd = ["/usr/local/cuda/bin/nvcc", "-O2", "-std=c++17", "-shared", "-Xcompiler", "-fPIC",
+           os.path.join(root, "tests", "sharded_emu", "mailbox.cpp"), "-I" + os.path.join(root, "include"),
+           "-L" + libdir, "-lqsb200", "-Xlinker", "-rpath=" + libdir, "-o", out]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    assert r.returncode == 0, r.stdout + r.stderr
+    E = C.CDLL(out)
+    E.mailbox_run.restype = C.c_int
+    E.mailbox_run.argtypes = [C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_size_t, C.c_void_p,
+                              C.POINTER(C.c_int), C.POINTER(C.c_size_t)]
+    return E
+
+
+@pytest.mark.parametrize("dt,tol", [("c128", 1e-12), ("c64", 1e-5)])
+@pytest.mark.parametrize("n,g_bits", [(14, 1), (15, 2)])
+def test_c_abi_sharded_exchange_function(need_gpu, mailbox, n, g_bits, dt, tol):
+    """One qs_sharded per shard, each in its own host thread, swapping halves
+    through the caller's exchange function (here a host mailbox and a device
+    copy; NCCL send/receive in a multi-GPU job): packed halves in 256 MB
+    pieces, the same result as the oracle."""
+    import ctypes as C
+
+    from qpanda_b200.capi import QS_C64, QS_C128
+    gates = np.ascontiguousarray(_circuit(n, 90 + n))
+    code = QS_C64 if dt == "c64" else QS_C128
+    npdt = np.complex64 if dt == "c64" else np.complex128
+    out = np.empty((1 << g_bits) << (n - g_bits), dtype=npdt)
+    pos = np.empty(n, dtype=np.int32)
+    swaps = C.c_size_t()
+    rc = mailbox.mailbox_run(n, g_bits, code, gates.ctypes.data, len(gates), out.ctypes.data,
+                             pos.ctypes.data_as(C.POINTER(C.c_int)), C.byref(swaps))
+    assert rc == 0, rc
+    assert swaps.value > 0
+    shards = np.split(out.astype(np.complex128), 1 << g_bits)
+    got = gather_logical(shards, n, g_bits, list(pos))
+    assert np.abs(got - _sharded_reference(n, gates)).max() < tol
