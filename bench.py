@@ -62,7 +62,7 @@ def parse():
     ap.add_argument("--no-secondary", action="store_true",
                     help="default workload: skip the short runs of the other workloads")
     ap.add_argument("--workload", default="circuit32",
-                    choices=["circuit32", "circuit20", "vqe-sweep", "requests", "qft28", "passes"],
+                    choices=["circuit32", "circuit20", "vqe-sweep", "requests", "qft28", "passes", "kernels"],
                     help="circuit32: the 32-qubit random circuit (default); circuit20: the 20-qubit complex128 "
                          "random circuit on the per-gate path, CPU reference timed directly; vqe-sweep: 4096 "
                          "hardware-efficient-ansatz circuits of 10-22 qubits in one persistent launch; "
@@ -1265,6 +1265,105 @@ def run_qft(args):
         dist.destroy_process_group()
 
 
+# ----------------------------------------------------------------- every kernel
+def run_kernels(args):
+    """Each kernel of the library on one complex64 state of --qubits (28 when
+    left at 32: 2 GiB, far above L2), a few launches each after one untimed
+    one, timed with CUDA events: mean time, algorithmic bytes (reads plus
+    writes the operation needs, per the per-gate byte rule) and GB/s against
+    the HBM peak.  The command the per-kernel ncu captures run."""
+    import ctypes as C
+
+    import torch
+    from qpanda_b200 import Batch, FusionPlan, StateVector, circuits, lib
+    from qpanda_b200.capi import check
+    torch.cuda.set_device(0)
+    n = 28 if args.qubits == N_QUBITS else args.qubits
+    N, S = 1 << n, 8
+    L = lib()
+    stream = torch.cuda.current_stream()
+    peak, peak_kind = peaks()
+    sv = StateVector(n, "c64")
+    h = sv.handle
+    init = circuits.make_gates([("H", (q,)) for q in range(n)] + [("RY", (q,), 0.3 + 0.1 * q) for q in range(n)])
+    sv.apply(init)
+    reps = max(2, args.steps)
+    out = {}
+
+    def timed(name, fn, bytes_per_call, calls=reps):
+        fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(calls):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        t = e0.elapsed_time(e1) / 1e3 / calls
+        out[name] = {"ms": t * 1e3, "algorithmic_bytes": bytes_per_call, "gbs": bytes_per_call / t / 1e9,
+                     "frac": bytes_per_call / t / 1e9 / peak}
+
+    def gate(spec):
+        g = circuits.make_gates(spec)
+        return lambda: check(L.qs_gate_apply(h, C.c_void_p(g.ctypes.data)))
+
+    timed("k_pair: dense 2x2 on qubit 0", gate([("RX", (0,), 0.7)]), 2 * S * N)
+    timed("k_pair: dense 2x2 on qubit 13", gate([("RX", (13,), 0.7)]), 2 * S * N)
+    timed("k_pair: dense 2x2 on qubit 27", gate([("RX", (n - 1,), 0.7)]), 2 * S * N)
+    timed("k_pair: CNOT (2, 20)", gate([("CNOT", (2, 20))]), 2 * S * N // 2)
+    timed("k_pair: SWAP (1, 24)", gate([("SWAP", (1, 24))]), 2 * S * N // 2)
+    timed("k_phase: CR (0, 1)", gate([("CR", (0, 1), 0.4)]), 2 * S * N // 4)
+    timed("k_phase: CR (12, 25)", gate([("CR", (12, 25), 0.4)]), 2 * S * N // 4)
+    m2 = np.eye(4, dtype=np.complex128).reshape(-1).view(np.float64).copy()
+    timed("k_quad: 4x4 on (3, 17)", lambda: check(L.qs_apply_2q(h, 3, 17, m2.ctypes.data_as(C.POINTER(C.c_double)),
+                                                                 0)), 2 * S * N)
+    run = circuits.make_gates([("RY", (q,), 0.2 * q) for q in range(10)])
+    timed("k_lowstage: 10 rotations on qubits 0..9 (one pass)",
+          lambda: check(L.qs_gates_apply(h, C.c_void_p(run.ctypes.data), len(run))), 2 * S * N)
+    qs20 = np.arange(20, dtype=np.int32)
+    dev = torch.empty(1 << 20, dtype=torch.float64, device="cuda")
+    timed("k_marginal_direct: qubits 0..19 (the sampler's first levels)",
+          lambda: check(L.qs_probs_device(h, qs20.ctypes.data_as(C.POINTER(C.c_int)), 20, C.c_void_p(dev.data_ptr()))),
+          S * N + (8 << 20))
+    q3 = np.array([3, 17, n - 2], dtype=np.int32)
+    dev3 = torch.empty(8, dtype=torch.float64, device="cuda")
+    timed("k_marginal: qubits (3, 17, 26)",
+          lambda: check(L.qs_probs_device(h, q3.ctypes.data_as(C.POINTER(C.c_int)), 3, C.c_void_p(dev3.data_ptr()))),
+          S * N)
+    qs = np.arange(n, dtype=np.int32)
+    u = np.random.default_rng(1).uniform(size=(SHOTS, n))
+    timed("qs_sample: marginal + fold + k_shots, 1024 shots of all qubits", lambda: sv.sample(qs, u), S * N, calls=2)
+    timed("qs_prob_zero: k_half_sum + k_finalize (qubit 5)", lambda: sv.prob_zero(5), S * N // 2)
+    timed("qs_measure: k_half_sum + k_finalize + k_collapse (qubit 6)", lambda: sv.measure(6, 0.5),
+          S * N // 2 + S * N + S * N // 2, calls=2)
+    amp = C.c_void_p()
+    check(L.qs_device_ptr(h, C.byref(amp)))
+    ow = torch.zeros(2, dtype=torch.float64, device="cuda")
+    timed("qs_measure_noalloc: k_na_chunk_sum + k_na_decide + k_na_collapse (qubit 7)",
+          lambda: check(L.qs_measure_noalloc(amp, n, 0, 7, 0.5, C.c_void_p(ow.data_ptr()),
+                                             C.c_void_p(ow.data_ptr() + 8), None)),
+          S * N // 2 + S * N + S * N // 2, calls=2)
+    other = StateVector(n, "c64")
+    timed("k_inner: <a|b>", lambda: sv.inner(other), 2 * S * N)
+    g = circuits.random_layers(n, 4, SEED, iswap_frac=0.1)
+    for name, kw in (("k_tile_tmem: tiled pass, tile in tensor memory", {}),
+                     ("k_fused_tile: tiled pass, tile in shared memory", {"tile_in_tmem": 0})):
+        plan = FusionPlan(n, g, **kw)
+        npass = plan.num_launches()
+        timed(name + f" (mean of the {npass} passes of a 4-layer circuit)",
+              lambda: (plan.apply(sv), None)[1], 2 * S * N * npass)
+        out[name + f" (mean of the {npass} passes of a 4-layer circuit)"]["ms"] /= npass
+        plan.close()
+    sweep = circuits.vqe_sweep(512, SWEEP_SEED)
+    b = Batch(sweep)
+    timed("k_batch: 512 circuits of 10-22 qubits", lambda: b.run(), sweep_bytes(sweep))
+    b.close()
+    other.close()
+    sv.close()
+    print(json.dumps({"workload": f"kernels-{n}q-c64", "peak_gbs": peak, "peak_source": peak_kind,
+                      "l2": f"{S * N >> 30} GiB state > L2", "kernels": out}))
+
+
 # ----------------------------------------------------------------- pass profile
 def run_passes(args):
     """The random circuit at --qubits applied once in each tiled layout (in
@@ -1318,6 +1417,8 @@ def main():
         run_passes(args)
     elif args.workload == "circuit20":
         run_circuit20(args)
+    elif args.workload == "kernels":
+        run_kernels(args)
     else:
         run_b200(args)
 
