@@ -54,6 +54,9 @@ def parse():
                     help="tiled passes: qubits 0..low-1 in every tile (contiguous runs of 2^low amplitudes)")
     ap.add_argument("--remap", type=int, default=1, choices=[0, 1],
                     help="tiled passes: 1 = contiguous tile writes through a second state-size buffer")
+    ap.add_argument("--tile-in-tmem", type=int, default=1, choices=[0, 1],
+                    help="tiled passes: 1 = the tile in tensor memory where a pass fits (k_tile_tmem), "
+                         "0 = always in shared memory (k_fused_tile)")
     ap.add_argument("--tpr", type=int, default=1, choices=[1, 2],
                     help="tiled passes: threads per tile row (1: 128 per lane, 2: 256, 16 columns each)")
     ap.add_argument("--qubits", type=int, default=N_QUBITS)
@@ -325,7 +328,8 @@ def timed_steps(L, h, gates, plan, steps, stream, torch, kinds, path):
     ng = len(gates)
     nb = plan.num_launches() if plan is not None else 0
     nl = nb if path == "fused" else ng
-    fused_name = ("k_fused_tile (tiled pass)" if getattr(plan, "kernel", "tiled") == "tiled"
+    fused_name = (("k_tile_tmem (tiled pass, tile in tensor memory)" if getattr(plan, "tile_in_tmem", 0)
+                   else "k_fused_tile (tiled pass)") if getattr(plan, "kernel", "tiled") == "tiled"
                   else "k_fused_tc (5-qubit block)")
     gptr = [gates[i:i + 1].ctypes.data for i in range(ng)]
     whole = path == "fused" and getattr(plan, "remap", False)
@@ -384,8 +388,10 @@ def run_b200(args):
     h = sv.handle
     remap = args.kernel == "tiled" and args.remap == 1
     plan = FusionPlan(n, gates, kernel=args.kernel, remap=remap, low_qubits=args.low, max_sub=args.max_sub,
+                      tile_in_tmem=args.tile_in_tmem,
                       threads_per_row=args.tpr)
     plan.remap = remap
+    plan.tile_in_tmem = args.tile_in_tmem
     nb = plan.num_launches()
     nblocks = plan.num_blocks()
     path = args.path
@@ -459,6 +465,7 @@ def run_b200(args):
         nf = 30
         gf = workload(nf, depth)
         pf = FusionPlan(nf, gf, kernel=args.kernel, remap=remap, low_qubits=args.low, max_sub=args.max_sub,
+                        tile_in_tmem=args.tile_in_tmem,
                         threads_per_row=args.tpr)
         a = StateVector(nf, "c64")
         pf.apply(a)
@@ -502,6 +509,7 @@ def run_b200(args):
             if args.kernel == "tiled":
                 o.max_sub = args.max_sub
                 o.threads_per_row = args.tpr
+                o.tile_in_tmem = args.tile_in_tmem
             check(L.qs_plan_create_ex(n, C.c_void_p(pin_g.data_ptr()), ng, C.byref(o), C.byref(ph)))
             c2 = time.perf_counter()
             check(L.qs_plan_apply(h, ph))
@@ -556,7 +564,7 @@ def run_b200(args):
             "data": "synthetic",
             "config": {"workload": f"random-circuit-{n}q-depth{depth}-c64", "qubits": n, "depth": depth,
                        "gates": ng, "fused_blocks": nblocks, "fused_passes": nb, "kernel": args.kernel,
-                       "remap": remap, "low_qubits": args.low, "max_sub": args.max_sub, "threads_per_row": args.tpr, "device_bytes": (amp_b << n) * (2 if remap and path == "fused" else 1),
+                       "remap": remap, "low_qubits": args.low, "max_sub": args.max_sub, "threads_per_row": args.tpr, "tile_in_tmem": args.tile_in_tmem, "device_bytes": (amp_b << n) * (2 if remap and path == "fused" else 1),
                        "iswap_frac": ISWAP_FRAC, "seed": SEED, "path": path,
                        "state_bytes": amp_b << n, "l2": "inputs larger than L2 (32 GiB state), no flush",
                        "parallelism": f"replicas x{ws}"},
