@@ -12,13 +12,15 @@
 //      (tcgen05.st); barrier; one thread issues the block's 12 MMAs
 //      (kind::f16, A from TMEM, B = the block matrix in shared memory,
 //      D = x_hi R_hi + x_hi R_lo + x_lo R_hi in the other region) and commits
-//      to the group's mbarrier; every thread issues its copies of the next tile
-//      into the staging buffer it has finished reading;
+//      to the group's mbarrier (a one-block pass issues the next tile's
+//      copies now);
 //   3. per block: wait, load the row's 64 results (tcgen05.ld); before the
-//      next block swap the leaving column bits with the entering lane bits by
-//      warp shuffles, split, write them as the next A and issue the next MMAs;
-//      after the last block store the row to HBM (in place, or at the
-//      positions of a remapping pass's StoreMap).
+//      next block write them through the staging buffer (free since the
+//      gather) and read the thread's row of the next block, split, write it as
+//      the next A and issue the next MMAs - after the last exchange every
+//      thread issues its copies of the next tile; after the last block store
+//      the row to HBM (in place, or at the positions of a remapping pass's
+//      StoreMap).
 // The four groups' chains overlap each other on the SM.
 //
 // The previous pass's norm correction (a scalar) is folded into block 0's
@@ -36,17 +38,6 @@ using qs_tmem::TLayout;
 
 // ------------------------------------------------------------------ host layout
 namespace {
-
-// 128-byte lines one warp-wide store of the last block touches, times the
-// stores per thread: lanes whose tile bits are written at positions 1..3
-// (0..3 without column pairs) share lines.
-int tmem_store_cost(uint32_t lanes, const int *WT, bool vec)
-{
-    int k = 0;
-    for (int t = 0; t < 12; ++t)
-        if (((lanes >> t) & 1) && WT[t] <= 3 && (WT[t] >= 1 || !vec)) ++k;
-    return (vec ? 16 : 32) * (32 >> (k > 5 ? 5 : k));
-}
 
 }  // namespace
 
@@ -87,127 +78,121 @@ int qs_tmem_layout_build(int n, const qs_tiled_desc *d, TLayout *L)
             return qs_fail(QS_ERR_ARG, "tiled pass: write positions must be distinct and in range");
         wseen |= 1ull << WT[t];
     }
-    uint32_t uni = 0;
-    for (int b = 0; b < nsub; ++b) uni |= qm[b];
-    const uint32_t cand = ~uni & 0xfffu;
-    if (__builtin_popcount(cand) < 2) return QS_ERR_UNSUPPORTED;
     const int last = nsub - 1;
     int z = -1;                                  // tile bit written at position 0
     for (int t = 0; t < 12; ++t)
         if (WT[t] == 0) z = t;
-    const bool zlast = z >= 0 && ((qm[last] >> z) & 1);
 
-    // warp bits: two tile bits outside every block; the last block's lanes are
-    // the rest of its row bits, so pick the pair that leaves the lanes with the
-    // cheapest stores, then one that keeps tile bit 0 out (a lane there gives
-    // the 8-byte gather its bank bit 0), then the higher write positions
-    int wa = -1, wb = -1;
-    long best = 1L << 40;
-    for (int a = 0; a < 12; ++a)
-        for (int b = a + 1; b < 12; ++b) {
-            if (!((cand >> a) & 1) || !((cand >> b) & 1)) continue;
-            const uint32_t lanes = 0xfffu & ~qm[last] & ~(1u << a) & ~(1u << b);
-            long c = (long)tmem_store_cost(lanes, WT, zlast) * 4096;
-            if (a == 0 || b == 0) c += 2048;
-            c -= WT[a] + WT[b];
-            if (c < best) { best = c; wa = a; wb = b; }
-        }
-    const int W[2] = {wa, wb};
-    const uint32_t wmask = (1u << wa) | (1u << wb);
-
-    // block 0's lanes: tile bit 0 first when it is one, then ascending
-    int lanes0[5], nl = 0;
-    if (!((qm[0] | wmask) & 1u)) lanes0[nl++] = 0;
-    for (int t = 1; t < 12; ++t)
-        if (!(((qm[0] | wmask) >> t) & 1)) lanes0[nl++] = t;
-    if (nl != 5) return qs_fail(QS_ERR_ARG, "tiled pass: row bits");
-
-    // block 0's register order: search the 120 orders of its column bits;
-    // transitions pair leaving and entering bits in order, except that the
-    // bit written at position 0 takes register bit 0 when it enters and
-    // register bit 0 leaves.  Keep the order that gives the last block 16-byte
-    // stores (register bit 0 written at position 0), then 16-byte gathers
-    // (register bit 0 of block 0 = tile bit 0).
-    int cols0[5], nc = 0;
-    for (int t = 0; t < 12; ++t)
-        if ((qm[0] >> t) & 1) cols0[nc++] = t;
-    int best_regs[qs_tmem::kMaxSub][5], best_lanes[qs_tmem::kMaxSub][5];
-    int best_sr[qs_tmem::kMaxSub][5], best_sl[qs_tmem::kMaxSub][5], best_ns[qs_tmem::kMaxSub];
-    int best_score = -1;
-    int perm[5] = {0, 1, 2, 3, 4};
-    do {
-        int regs[qs_tmem::kMaxSub][5], lanes[qs_tmem::kMaxSub][5];
-        int sr[qs_tmem::kMaxSub][5], sl[qs_tmem::kMaxSub][5], ns[qs_tmem::kMaxSub] = {0, 0, 0};
-        for (int p = 0; p < 5; ++p) { regs[0][p] = cols0[perm[p]]; lanes[0][p] = lanes0[p]; }
-        for (int b = 0; b + 1 < nsub; ++b) {
-            int lp[5], ln = 0, ei[5], en = 0;
-            for (int p = 0; p < 5; ++p)
-                if (!((qm[b + 1] >> regs[b][p]) & 1)) lp[ln++] = p;
-            for (int i = 0; i < 5; ++i)
-                if ((qm[b + 1] >> lanes[b][i]) & 1) ei[en++] = i;
-            // z enters now and register 0 leaves: pair them first
-            int zi = -1;
-            for (int k = 0; k < en; ++k)
-                if (lanes[b][ei[k]] == z) zi = k;
-            if (zi > 0 && ln > 0 && lp[0] == 0) std::swap(ei[0], ei[zi]);
-            for (int p = 0; p < 5; ++p) { regs[b + 1][p] = regs[b][p]; lanes[b + 1][p] = lanes[b][p]; }
-            for (int k = 0; k < ln; ++k) {
-                sr[b][k] = lp[k];
-                sl[b][k] = ei[k];
-                regs[b + 1][lp[k]] = lanes[b][ei[k]];
-                lanes[b + 1][ei[k]] = regs[b][lp[k]];
-            }
-            ns[b] = ln;
-        }
-        const int score = (zlast && regs[last][0] == z ? 2 : 0) + (regs[0][0] == 0 ? 1 : 0);
-        if (score > best_score) {
-            best_score = score;
-            memcpy(best_regs, regs, sizeof(regs));
-            memcpy(best_lanes, lanes, sizeof(lanes));
-            memcpy(best_sr, sr, sizeof(sr));
-            memcpy(best_sl, sl, sizeof(sl));
-            memcpy(best_ns, ns, sizeof(ns));
-        }
-    } while (best_score < 3 && std::next_permutation(perm, perm + 5));
-
-    L->nsub = nsub;
-    L->pair_in = best_regs[0][0] == 0;
-    L->vec_out = WT[best_regs[last][0]] == 0;
-    for (int b = 0; b + 1 < nsub; ++b) {
-        L->nswap[b] = (int8_t)best_ns[b];
-        for (int k = 0; k < best_ns[b]; ++k) {
-            L->swap_r[b][k] = (int8_t)best_sr[b][k];
-            L->swap_l[b][k] = (int8_t)best_sl[b][k];
-        }
+    // Each block's tile bits: 5 columns (register bits), 5 lanes, 2 warps.
+    // Warps take the two non-column bits that matter least: for the last
+    // block the highest write positions (its lanes then cover the lowest ones
+    // and its stores coalesce), otherwise the highest tile bits; tile bit 0
+    // stays a lane when it is not a column (an 8-byte gather's bank bit 0).
+    // Lanes: tile bit 0 first, then ascending.  Registers: the bit written at
+    // position 0 first in the last block (16-byte stores), tile bit 0 first in
+    // block 0 (16-byte gathers), then ascending.
+    int regs[qs_tmem::kMaxSub][5], lanes[qs_tmem::kMaxSub][5], warps[qs_tmem::kMaxSub][2];
+    for (int b = 0; b < nsub; ++b) {
+        int nonq[7], nn = 0;
+        for (int t = 0; t < 12; ++t)
+            if (!((qm[b] >> t) & 1)) nonq[nn++] = t;
+        auto rank = [&](int t) { return (t == 0 ? -1000 : 0) + (b == last ? WT[t] : t); };
+        std::stable_sort(nonq, nonq + 7, [&](int x, int y) { return rank(x) < rank(y); });
+        warps[b][0] = nonq[5];
+        warps[b][1] = nonq[6];
+        std::sort(nonq, nonq + 5);                   // ascending, so tile bit 0 (if a lane) comes first
+        for (int i = 0; i < 5; ++i) lanes[b][i] = nonq[i];
+        int cols[5], nc = 0;
+        for (int t = 0; t < 12; ++t)
+            if ((qm[b] >> t) & 1) cols[nc++] = t;
+        int head = -1;
+        if (b == last && z >= 0 && ((qm[b] >> z) & 1)) head = z;
+        else if (b == 0 && (qm[b] & 1u)) head = 0;
+        int k = 0;
+        if (head >= 0) regs[b][k++] = head;
+        for (int c = 0; c < 5; ++c)
+            if (cols[c] != head) regs[b][k++] = cols[c];
     }
+    L->nsub = nsub;
+    L->pair_in = regs[0][0] == 0;
+    L->vec_out = WT[regs[last][0]] == 0;
     for (int b = 0; b < nsub; ++b)
-        for (int p = 0; p < 5; ++p) L->mperm[b][p] = (int8_t)mbit[b][best_regs[b][p]];
+        for (int p = 0; p < 5; ++p) L->mperm[b][p] = (int8_t)mbit[b][regs[b][p]];
 
-    // staging swizzle: the lanes of one shared-memory phase (lane bits 0..2 for
-    // 16-byte gathers, 0..3 for 8-byte ones) must read distinct bank slots
-    // (stage-slot bits 1..3, and bit 0 for 8-byte reads); tile bits >= 4 get
-    // the free ones through f
+    // staging swizzle: the lanes of one shared-memory phase of the gather
+    // (lane bits 0..2 for 16-byte gathers, 0..3 for 8-byte ones) must read
+    // distinct bank slots (stage-slot bits 1..3, and bit 0 for 8-byte reads);
+    // tile bits >= 4 get the free ones through f
     uint16_t fbit[12] = {0};
     {
         const int phase = L->pair_in ? 3 : 4;
         uint32_t used = 0;
         for (int i = 0; i < phase; ++i)
-            if (best_lanes[0][i] <= 3) used |= 1u << best_lanes[0][i];
+            if (lanes[0][i] <= 3) used |= 1u << lanes[0][i];
         for (int i = 0; i < phase; ++i) {
-            const int t = best_lanes[0][i];
+            const int t = lanes[0][i];
             if (t <= 3) continue;
-            for (int s = 1; s <= 3; ++s)
-                if (!((used >> s) & 1)) { used |= 1u << s; fbit[t] = (uint16_t)(1u << s); break; }
+            for (int sb = 1; sb <= 3; ++sb)
+                if (!((used >> sb) & 1)) { used |= 1u << sb; fbit[t] = (uint16_t)(1u << sb); break; }
         }
     }
     auto slot = [&](int t) { return (uint16_t)((1u << t) ^ fbit[t]); };
-    for (int i = 0; i < 5; ++i) L->s_lane[i] = slot(best_lanes[0][i]);
-    for (int v = 0; v < 2; ++v) L->s_warp[v] = slot(W[v]);
+    for (int i = 0; i < 5; ++i) L->s_lane[i] = slot(lanes[0][i]);
+    for (int v = 0; v < 2; ++v) L->s_warp[v] = slot(warps[0][v]);
     for (int j = 0; j < 32; ++j) {
-        uint16_t s = 0;
+        uint16_t sv = 0;
         for (int p = 0; p < 5; ++p)
-            if ((j >> p) & 1) s ^= slot(best_regs[0][p]);
-        L->s_col[j] = s;
+            if ((j >> p) & 1) sv ^= slot(regs[0][p]);
+        L->s_col[j] = sv;
+    }
+
+    // exchange swizzles: slot = index ^ g(index), g linear from tile bits >= 4
+    // into slot bits 0..3, chosen so that the 16 lanes of a half warp hit 16
+    // distinct 8-byte bank slots both when block b writes and when block b + 1
+    // reads (their lane bits 0..3 must have independent bank vectors)
+    for (int b = 0; b + 1 < nsub; ++b) {
+        uint16_t g[12] = {0};
+        const int *wl = lanes[b], *rl = lanes[b + 1];
+        auto bank = [&](int t, const uint16_t *gg) { return (uint32_t)(t < 4 ? (1u << t) : gg[t]); };
+        auto independent = [&](const int *ls, const uint16_t *gg) {
+            for (uint32_t m = 1; m < 16; ++m) {
+                uint32_t x = 0;
+                for (int i = 0; i < 4; ++i)
+                    if ((m >> i) & 1) x ^= bank(ls[i], gg);
+                if (!x) return false;
+            }
+            return true;
+        };
+        int high[8], nh = 0;
+        for (int i = 0; i < 4; ++i) {
+            if (wl[i] >= 4 && std::find(high, high + nh, wl[i]) == high + nh) high[nh++] = wl[i];
+            if (rl[i] >= 4 && std::find(high, high + nh, rl[i]) == high + nh) high[nh++] = rl[i];
+        }
+        uint32_t seed = 0x9e3779b9u;
+        bool ok = false;
+        for (int attempt = 0; attempt < 4096 && !ok; ++attempt) {
+            for (int h = 0; h < nh; ++h) {
+                seed = seed * 1664525u + 1013904223u;
+                g[high[h]] = (uint16_t)(attempt == 0 ? (1u << (h & 3)) : 1u + (seed >> 28) % 15u);
+            }
+            ok = independent(wl, g) && independent(rl, g);
+        }
+        auto xs = [&](int t) { return (uint16_t)((1u << t) ^ g[t]); };
+        for (int i = 0; i < 5; ++i) {
+            L->xw_lane[b][i] = xs(lanes[b][i]);
+            L->xr_lane[b][i] = xs(lanes[b + 1][i]);
+        }
+        for (int v = 0; v < 2; ++v) {
+            L->xw_warp[b][v] = xs(warps[b][v]);
+            L->xr_warp[b][v] = xs(warps[b + 1][v]);
+        }
+        for (int j = 0; j < 32; ++j) {
+            uint16_t w = 0, rr = 0;
+            for (int p = 0; p < 5; ++p)
+                if ((j >> p) & 1) { w ^= xs(regs[b][p]); rr ^= xs(regs[b + 1][p]); }
+            L->xw_col[b][j] = w;
+            L->xr_col[b][j] = rr;
+        }
     }
     for (int b = 0; b < 7; ++b) {
         L->g_bit[b] = 1ull << d->T[b + 1];
@@ -221,12 +206,12 @@ int qs_tmem_layout_build(int n, const qs_tiled_desc *d, TLayout *L)
         L->gk[k] = g;
         L->cf_k[k] = c;
     }
-    for (int i = 0; i < 5; ++i) L->o_lane[i] = 1ull << WT[best_lanes[last][i]];
-    for (int v = 0; v < 2; ++v) L->o_warp[v] = 1ull << WT[W[v]];
+    for (int i = 0; i < 5; ++i) L->o_lane[i] = 1ull << WT[lanes[last][i]];
+    for (int v = 0; v < 2; ++v) L->o_warp[v] = 1ull << WT[warps[last][v]];
     for (int j = 0; j < 32; ++j) {
         uint64_t o = 0;
         for (int p = 0; p < 5; ++p)
-            if ((j >> p) & 1) o |= 1ull << WT[best_regs[last][p]];
+            if ((j >> p) & 1) o |= 1ull << WT[regs[last][p]];
         L->o_col[j] = o;
     }
     return QS_OK;
@@ -387,38 +372,22 @@ __device__ __forceinline__ void split_store(uint32_t taddr, const float (&y)[64]
     }
 }
 
-// Swap register bit R of the row's complex index with the lane bit `lm`
-// (a mask): afterwards the value at (lane bit a, register bit c) is the one
-// that was at (lane bit c, register bit a).
-template <int R>
-__device__ __forceinline__ void swap_bit(float (&y)[64], bool up, int lm)
+// Between two blocks: the thread's 32 results (y[2j], y[2j+1] = register j)
+// to their slots of the staging buffer (xw ^ wcol[j]), a barrier of the group,
+// then its row of the next block from slots xr ^ rcol[j].  8-byte accesses;
+// the swizzle makes each half warp's 16 accesses hit distinct banks.
+__device__ __forceinline__ void exchange_through(float (&y)[64], uint32_t stage, uint32_t xw, uint32_t xr,
+                                                 const uint16_t *wcol, const uint16_t *rcol, int bar_id)
 {
 #pragma unroll
-    for (int j = 0; j < 32; ++j) {
-        if (j & (1 << R)) continue;
-        const int j1 = j | (1 << R);
-        const float s0 = up ? y[2 * j] : y[2 * j1];
-        const float s1 = up ? y[2 * j + 1] : y[2 * j1 + 1];
-        const float r0 = __shfl_xor_sync(0xffffffffu, s0, lm);
-        const float r1 = __shfl_xor_sync(0xffffffffu, s1, lm);
-        if (up) { y[2 * j] = r0; y[2 * j + 1] = r1; }
-        else { y[2 * j1] = r0; y[2 * j1 + 1] = r1; }
-    }
-}
-
-__device__ __forceinline__ void exchange(float (&y)[64], const TLayout &L, int b, int lane)
-{
-    for (int k = 0; k < L.nswap[b]; ++k) {
-        const int lm = 1 << L.swap_l[b][k];
-        const bool up = (lane & lm) != 0;
-        switch (L.swap_r[b][k]) {
-        case 0: swap_bit<0>(y, up, lm); break;
-        case 1: swap_bit<1>(y, up, lm); break;
-        case 2: swap_bit<2>(y, up, lm); break;
-        case 3: swap_bit<3>(y, up, lm); break;
-        default: swap_bit<4>(y, up, lm); break;
-        }
-    }
+    for (int j = 0; j < 32; ++j)
+        asm volatile("st.shared.v2.f32 [%0], {%1, %2};"
+                     :: "r"(stage + ((xw ^ wcol[j]) << 3)), "f"(y[2 * j]), "f"(y[2 * j + 1]) : "memory");
+    group_bar(bar_id);
+#pragma unroll
+    for (int j = 0; j < 32; ++j)
+        asm volatile("ld.shared.v2.f32 {%0, %1}, [%2];"
+                     : "=f"(y[2 * j]), "=f"(y[2 * j + 1]) : "r"(stage + ((xr ^ rcol[j]) << 3)) : "memory");
 }
 
 // The group's copies of a tile: chunk c = 128 k + t (tile indices 2c, 2c+1,
@@ -496,6 +465,19 @@ __global__ void __launch_bounds__(kCtaThreads, 1) k_tile_tmem(const float *amp, 
 #pragma unroll
     for (int v = 0; v < 2; ++v)
         if ((wq >> v) & 1) orow |= L.o_warp[v];
+    uint32_t xw0 = 0, xr0 = 0, xw1 = 0, xr1 = 0;       // the thread's exchange slots, transitions 0 and 1
+#pragma unroll
+    for (int i = 0; i < 5; ++i)
+        if ((lane >> i) & 1) {
+            xw0 ^= L.xw_lane[0][i]; xr0 ^= L.xr_lane[0][i];
+            xw1 ^= L.xw_lane[1][i]; xr1 ^= L.xr_lane[1][i];
+        }
+#pragma unroll
+    for (int v = 0; v < 2; ++v)
+        if ((wq >> v) & 1) {
+            xw0 ^= L.xw_warp[0][v]; xr0 ^= L.xr_warp[0][v];
+            xw1 ^= L.xw_warp[1][v]; xr1 ^= L.xr_warp[1][v];
+        }
     uint64_t g_t = 0;
     uint32_t cs_t = (uint32_t)ltid;
 #pragma unroll
@@ -545,8 +527,8 @@ __global__ void __launch_bounds__(kCtaThreads, 1) k_tile_tmem(const float *amp, 
         asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
         group_bar(bar_id);
         if (ltid == 0) issue_ts(tgrp + 64, tgrp, smem_u32(smem + kOffB), smem_u32(smem + kOffB + kB), mb);
-        // every thread of the group has read the staging buffer: next tile's copies
-        if (tile + stride < P.tiles) copy_tile(amp, tnext, L, stage, g_t, cs_t);
+        // a one-block pass needs the staging buffer no more: the next tile's copies
+        if (L.nsub == 1 && tile + stride < P.tiles) copy_tile(amp, tnext, L, stage, g_t, cs_t);
 
         for (int b = 0; b < L.nsub; ++b) {
             const bool ok = mbar_wait(mb, phase);
@@ -558,14 +540,16 @@ __global__ void __launch_bounds__(kCtaThreads, 1) k_tile_tmem(const float *amp, 
             tmem_ld32(tlane + dreg + 32, y + 32);
             asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
             if (b + 1 < L.nsub) {
-                exchange(y, L, b, lane);
+                exchange_through(y, stage, b ? xw1 : xw0, b ? xr1 : xr0, L.xw_col[b], L.xr_col[b], bar_id);
                 split_store(tlane + dreg, y);                            // the next block's A
                 asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
                 asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-                group_bar(bar_id);
+                group_bar(bar_id);                                       // also: every exchange read is done
                 if (ltid == 0)
                     issue_ts(tgrp + (dreg ^ 64u), tgrp + dreg, smem_u32(smem + kOffB + (2 * (b + 1)) * kB),
                              smem_u32(smem + kOffB + (2 * (b + 1) + 1) * kB), mb);
+                // after the last exchange the staging buffer is free: the next tile's copies
+                if (b + 2 == L.nsub && tile + stride < P.tiles) copy_tile(amp, tnext, L, stage, g_t, cs_t);
             } else {
                 const uint64_t obase = store_base(tile, tbase, P.W) | orow;
                 float t = 0.f;

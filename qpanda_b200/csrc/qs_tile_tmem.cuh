@@ -14,20 +14,23 @@
 //
 // Rows and warps.  Row r's bits 0..4 are a warp's lanes, bits 5..6 the four
 // warps of a 128-thread lane group (warp w may only touch TMEM lanes
-// 32w..32w+31).  The two warp bits are tile qubits outside every block of the
-// pass, so between blocks each warp keeps its own 1024 amplitudes: a block
-// leaves some of its 5 column bits and takes d new ones, and the new ones are
-// lane bits.  The exchange swaps register bit p_k (a leaving column) with
-// lane bit i_k (an entering one) by warp shuffles, k < d.  The next block's
-// columns are then read off the registers: its matrix is this kernel's
-// column order, a bit permutation of the plan's, applied when the CTA loads it.
+// 32w..32w+31).  Each block has its own assignment of the 12 tile bits to its
+// 5 columns (register index bits), 5 lane bits and 2 warp bits: block 0's
+// suits the gather, the last block's the stores.  Between two blocks the
+// group's 4096 amplitudes go through its staging buffer - each thread writes
+// its row's 32 results at their tile positions and reads its row of the next
+// block - with a per-transition XOR swizzle that keeps both the write and the
+// read phases of a half warp on distinct banks.  A block's matrix is this
+// kernel's column order, a bit permutation of the plan's, applied when the
+// CTA loads it.
 //
 // Staging.  Copies land in a 32 KB staging buffer per lane group in tile
 // order, with stage bits 1..3 XOR'd by a linear function f of stage bits
 // >= 4 (swizzle); each thread then gathers its own block-0 row.  f is chosen
 // per pass so that the lanes of one shared-memory phase read distinct banks,
 // and being constant on the 8 consecutive chunks of a quarter warp's copy it
-// keeps the copies conflict-free.
+// keeps the copies conflict-free.  The buffer is free from the gather until
+// the last exchange, after which the next tile's copies are issued into it.
 #pragma once
 
 #include <stdint.h>
@@ -52,10 +55,12 @@ struct TLayout {
     uint64_t gk[16];             // global offset of tile bits 8..11 = k
     uint16_t cf_bit[7];          // stage-chunk XOR of chunk bit b, b < 7
     uint16_t cf_k[16];           // stage-chunk XOR of k
-    // exchange before block b + 1: swap register bit swap_r[b][k] with lane bit swap_l[b][k]
-    int8_t nswap[kMaxSub - 1];
-    int8_t swap_r[kMaxSub - 1][5];
-    int8_t swap_l[kMaxSub - 1][5];
+    // exchange before block b + 1 through the staging buffer: block b's value
+    // of register j of thread (warp w, lane l) is written at slot
+    // xw(w, l) ^ xw_col[b][j]; block b + 1's register j is read from
+    // xr(w, l) ^ xr_col[b][j]; xw / xr are XORs of the lane and warp parts
+    uint16_t xw_lane[kMaxSub - 1][5], xw_warp[kMaxSub - 1][2], xw_col[kMaxSub - 1][32];
+    uint16_t xr_lane[kMaxSub - 1][5], xr_warp[kMaxSub - 1][2], xr_col[kMaxSub - 1][32];
     // matrix of block b: register bit p is matrix index bit mperm[b][p]
     int8_t mperm[kMaxSub][5];
     // stores of the last block: global offsets of its lane bits, warp bits and register index
@@ -83,7 +88,7 @@ __host__ __device__ inline uint32_t tmem_b_offset(uint32_t n, uint32_t k)
 
 struct qs_tiled_desc;
 // Host: the TLayout of a tiled pass for k_tile_tmem.  QS_OK, or
-// QS_ERR_UNSUPPORTED when the pass does not fit this kernel (fewer than two
-// tile qubits outside all of its blocks, or tile bit 0 not at position 0),
-// in which case the caller runs the shared-memory kernel.  n: qubits.
+// QS_ERR_UNSUPPORTED when the pass does not fit this kernel (tile bit 0 not
+// at position 0: its 16-byte copies need adjacent pairs), in which case the
+// caller runs the shared-memory kernel.  n: qubits.
 int qs_tmem_layout_build(int n, const qs_tiled_desc *d, qs_tmem::TLayout *L);

@@ -317,12 +317,14 @@ extern "C" int tile_emu_rebind(const qs_plan *proto, const qs_gate *gates, size_
 //     stage slot  xrow(w, l) ^ s_col[j];
 //   * each block's product with its matrix permuted to the kernel's column
 //     order (tmem_matrix_index over mperm[b]) in FP64;
-//   * the exchanges between blocks as the warp shuffles of swap_bit do them;
+//   * the exchanges between blocks through the staging buffer (every slot
+//     written once, then read once);
 //   * the last block's stores at store_base | o_lane / o_warp | o_col.
 // Every staging slot must be written once and read once per tile, every output
 // amplitude written once per pass.  conflicts[0] counts shared-memory phases
 // of the gather whose lanes share a bank slot, conflicts[1] those of the
-// copies; passes[0] / [1] count the passes the kernel took / left.
+// copies, conflicts[2] those of the exchanges between blocks; passes[0] / [1]
+// count the passes the kernel took / left.
 extern "C" int tmem_emu_apply(const qs_plan *P, int n, double *state, int remap, int *passes, long long *conflicts)
 {
     g_err[0] = 0;
@@ -467,24 +469,63 @@ extern "C" int tmem_emu_apply(const qs_plan *P, int n, double *state, int remap,
                     }
                 y.swap(y2);
                 if (b + 1 < d.nsub) {
-                    for (int s = 0; s < T.nswap[b]; ++s) {
-                        const int R = T.swap_r[b][s], lm = 1 << T.swap_l[b][s];
-                        if (R < 0 || R > 4 || lm > 16 || lm < 1) return fail("swap out of range", b, s);
-                        y2 = y;
-                        for (int w = 0; w < 4; ++w)
-                            for (int l = 0; l < 32; ++l) {
-                                const bool up = (l & lm) != 0;
-                                const int pl = l ^ lm;
-                                for (int j = 0; j < 32; ++j) {
-                                    if (j & (1 << R)) continue;
-                                    const int j1 = j | (1 << R);
-                                    // partner's send: its up ? y[j] : y[j1]
-                                    const bool pup = !up;
-                                    const cd recv = y2[(32 * w + pl) * 32 + (pup ? j : j1)];
-                                    if (up) y[(32 * w + l) * 32 + j] = recv;
-                                    else y[(32 * w + l) * 32 + j1] = recv;
-                                }
+                    // through the staging buffer: every slot written once, read once
+                    std::vector<cd> ex(4096);
+                    std::vector<int> ew(4096, 0), er(4096, 0);
+                    for (int w = 0; w < 4; ++w)
+                        for (int l = 0; l < 32; ++l) {
+                            uint32_t xw = 0, xr = 0;
+                            for (int i = 0; i < 5; ++i)
+                                if ((l >> i) & 1) { xw ^= T.xw_lane[b][i]; xr ^= T.xr_lane[b][i]; }
+                            for (int v = 0; v < 2; ++v)
+                                if ((w >> v) & 1) { xw ^= T.xw_warp[b][v]; xr ^= T.xr_warp[b][v]; }
+                            for (int j = 0; j < 32; ++j) {
+                                const uint32_t sl = xw ^ T.xw_col[b][j];
+                                if (sl >= 4096) return fail("exchange write slot out of range", l, j);
+                                ex[sl] = y[(32 * w + l) * 32 + j];
+                                ew[sl]++;
                             }
+                        }
+                    for (int o = 0; o < 4096; ++o)
+                        if (ew[o] != 1) return fail("exchange slot not written exactly once", (long long)t, o);
+                    for (int w = 0; w < 4; ++w)
+                        for (int l = 0; l < 32; ++l) {
+                            uint32_t xr = 0;
+                            for (int i = 0; i < 5; ++i)
+                                if ((l >> i) & 1) xr ^= T.xr_lane[b][i];
+                            for (int v = 0; v < 2; ++v)
+                                if ((w >> v) & 1) xr ^= T.xr_warp[b][v];
+                            for (int j = 0; j < 32; ++j) {
+                                const uint32_t sl = xr ^ T.xr_col[b][j];
+                                if (sl >= 4096) return fail("exchange read slot out of range", l, j);
+                                y2[(32 * w + l) * 32 + j] = ex[sl];
+                                er[sl]++;
+                            }
+                        }
+                    for (int o = 0; o < 4096; ++o)
+                        if (er[o] != 1) return fail("exchange slot not read exactly once", (long long)t, o);
+                    y.swap(y2);
+                    if (t == 0) {
+                        // half warps of both phases: 16 distinct 8-byte bank slots
+                        for (int ph = 0; ph < 2; ++ph)
+                            for (int w = 0; w < 4; ++w)
+                                for (int j = 0; j < 32; ++j)
+                                    for (int h = 0; h < 2; ++h) {
+                                        unsigned seen = 0;
+                                        bool clash = false;
+                                        for (int l = 16 * h; l < 16 * h + 16; ++l) {
+                                            uint32_t x = 0;
+                                            for (int i = 0; i < 5; ++i)
+                                                if ((l >> i) & 1) x ^= ph ? T.xr_lane[b][i] : T.xw_lane[b][i];
+                                            for (int v = 0; v < 2; ++v)
+                                                if ((w >> v) & 1) x ^= ph ? T.xr_warp[b][v] : T.xw_warp[b][v];
+                                            const uint32_t sl = x ^ (ph ? T.xr_col[b][j] : T.xw_col[b][j]);
+                                            const unsigned bit = 1u << (sl & 15);
+                                            if (seen & bit) clash = true;
+                                            seen |= bit;
+                                        }
+                                        if (clash) conflicts[2]++;
+                                    }
                     }
                 } else {
                     const uint64_t ob = emu_store_base(t, tbase, W);
