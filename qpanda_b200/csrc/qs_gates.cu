@@ -129,6 +129,22 @@ k_quad(T *__restrict__ a, uint64_t items, Holes h, uint64_t cmask, uint64_t o0, 
             apply4(v, M);
 #pragma unroll
             for (int j = 0; j < 4; ++j) pa[idx[j]] = V{v[2 * j], v[2 * j + 1]};
+        } else if constexpr (sizeof(T) == 4) {
+            // base has bit 0 clear: each member pair (idx, idx + 1) is one float4
+            float4 *p4 = reinterpret_cast<float4 *>(a);
+            float4 t[4];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) t[j] = p4[idx[j] >> 1];
+            T v0[8], v1[8];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                v0[2 * j] = t[j].x; v0[2 * j + 1] = t[j].y;
+                v1[2 * j] = t[j].z; v1[2 * j + 1] = t[j].w;
+            }
+            apply4(v0, M);
+            apply4(v1, M);
+#pragma unroll
+            for (int j = 0; j < 4; ++j) p4[idx[j] >> 1] = make_float4(v0[2 * j], v0[2 * j + 1], v1[2 * j], v1[2 * j + 1]);
         } else {
             T v0[8], v1[8];
 #pragma unroll
@@ -157,10 +173,17 @@ k_phase(T *__restrict__ a, uint64_t items, Holes h, uint64_t mask, T pr, T pi)
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
     for (uint64_t w = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; w < items; w += stride) {
         uint64_t i = insert_holes(VEC ? (w << 1) : w, h) | mask;
+        if constexpr (VEC && sizeof(T) == 4) {
+            // i has bit 0 clear: amplitudes i, i + 1 are one float4
+            float4 *p4 = reinterpret_cast<float4 *>(a) + (i >> 1);
+            const float4 t = *p4;
+            *p4 = make_float4(t.x * pr - t.y * pi, t.x * pi + t.y * pr, t.z * pr - t.w * pi, t.z * pi + t.w * pr);
+        } else {
 #pragma unroll
-        for (int j = 0; j < (VEC ? 2 : 1); ++j) {
-            V t = pa[i + j];
-            pa[i + j] = V{t.x * pr - t.y * pi, t.x * pi + t.y * pr};
+            for (int j = 0; j < (VEC ? 2 : 1); ++j) {
+                V t = pa[i + j];
+                pa[i + j] = V{t.x * pr - t.y * pi, t.x * pi + t.y * pr};
+            }
         }
     }
 }

@@ -5,41 +5,32 @@
 // qubit K (= 10) mixes amplitudes inside aligned runs of 2^K.  A run of such
 // gates - consecutive in the gate list; their controls and phase masks may
 // include any qubits - is applied in one pass: each CTA loads a 2^K-amplitude
-// tile (16-byte loads), applies every gate of the run to it in shared memory
-// with a barrier between gates, and writes it back.  A gate whose controls or
-// mask bits at or above K are not all set in the tile's base leaves the tile
-// alone.  The per-amplitude arithmetic is k_pair's and k_phase's
-// (qs_gates.cu), so the state after the run is the state after the gates one
-// by one.  Gates on higher targets keep the streaming kernels, whose
-// pair-index remapping handles any stride.
+// tile (16-byte loads) into shared memory and each of its 2^(K-3) threads
+// takes 8 of the tile's amplitudes into registers.  Which 3 tile bits index a
+// thread's registers (its *layout*) is chosen on the host per stretch of the
+// run so that every gate's target bits are register bits when it is applied:
+// the gate then mixes register pairs of one thread, with no shared-memory
+// traffic and no barrier.  Only when the next gate needs other register bits
+// do the amplitudes go back through shared memory (8 stores, a barrier, 8
+// loads per thread).  A gate whose controls or mask bits at or above K are not
+// all set in the tile's base leaves the tile alone; controls and mask bits
+// below K are a per-amplitude predicate.  The per-amplitude arithmetic is
+// k_pair's and k_phase's (qs_gates.cu), so the state after the run is the
+// state after the gates one by one.  Gates on higher targets keep the
+// streaming kernels, whose pair-index remapping handles any stride.
+//
+// The layouts, the shared-memory swizzle (every access phase on distinct
+// banks) and the planner are in qs_lowstage.cuh.
 #include <cstring>
 #include <vector>
 
 #include "qs_common.cuh"
+#include "qs_lowstage.cuh"
 #include "qs_prim.h"
 
 namespace {
 
-constexpr int kLowBits = 10;
-constexpr int kMaxRun = 24;
-constexpr int kThreads = 256;
-
-template <typename T>
-struct LowPrim {
-    uint64_t need;               // bits >= K that every touched amplitude has set
-    uint32_t holes;              // bits < K with a zero inserted when enumerating
-    uint32_t set;                // bits < K set in every touched amplitude
-    uint32_t off0, off1;         // pair members (kind PAIR)
-    uint32_t nholes;
-    uint32_t kind;
-    T m[8];                      // PAIR: 2x2 row-major complex; PHASE: m[0] + i m[1]
-};
-
-template <typename T>
-struct LowRun {
-    int count;
-    LowPrim<T> p[kMaxRun];
-};
+using namespace qs_low;
 
 template <typename T>
 __device__ __forceinline__ void cmul_add2(T &xr, T &xi, T ar, T ai, T br, T bi, const T *r0, const T *r1)
@@ -51,66 +42,124 @@ __device__ __forceinline__ void cmul_add2(T &xr, T &xi, T ar, T ai, T br, T bi, 
     xr = re; xi = im;
 }
 
-// insert a zero at every set bit of `holes` (ascending)
-__device__ __forceinline__ uint32_t spread(uint32_t w, uint32_t holes)
+// the pairs (r | B0, r | B1) over r with no bit of HB: one thread's share of
+// a pair gate whose target bits are register bits
+template <typename T, int HB, int B0, int B1>
+__device__ __forceinline__ void apply_pairs(T (&vr)[8], T (&vi)[8], const T (&m)[8], uint32_t tb,
+                                            const uint32_t (&rb)[kRegBits], uint32_t set)
 {
-    while (holes) {
-        const uint32_t low = (holes & (0u - holes)) - 1;     // bits below the lowest hole
-        w = ((w & ~low) << 1) | (w & low);
-        holes &= holes - 1;
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+        if (r & HB) continue;
+        if (((tb | reg_off(r, rb)) & set) != set) continue;
+        const T ar = vr[r | B0], ai = vi[r | B0], br = vr[r | B1], bi = vi[r | B1];
+        cmul_add2(vr[r | B0], vi[r | B0], ar, ai, br, bi, &m[0], &m[2]);
+        cmul_add2(vr[r | B1], vi[r | B1], ar, ai, br, bi, &m[4], &m[6]);
     }
-    return w;
 }
 
 template <typename T>
-__global__ void __launch_bounds__(kThreads) k_lowstage(T *__restrict__ a, uint64_t tiles, int K, LowRun<T> R)
+__device__ __forceinline__ void apply_phase(T (&vr)[8], T (&vi)[8], T pr, T pi, uint32_t tb,
+                                            const uint32_t (&rb)[kRegBits], uint32_t set)
+{
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+        if (((tb | reg_off(r, rb)) & set) != set) continue;
+        const T x = vr[r], y = vi[r];
+        vr[r] = x * pr - y * pi;
+        vi[r] = x * pi + y * pr;
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kMaxThreads) k_lowstage(T *__restrict__ a, uint64_t tiles, int K, Run<T> R)
 {
     typedef typename vec2<T>::type V;
     extern __shared__ __align__(16) unsigned char lsm[];
     V *tile = reinterpret_cast<V *>(lsm);
     const uint32_t TN = 1u << K;
-    V *pa = reinterpret_cast<V *>(a);
-    for (uint64_t t = blockIdx.x; t < tiles; t += gridDim.x) {
-        const uint64_t base = t << K;
-        // load: 16-byte vectors
+    const int tbits = K - kRegBits;
+    const uint32_t t = threadIdx.x;
+    uint32_t tb = 0, pt = 0, rb[kRegBits], pr[kRegBits];
+    auto set_layout = [&](const Layout &L) {
+        tb = thread_off(L, t, tbits);
+        pt = phys<T>(tb);
+#pragma unroll
+        for (int j = 0; j < kRegBits; ++j) {
+            rb[j] = L.rb[j];
+            pr[j] = phys<T>(rb[j]);
+        }
+    };
+    T vr[8], vi[8];
+    auto read_regs = [&]() {
+#pragma unroll
+        for (int r = 0; r < 8; ++r) {
+            const V x = tile[pt ^ reg_off(r, pr)];
+            vr[r] = x.x;
+            vi[r] = x.y;
+        }
+    };
+    auto write_regs = [&]() {
+#pragma unroll
+        for (int r = 0; r < 8; ++r) tile[pt ^ reg_off(r, pr)] = V{vr[r], vi[r]};
+    };
+    for (uint64_t tl = blockIdx.x; tl < tiles; tl += gridDim.x) {
+        const uint64_t base = tl << K;
+        // HBM -> shared memory, 16-byte chunks
         if constexpr (sizeof(T) == 4) {
-            const float4 *src = reinterpret_cast<const float4 *>(pa + base);
-            float4 *dst = reinterpret_cast<float4 *>(tile);
-            for (uint32_t i = threadIdx.x; i < TN / 2; i += kThreads) dst[i] = src[i];
+            const float4 *src = reinterpret_cast<const float4 *>(a) + (base >> 1);
+            float4 *dst = reinterpret_cast<float4 *>(lsm);
+            for (uint32_t c = t; c < TN / 2; c += blockDim.x) {
+                const float4 v = src[c];
+                const uint32_t p = phys<T>(2 * c);
+                dst[p >> 1] = (p & 1) ? make_float4(v.z, v.w, v.x, v.y) : v;
+            }
         } else {
-            for (uint32_t i = threadIdx.x; i < TN; i += kThreads) tile[i] = pa[base + i];
+            const double2 *src = reinterpret_cast<const double2 *>(a) + base;
+            for (uint32_t c = t; c < TN; c += blockDim.x) tile[phys<T>(c)] = src[c];
         }
         __syncthreads();
+        set_layout(R.L[0]);
+        read_regs();
         for (int g = 0; g < R.count; ++g) {
-            const LowPrim<T> &p = R.p[g];
-            if ((base & p.need) != p.need) continue;          // the same for the whole CTA
-            const uint32_t items = TN >> p.nholes;
-            if (p.kind == QS_PRIM_PAIR) {
-                for (uint32_t w = threadIdx.x; w < items; w += kThreads) {
-                    const uint32_t i = spread(w, p.holes) | p.set;
-                    V x = tile[i | p.off0], y = tile[i | p.off1];
-                    T xr, xi, yr, yi;
-                    cmul_add2(xr, xi, x.x, x.y, y.x, y.y, &p.m[0], &p.m[2]);
-                    cmul_add2(yr, yi, x.x, x.y, y.x, y.y, &p.m[4], &p.m[6]);
-                    tile[i | p.off0] = V{xr, xi};
-                    tile[i | p.off1] = V{yr, yi};
-                }
-            } else {
-                const T pr = p.m[0], pi = p.m[1];
-                for (uint32_t w = threadIdx.x; w < items; w += kThreads) {
-                    const uint32_t i = spread(w, p.holes) | p.set;
-                    const V x = tile[i];
-                    tile[i] = V{x.x * pr - x.y * pi, x.x * pi + x.y * pr};
-                }
+            const Op<T> &op = R.op[g];
+            if (op.layout >= 0) {                         // the same for the whole CTA
+                write_regs();                             // own slots: no barrier needed before
+                __syncthreads();
+                set_layout(R.L[op.layout]);
+                read_regs();
             }
-            __syncthreads();
+            if ((base & op.need) != op.need) continue;    // the same for the whole CTA
+            T m[8];
+#pragma unroll
+            for (int j = 0; j < 8; ++j) m[j] = op.m[j];
+            switch (op.kind) {
+            case OP_PHASE: apply_phase(vr, vi, m[0], m[1], tb, rb, op.set); break;
+            case OP_1Q + 0: apply_pairs<T, 1, 0, 1>(vr, vi, m, tb, rb, op.set); break;
+            case OP_1Q + 1: apply_pairs<T, 2, 0, 2>(vr, vi, m, tb, rb, op.set); break;
+            case OP_1Q + 2: apply_pairs<T, 4, 0, 4>(vr, vi, m, tb, rb, op.set); break;
+            case OP_EX + 0: apply_pairs<T, 3, 1, 2>(vr, vi, m, tb, rb, op.set); break;
+            case OP_EX + 1: apply_pairs<T, 5, 1, 4>(vr, vi, m, tb, rb, op.set); break;
+            case OP_EX + 2: apply_pairs<T, 6, 2, 4>(vr, vi, m, tb, rb, op.set); break;
+            case OP_EX + 3: apply_pairs<T, 3, 2, 1>(vr, vi, m, tb, rb, op.set); break;
+            case OP_EX + 4: apply_pairs<T, 5, 4, 1>(vr, vi, m, tb, rb, op.set); break;
+            default: apply_pairs<T, 6, 4, 2>(vr, vi, m, tb, rb, op.set); break;
+            }
         }
+        write_regs();
+        __syncthreads();
+        // shared memory -> HBM
         if constexpr (sizeof(T) == 4) {
-            float4 *dst = reinterpret_cast<float4 *>(pa + base);
-            const float4 *src = reinterpret_cast<const float4 *>(tile);
-            for (uint32_t i = threadIdx.x; i < TN / 2; i += kThreads) dst[i] = src[i];
+            float4 *dst = reinterpret_cast<float4 *>(a) + (base >> 1);
+            const float4 *src = reinterpret_cast<const float4 *>(lsm);
+            for (uint32_t c = t; c < TN / 2; c += blockDim.x) {
+                const uint32_t p = phys<T>(2 * c);
+                const float4 v = src[p >> 1];
+                dst[c] = (p & 1) ? make_float4(v.z, v.w, v.x, v.y) : v;
+            }
         } else {
-            for (uint32_t i = threadIdx.x; i < TN; i += kThreads) pa[base + i] = tile[i];
+            double2 *dst = reinterpret_cast<double2 *>(a) + base;
+            for (uint32_t c = t; c < TN; c += blockDim.x) dst[c] = tile[phys<T>(c)];
         }
         __syncthreads();
     }
@@ -119,48 +168,29 @@ __global__ void __launch_bounds__(kThreads) k_lowstage(T *__restrict__ a, uint64
 template <typename T>
 int launch_run(qs_state *s, const std::vector<qs_prim> &run, int K)
 {
-    LowRun<T> R;
-    memset(&R, 0, sizeof(R));
-    R.count = (int)run.size();
-    const uint64_t low = (1ull << K) - 1;
-    for (size_t g = 0; g < run.size(); ++g) {
-        const qs_prim &q = run[g];
-        LowPrim<T> &p = R.p[g];
-        p.kind = (uint32_t)q.kind;
-        if (q.kind == QS_PRIM_PAIR) {
-            p.need = q.cmask & ~low;
-            p.holes = (uint32_t)(q.holes & low);             // target/exchange bits and low controls
-            p.set = (uint32_t)(q.cmask & low);
-            p.off0 = (uint32_t)q.off0;
-            p.off1 = (uint32_t)q.off1;
-            for (int j = 0; j < 8; ++j) p.m[j] = (T)q.m[j];
-        } else {
-            p.need = q.holes & ~low;
-            p.holes = (uint32_t)(q.holes & low);
-            p.set = (uint32_t)(q.holes & low);
-            p.m[0] = (T)q.m[0];
-            p.m[1] = (T)q.m[1];
-        }
-        p.nholes = (uint32_t)__builtin_popcount(p.holes);
-    }
+    Run<T> R;
+    plan_run(run, K, &R);
     const uint64_t tiles = s->N >> K;
     const size_t smem = sizeof(typename vec2<T>::type) << K;
-    const unsigned grid = grid_for(tiles, 1, 8);
-    k_lowstage<T><<<grid, kThreads, smem, s->stream>>>(static_cast<T *>(s->amp), tiles, K, R);
+    const unsigned grid = grid_for(tiles, 1, 16);
+    k_lowstage<T><<<grid, 1u << (K - kRegBits), smem, s->stream>>>(static_cast<T *>(s->amp), tiles, K, R);
     QS_LAUNCH_CHECK("k_lowstage");
     return QS_OK;
 }
 
 }  // namespace
 
-// Width of the staged tiles for an n-qubit state.
-int qs_lowstage_bits(int n) { return n < kLowBits ? n : kLowBits; }
+// Width of the staged tiles for an n-qubit state (0: no staging on states
+// this small).
+int qs_lowstage_bits(int n) { return n < kMinLowBits ? 0 : n < kLowBits ? n : kLowBits; }
 
 // Whether primitive p can join a staged run on an n-qubit state: its target
 // bits below the tile width (controls and phase masks may be anywhere).
 bool qs_lowstage_fits(const qs_prim &p, int n)
 {
-    const uint64_t low = (1ull << qs_lowstage_bits(n)) - 1;
+    const int K = qs_lowstage_bits(n);
+    if (!K) return false;
+    const uint64_t low = (1ull << K) - 1;
     if (p.kind == QS_PRIM_PHASE) return true;
     return ((p.holes & ~p.cmask) & ~low) == 0 && (p.off0 & ~low) == 0 && (p.off1 & ~low) == 0;
 }
@@ -192,5 +222,6 @@ int qs_launch_lowstage(qs_state *s, const std::vector<qs_prim> &run)
     if (run.empty()) return QS_OK;
     if ((int)run.size() > kMaxRun) return qs_fail(QS_ERR_ARG, "staged run of %zu gates (at most %d)", run.size(), kMaxRun);
     const int K = qs_lowstage_bits(s->n);
+    if (!K) return qs_fail(QS_ERR_ARG, "staged run on a %d-qubit state (at least %d qubits)", s->n, kMinLowBits);
     return s->dtype == QS_C64 ? launch_run<float>(s, run, K) : launch_run<double>(s, run, K);
 }

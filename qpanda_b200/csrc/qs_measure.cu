@@ -54,31 +54,60 @@ __device__ __forceinline__ double p2(T re, T im)
     return fma(r, r, i * i);
 }
 
-// sum |a_i|^2 over i with bit q == 0 (q < 0: over all i).
+// sum |a_i|^2 over i with bit q == 0 (q < 0: over all i), read in chunks of
+// two neighbouring amplitudes (one 16-byte load for complex64): chunk c holds
+// amplitudes 2c, 2c + 1.  q < 0: every chunk, both halves; q == 0: every
+// chunk, first half; q >= 1: the chunks with bit q - 1 of c clear (the pair
+// index with a zero inserted), both halves.  A thread keeps four chunks in
+// flight; the per-thread order, and so the partials, are fixed by the grid.
+template <typename T>
+struct Chunk2 {
+    T r0, i0, r1, i1;
+};
+
+template <typename T>
+__device__ __forceinline__ Chunk2<T> load_chunk(const T *a, uint64_t c, bool first_only)
+{
+    Chunk2<T> x;
+    if constexpr (sizeof(T) == 4) {
+        const float4 v = reinterpret_cast<const float4 *>(a)[c];
+        x.r0 = v.x; x.i0 = v.y; x.r1 = v.z; x.i1 = v.w;
+    } else {
+        const double2 *p = reinterpret_cast<const double2 *>(a) + 2 * c;
+        const double2 v0 = p[0];
+        x.r0 = v0.x; x.i0 = v0.y;
+        if (first_only) {
+            x.r1 = 0; x.i1 = 0;
+        } else {
+            const double2 v1 = p[1];
+            x.r1 = v1.x; x.i1 = v1.y;
+        }
+    }
+    return x;
+}
+
 template <typename T>
 __global__ void __launch_bounds__(kThreads)
 k_half_sum(const T *__restrict__ a, uint64_t items, int q, double *partials)
 {
-    typedef typename vec2<T>::type V;
-    const V *pa = reinterpret_cast<const V *>(a);
+    const bool first_only = q == 0;
+    const int sh = q > 0 ? q - 1 : 63;
+    const uint64_t lowm = q > 0 ? (1ull << sh) - 1 : ~0ull;
+    auto chunk = [&](uint64_t w) -> uint64_t { return q > 0 ? (((w >> sh) << (sh + 1)) | (w & lowm)) : w; };
+    auto val = [&](const Chunk2<T> &x) -> double {
+        return first_only ? p2(x.r0, x.i0) : p2(x.r0, x.i0) + p2(x.r1, x.i1);
+    };
     double acc = 0;
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-    // items = number of amplitude pairs (i, i+1) with bit q == 0 for q >= 1,
-    // or of single amplitudes for q == 0 / complex128.
-    for (uint64_t w = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; w < items; w += stride) {
-        if (q < 0) {
-            V x = pa[w];
-            acc += p2(x.x, x.y);
-        } else if (q == 0) {
-            V x = pa[w << 1];
-            acc += p2(x.x, x.y);
-        } else {
-            uint64_t lo = w & ((1ull << (q - 1)) - 1);
-            uint64_t i = (((w >> (q - 1)) << q) | lo) << 1;   // pair start, bit q of i is 0
-            V x = pa[i], y = pa[i + 1];
-            acc += p2(x.x, x.y) + p2(y.x, y.y);
-        }
+    uint64_t w = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    for (; w + 3 * stride < items; w += 4 * stride) {
+        Chunk2<T> x[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) x[u] = load_chunk(a, chunk(w + u * stride), first_only);
+#pragma unroll
+        for (int u = 0; u < 4; ++u) acc += val(x[u]);
     }
+    for (; w < items; w += stride) acc += val(load_chunk(a, chunk(w), first_only));
     double s = block_sum(acc);
     if (threadIdx.x == 0) partials[blockIdx.x] = s;
 }
@@ -479,12 +508,9 @@ constexpr size_t kBufOff = kResOff + 256;
 template <typename T>
 int half_sum(qs_state *s, int q, int *nblocks)
 {
-    uint64_t items;
-    if (q < 0) items = s->N;
-    else if (q == 0) items = s->N >> 1;
-    else items = s->N >> 2;
-    if (items == 0) items = 1;                 // n == 1, q == 1 cannot happen (q < n)
-    unsigned grid = grid_for(items, kThreads, 4);
+    // chunks of two amplitudes (k_half_sum); q < n, so q >= 1 implies N >= 4
+    const uint64_t items = q > 0 ? s->N >> 2 : s->N >> 1;
+    unsigned grid = grid_for(items, kThreads, 8);
     double *part = reinterpret_cast<double *>(static_cast<char *>(s->scratch) + kPartOff);
     k_half_sum<T><<<grid, kThreads, 0, s->stream>>>(static_cast<const T *>(s->amp), items, q, part);
     QS_LAUNCH_CHECK("k_half_sum");

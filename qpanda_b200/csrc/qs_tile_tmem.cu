@@ -37,10 +37,6 @@
 using qs_tmem::TLayout;
 
 // ------------------------------------------------------------------ host layout
-namespace {
-
-}  // namespace
-
 int qs_tmem_layout_build(int n, const qs_tiled_desc *d, TLayout *L)
 {
     memset(L, 0, sizeof(*L));
