@@ -57,6 +57,9 @@ def parse():
     ap.add_argument("--tile-in-tmem", type=int, default=1, choices=[0, 1],
                     help="tiled passes: 1 = the tile in tensor memory where a pass fits (k_tile_tmem), "
                          "0 = always in shared memory (k_fused_tile)")
+    ap.add_argument("--tune", type=int, default=1, choices=[0, 1],
+                    help="fused tiled path: 1 = pick tile_in_tmem, max_sub and low by timing the candidates on "
+                         "the state first (qs_plan_autotune, untimed); 0 = use the flags as given")
     ap.add_argument("--tpr", type=int, default=1, choices=[1, 2],
                     help="tiled passes: threads per tile row (1: 128 per lane, 2: 256, 16 columns each)")
     ap.add_argument("--qubits", type=int, default=N_QUBITS)
@@ -387,6 +390,20 @@ def run_b200(args):
     sv = StateVector(n, "c64")
     h = sv.handle
     remap = args.kernel == "tiled" and args.remap == 1
+    tuned = None
+    if args.tune and args.kernel == "tiled" and args.path == "fused" and args.tpr == 1:
+        from qpanda_b200 import autotune_plan
+        best, tms = autotune_plan(sv, gates, remap=remap, reps=1)
+        choice = torch.tensor([best.tile_in_tmem, best.max_sub, best.low_qubits], dtype=torch.int64,
+                              device=f"cuda:{local}")
+        if ws > 1:                                   # every rank runs rank 0's choice
+            import torch.distributed as dist
+            dist.broadcast(choice, 0)
+        args.tile_in_tmem, args.max_sub, args.low = (int(x) for x in choice.tolist())
+        tuned = {"by": "qs_plan_autotune (8 candidates, one timed application each, before warm-up)",
+                 "tile_in_tmem": args.tile_in_tmem, "max_sub": args.max_sub, "low_qubits": args.low,
+                 "tuning_ms_per_application": tms}
+        sv.reset()
     plan = FusionPlan(n, gates, kernel=args.kernel, remap=remap, low_qubits=args.low, max_sub=args.max_sub,
                       tile_in_tmem=args.tile_in_tmem,
                       threads_per_row=args.tpr)
@@ -564,7 +581,9 @@ def run_b200(args):
             "data": "synthetic",
             "config": {"workload": f"random-circuit-{n}q-depth{depth}-c64", "qubits": n, "depth": depth,
                        "gates": ng, "fused_blocks": nblocks, "fused_passes": nb, "kernel": args.kernel,
-                       "remap": remap, "low_qubits": args.low, "max_sub": args.max_sub, "threads_per_row": args.tpr, "tile_in_tmem": args.tile_in_tmem, "device_bytes": (amp_b << n) * (2 if remap and path == "fused" else 1),
+                       "remap": remap, "low_qubits": args.low, "max_sub": args.max_sub,
+                       "threads_per_row": args.tpr, "tile_in_tmem": args.tile_in_tmem, "tuned": tuned,
+                       "device_bytes": (amp_b << n) * (2 if remap and path == "fused" else 1),
                        "iswap_frac": ISWAP_FRAC, "seed": SEED, "path": path,
                        "state_bytes": amp_b << n, "l2": "inputs larger than L2 (32 GiB state), no flush",
                        "parallelism": f"replicas x{ws}"},

@@ -233,8 +233,8 @@ typedef struct qs_plan_opts {
                               (measured 3-4 % slower) */
     int tile_in_tmem;      /* tiled passes: 1 = the tile is the MMAs' A operand in tensor memory and the
                               block matrices the B operand in shared memory (default), for every pass
-                              with two tile qubits outside all of its blocks and position 0 in its tile;
-                              other passes, and 0, keep the tile in shared memory */
+                              with position 0 in its tile; other passes, and 0, keep the tile in
+                              shared memory */
 } qs_plan_opts;
 /* Defaults: 5-qubit blocks, tiled passes of 12 qubits with up to 2 blocks
  * (a pass of 3 blocks saves a pass but runs on a kernel with fewer resident
@@ -244,6 +244,16 @@ typedef struct qs_plan_opts {
 int qs_plan_default_opts(qs_plan_opts *opts);
 int qs_plan_create_ex(int n_qubits, const qs_gate *gates, size_t count, const qs_plan_opts *opts,
                       qs_plan **out);
+/* Pick a circuit's plan options by measurement: plans of `gates` with
+ * tile_in_tmem 0 and 1, max_sub 2 and 3 and low_qubits 2 and 3 (the other
+ * fields from *base, or the defaults when base is NULL) are each applied to
+ * s once untimed and `reps` times timed with CUDA events on the state's
+ * stream; *best gets the options of the fastest and *best_ms (may be NULL)
+ * its mean time per application.  Overwrites the state: reset it after.
+ * States below 12 qubits have no tiled passes: *best = the base options.
+ * No reference counterpart (the reference applies gates one at a time). */
+int qs_plan_autotune(qs_state *s, const qs_gate *gates, size_t count, const qs_plan_opts *base, int reps,
+                     qs_plan_opts *best, double *best_ms);
 /* Kernel launches (passes) the plan makes per application. */
 int qs_plan_launches(const qs_plan *plan, size_t *n_launches);
 int qs_plan_destroy(qs_plan *plan);

@@ -6,5 +6,5 @@ qpanda_b200/host/.  This Python package is a thin ctypes view of the C ABI
 (used by tests and bench.py) plus seeded workload generators.
 """
 from .capi import (GATE_DTYPE, OP, QS_C64, QS_C128, Batch, FusionPlan, QSError, Server,  # noqa: F401
-                   StateVector, autotune_batch, format_outcomes, lib)
+                   StateVector, autotune_batch, autotune_plan, format_outcomes, lib)
 from . import circuits  # noqa: F401

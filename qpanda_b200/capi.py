@@ -97,6 +97,7 @@ def lib():
         "qs_batch_autotune_cached": (i, [i, ip, vp, C.POINTER(sz), i, C.c_char_p, vp, dp, ip]),
         "qs_plan_create_ex": (i, [i, vp, sz, vp, C.POINTER(vp)]),
         "qs_plan_default_opts": (i, [vp]),
+        "qs_plan_autotune": (i, [vp, vp, sz, vp, i, vp, C.POINTER(C.c_double)]),
         "qs_plan_launches": (i, [vp, C.POINTER(sz)]),
         "qs_plan_destroy": (i, [vp]),
         "qs_plan_info": (i, [vp, C.POINTER(sz), C.POINTER(sz)]),
@@ -393,6 +394,20 @@ def _concat(circuits_list):
     gates = np.ascontiguousarray(np.concatenate([np.asarray(g, dtype=GATE_DTYPE) for _, g in circuits_list]),
                                  dtype=GATE_DTYPE)
     return nq, gates, offs
+
+
+def autotune_plan(sv, gates, remap=False, reps=1):
+    """Fastest tiled-plan options for this circuit on this state
+    (qs_plan_autotune: tile in tensor or shared memory, 2 or 3 blocks per
+    pass, 2 or 3 low qubits) and its time per application in ms.  Overwrites
+    the state."""
+    g = np.ascontiguousarray(gates, dtype=GATE_DTYPE)
+    base, best, ms = PlanOpts(), PlanOpts(), C.c_double()
+    check(lib().qs_plan_default_opts(C.byref(base)))
+    base.remap = int(remap)
+    check(lib().qs_plan_autotune(sv.handle, g.ctypes.data, g.size, C.byref(base), int(reps), C.byref(best),
+                                 C.byref(ms)))
+    return best, ms.value
 
 
 def autotune_batch(circuits_list, stride=8, cache=None):

@@ -905,6 +905,58 @@ extern "C" int qs_plan_status(qs_state *s)
     return QS_OK;
 }
 
+extern "C" int qs_plan_autotune(qs_state *s, const qs_gate *gates, size_t count, const qs_plan_opts *base,
+                                int reps, qs_plan_opts *best, double *best_ms)
+{
+    int r = qs_check_state(s);
+    if (r) return r;
+    if (!best) return qs_fail(QS_ERR_ARG, "qs_plan_autotune: null output");
+    if (reps < 1 || reps > 100) return qs_fail(QS_ERR_ARG, "qs_plan_autotune: reps %d outside [1, 100]", reps);
+    qs_plan_opts b0;
+    if (base) b0 = *base;
+    else qs_plan_default_opts(&b0);
+    b0.kernel = QS_PLAN_TILED;
+    *best = b0;
+    if (best_ms) *best_ms = 0;
+    if (s->n < 12) return QS_OK;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    QS_CUDA_TRY(cudaEventCreate(&e0));
+    if (cudaEventCreate(&e1) != cudaSuccess) {
+        cudaEventDestroy(e0);
+        return qs_fail(QS_ERR_CUDA, "qs_plan_autotune: cudaEventCreate failed");
+    }
+    double best_t = -1;
+    for (int tm = 1; tm >= 0 && !r; --tm)
+        for (int ms = 2; ms <= 3 && !r; ++ms)
+            for (int low = 3; low >= 2 && !r; --low) {
+                qs_plan_opts o = b0;
+                o.tile_in_tmem = tm;
+                o.max_sub = ms;
+                o.low_qubits = low;
+                qs_plan *P = nullptr;
+                if ((r = qs_plan_create_ex(s->n, gates, count, &o, &P))) break;
+                r = qs_plan_apply(s, P);
+                if (!r && cudaEventRecord(e0, s->stream) != cudaSuccess) r = qs_fail(QS_ERR_CUDA, "event record");
+                for (int k = 0; k < reps && !r; ++k) r = qs_plan_apply(s, P);
+                if (!r && cudaEventRecord(e1, s->stream) != cudaSuccess) r = qs_fail(QS_ERR_CUDA, "event record");
+                if (!r && cudaEventSynchronize(e1) != cudaSuccess) r = qs_fail(QS_ERR_CUDA, "event sync");
+                if (!r) r = qs_plan_status(s);
+                float ms_t = 0;
+                if (!r && cudaEventElapsedTime(&ms_t, e0, e1) != cudaSuccess) r = qs_fail(QS_ERR_CUDA, "event time");
+                qs_plan_destroy(P);
+                if (r) break;
+                const double t = (double)ms_t / reps;
+                if (best_t < 0 || t < best_t) {
+                    best_t = t;
+                    *best = o;
+                }
+            }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (!r && best_ms) *best_ms = best_t;
+    return r;
+}
+
 void qs_plan_block_bf16(const qs_plan *P, size_t b, uint16_t *out)
 {
     block_bf16(P->blocks[b], out);

@@ -236,3 +236,24 @@ def test_bounded_wait_expires_and_reports(need_gpu):
     o = OracleState(n)
     o.apply(g)
     assert np.abs(sv.get_state() - o.state()).max() < AMP_TOL
+
+
+def test_plan_autotune_picks_a_valid_plan(need_gpu):
+    """qs_plan_autotune times the candidate options on the state and returns
+    the fastest; a plan built with them gives the oracle's state."""
+    from qpanda_b200 import autotune_plan
+    n = 20
+    g = circuits.random_layers(n, 6, 777, iswap_frac=0.1)
+    sv = StateVector(n, "c64")
+    best, ms = autotune_plan(sv, g, remap=True)
+    assert ms > 0
+    assert best.tile_in_tmem in (0, 1) and best.max_sub in (2, 3) and best.low_qubits in (2, 3)
+    assert best.remap == 1 and best.block_qubits == 5
+    sv.reset()
+    p = FusionPlan(n, g, remap=best.remap, max_sub=best.max_sub, low_qubits=best.low_qubits,
+                   tile_in_tmem=best.tile_in_tmem)
+    p.apply(sv)
+    p.status(sv)
+    o = OracleState(n)
+    o.apply(g)
+    assert np.abs(sv.get_state() - o.state()).max() < AMP_TOL
