@@ -17,6 +17,7 @@
 #include <algorithm>
 #include <cstdio>
 #include <cstring>
+#include <functional>
 #include <map>
 #include <string>
 #include <thread>
@@ -416,7 +417,7 @@ extern "C" int qs_batch_create(int n_circ, const int *n_qubits, const qs_gate *g
     po.block_qubits = o.block_qubits;
     std::map<std::string, int> proto_of;              // signature -> index in protos
     std::vector<qs_plan *> protos, plans(n_circ, nullptr);
-    std::vector<int> proto_id(n_circ);
+    std::vector<int> proto_id(n_circ), proto_rep;     // proto_rep: a circuit of each structure
     B->nq.resize(n_circ);
     B->nq_eff.resize(n_circ);
     for (int c = 0; c < n_circ && !r; ++c) {
@@ -428,54 +429,68 @@ extern "C" int qs_batch_create(int n_circ, const int *n_qubits, const qs_gate *g
             if (qs_gate_qubits(&g[i]) >> n_qubits[c])
                 r = qs_fail(QS_ERR_ARG, "qs_batch_create: circuit %d gate %zu uses a qubit >= %d", c, i, n_qubits[c]);
         if (r) break;
-        std::string sig = signature(B->nq_eff[c], g, cnt);
-        auto it = proto_of.find(sig);
-        if (it == proto_of.end()) {
-            qs_plan *pp = nullptr;
-            if ((r = qs_plan_create_ex(B->nq_eff[c], g, cnt, &po, &pp))) break;
-            proto_of[sig] = (int)protos.size();
-            proto_id[c] = (int)protos.size();
-            protos.push_back(pp);
-        } else {
-            proto_id[c] = it->second;
-        }
+        auto ins = proto_of.emplace(signature(B->nq_eff[c], g, cnt), (int)proto_rep.size());
+        if (ins.second) proto_rep.push_back(c);
+        proto_id[c] = ins.first->second;
     }
-    // rebind the block matrices of every circuit (parallel on the host)
-    if (!r) {
-        std::vector<int> rc(n_circ, QS_OK);
-        const int nt = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+    // Host work in parallel: the plan of each structure with its pass layouts,
+    // then every circuit's block matrices rebound onto its structure's plan.
+    const int nt = std::max(1, (int)std::min(16u, std::thread::hardware_concurrency()));
+    auto parallel = [nt](int count, const std::function<void(int)> &f) {
         std::vector<std::thread> th;
-        for (int t = 0; t < nt; ++t)
+        for (int t = 0; t < std::min(nt, count); ++t)
             th.emplace_back([&, t]() {
-                for (int c = t; c < n_circ; c += nt)
-                    rc[c] = qs_plan_rebind(protos[proto_id[c]], gates + offsets[c], offsets[c + 1] - offsets[c],
-                                           &plans[c]);
+                for (int i = t; i < count; i += nt) f(i);
             });
         for (auto &x : th) x.join();
+    };
+    const int input_mode = o.max_sub <= 2 ? 0 : 1;   // tile-order staging, or per-row copies
+    const int np = (int)proto_rep.size();
+    protos.assign(np, nullptr);
+    std::vector<std::vector<Layout>> p_layouts(np);
+    std::vector<std::vector<LoadMap>> p_loads(np);
+    std::vector<int> prc(np, QS_OK);
+    std::vector<std::string> perr(np);
+    if (!r)
+        parallel(np, [&](int pi) {
+            const int c = proto_rep[pi];
+            int rr = qs_plan_create_ex(B->nq_eff[c], gates + offsets[c], offsets[c + 1] - offsets[c], &po, &protos[pi]);
+            const qs_plan *pp = protos[pi];
+            for (size_t u = 0; !rr && u < pp->passes.size(); ++u) {
+                const PlanPass &pass = pp->passes[u];
+                Layout L;
+                LoadMap M;
+                int qpos[3][5];
+                for (size_t b = 0; b < pass.count; ++b)
+                    for (int j = 0; j < 5; ++j) qpos[b][j] = pp->blocks[pass.first + b].q[j];
+                int rows[3][7];
+                if ((rr = qs_tile_row_orders(pp->n, pass.T, (int)pass.count, qpos, rows, nullptr, input_mode))) break;
+                if ((rr = qs_tile_layout_build(pp->n, pass.T, (int)pass.count, qpos, rows, &L, &M))) break;
+                L.pad = (int32_t)pass.first;
+                p_layouts[pi].push_back(L);
+                p_loads[pi].push_back(M);
+            }
+            if (rr) perr[pi] = qs_last_error();
+            prc[pi] = rr;
+        });
+    for (int pi = 0; pi < np && !r; ++pi)
+        if (prc[pi]) r = qs_fail(prc[pi], "qs_batch_create: circuit %d: %s", proto_rep[pi], perr[pi].c_str());
+    if (!r) {
+        std::vector<int> rc(n_circ, QS_OK);
+        parallel(n_circ, [&](int c) {
+            rc[c] = qs_plan_rebind(protos[proto_id[c]], gates + offsets[c], offsets[c + 1] - offsets[c], &plans[c]);
+        });
         for (int c = 0; c < n_circ && !r; ++c)
             if (rc[c]) r = qs_fail(QS_ERR_ARG, "qs_batch_create: rebinding circuit %d failed", c);
     }
     // ---- device memory
     std::vector<Layout> layouts;                      // per proto, concatenated
     std::vector<LoadMap> loads;                       // their tile-order copy maps
-    std::vector<size_t> layout_first(protos.size());
-    const int input_mode = o.max_sub <= 2 ? 0 : 1;   // tile-order staging, or per-row copies
-    for (size_t pi = 0; pi < protos.size() && !r; ++pi) {
+    std::vector<size_t> layout_first(np);
+    for (int pi = 0; pi < np && !r; ++pi) {
         layout_first[pi] = layouts.size();
-        const qs_plan *pp = protos[pi];
-        for (const PlanPass &pass : pp->passes) {
-            Layout L;
-            LoadMap M;
-            int qpos[3][5];
-            for (size_t b = 0; b < pass.count; ++b)
-                for (int j = 0; j < 5; ++j) qpos[b][j] = pp->blocks[pass.first + b].q[j];
-            int rows[3][7];
-            if ((r = qs_tile_row_orders(pp->n, pass.T, (int)pass.count, qpos, rows, nullptr, input_mode))) break;
-            if ((r = qs_tile_layout_build(pp->n, pass.T, (int)pass.count, qpos, rows, &L, &M))) break;
-            L.pad = (int32_t)pass.first;
-            layouts.push_back(L);
-            loads.push_back(M);
-        }
+        layouts.insert(layouts.end(), p_layouts[pi].begin(), p_layouts[pi].end());
+        loads.insert(loads.end(), p_loads[pi].begin(), p_loads[pi].end());
     }
     std::vector<size_t> mat_off(n_circ);
     size_t mat_total = 0;
