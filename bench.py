@@ -400,7 +400,8 @@ def run_b200(args):
             import torch.distributed as dist
             dist.broadcast(choice, 0)
         args.tile_in_tmem, args.max_sub, args.low = (int(x) for x in choice.tolist())
-        tuned = {"by": "qs_plan_autotune (8 candidates, one timed application each, before warm-up)",
+        tuned = {"by": "qs_plan_autotune (12 candidates with remap, 8 without; one timed application each, "
+                       "before warm-up)",
                  "tile_in_tmem": args.tile_in_tmem, "max_sub": args.max_sub, "low_qubits": args.low,
                  "tuning_ms_per_application": tms}
         sv.reset()

@@ -245,8 +245,10 @@ int qs_plan_default_opts(qs_plan_opts *opts);
 int qs_plan_create_ex(int n_qubits, const qs_gate *gates, size_t count, const qs_plan_opts *opts,
                       qs_plan **out);
 /* Pick a circuit's plan options by measurement: plans of `gates` with
- * tile_in_tmem 0 and 1, max_sub 2 and 3 and low_qubits 2 and 3 (the other
- * fields from *base, or the defaults when base is NULL) are each applied to
+ * tile_in_tmem 0 and 1, max_sub 2 and 3 and low_qubits 2 and 3 - and 1 for a
+ * remapping base, whose passes read the qubits they share with the previous
+ * pass as contiguous runs anyway - (the other fields from *base, or the
+ * defaults when base is NULL) are each applied to
  * s once untimed and `reps` times timed with CUDA events on the state's
  * stream; *best gets the options of the fastest and *best_ms (may be NULL)
  * its mean time per application.  Overwrites the state: reset it after.

@@ -399,8 +399,8 @@ def _concat(circuits_list):
 def autotune_plan(sv, gates, remap=False, reps=1):
     """Fastest tiled-plan options for this circuit on this state
     (qs_plan_autotune: tile in tensor or shared memory, 2 or 3 blocks per
-    pass, 2 or 3 low qubits) and its time per application in ms.  Overwrites
-    the state."""
+    pass, 2 or 3 low qubits, or 1 with remap) and its time per application
+    in ms.  Overwrites the state."""
     g = np.ascontiguousarray(gates, dtype=GATE_DTYPE)
     base, best, ms = PlanOpts(), PlanOpts(), C.c_double()
     check(lib().qs_plan_default_opts(C.byref(base)))

@@ -928,7 +928,7 @@ extern "C" int qs_plan_autotune(qs_state *s, const qs_gate *gates, size_t count,
     double best_t = -1;
     for (int tm = 1; tm >= 0 && !r; --tm)
         for (int ms = 2; ms <= 3 && !r; ++ms)
-            for (int low = 3; low >= 2 && !r; --low) {
+            for (int low = 3; low >= (b0.remap ? 1 : 2) && !r; --low) {
                 qs_plan_opts o = b0;
                 o.tile_in_tmem = tm;
                 o.max_sub = ms;
