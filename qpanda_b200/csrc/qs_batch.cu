@@ -507,9 +507,10 @@ extern "C" int qs_batch_create(int n_circ, const int *n_qubits, const qs_gate *g
     std::vector<BatchCirc> hc(n_circ);
     if (!r) {
         std::vector<uint16_t> hm(mat_total);
-        for (int c = 0; c < n_circ; ++c)
+        parallel(n_circ, [&](int c) {
             for (size_t b = 0; b < plans[c]->blocks.size(); ++b)
                 qs_plan_block_bf16(plans[c], b, hm.data() + mat_off[c] + b * 2 * 64 * 64);
+        });
         e = cudaMalloc(&B->d_states, B->state_bytes);
         if (e == cudaSuccess) e = cudaMalloc(&B->d_mats, std::max<size_t>(hm.size() * 2, 16));
         if (e == cudaSuccess) e = cudaMalloc(&B->d_layouts, std::max<size_t>(layouts.size() * sizeof(Layout), 16));
