@@ -43,15 +43,16 @@ __device__ __forceinline__ void cmul_add2(T &xr, T &xi, T ar, T ai, T br, T bi, 
 }
 
 // the pairs (r | B0, r | B1) over r with no bit of HB: one thread's share of
-// a pair gate whose target bits are register bits
-template <typename T, int HB, int B0, int B1>
+// a pair gate whose target bits are register bits; PRED: low control bits
+// (set) to check per pair
+template <typename T, int HB, int B0, int B1, bool PRED>
 __device__ __forceinline__ void apply_pairs(T (&vr)[8], T (&vi)[8], const T (&m)[8], uint32_t tb,
                                             const uint32_t (&rb)[kRegBits], uint32_t set)
 {
 #pragma unroll
     for (int r = 0; r < 8; ++r) {
         if (r & HB) continue;
-        if (((tb | reg_off(r, rb)) & set) != set) continue;
+        if (PRED && ((tb | reg_off(r, rb)) & set) != set) continue;
         const T ar = vr[r | B0], ai = vi[r | B0], br = vr[r | B1], bi = vi[r | B1];
         cmul_add2(vr[r | B0], vi[r | B0], ar, ai, br, bi, &m[0], &m[2]);
         cmul_add2(vr[r | B1], vi[r | B1], ar, ai, br, bi, &m[4], &m[6]);
@@ -80,14 +81,21 @@ __global__ void __launch_bounds__(kMaxThreads) k_lowstage(T *__restrict__ a, uin
     const uint32_t TN = 1u << K;
     const int tbits = K - kRegBits;
     const uint32_t t = threadIdx.x;
+    // per layout, this thread's tile offset and its slot: computed once per CTA
+    uint2 *lt = reinterpret_cast<uint2 *>(lsm + (sizeof(V) << K));
+    for (int l = 0; l < R.nlayouts; ++l) {
+        const uint32_t o = thread_off(R.L[l], t, tbits);
+        lt[l * blockDim.x + t] = make_uint2(o, phys<T>(o));
+    }
     uint32_t tb = 0, pt = 0, rb[kRegBits], pr[kRegBits];
-    auto set_layout = [&](const Layout &L) {
-        tb = thread_off(L, t, tbits);
-        pt = phys<T>(tb);
+    auto set_layout = [&](int l) {
+        const uint2 v = lt[l * blockDim.x + t];
+        tb = v.x;
+        pt = v.y;
 #pragma unroll
         for (int j = 0; j < kRegBits; ++j) {
-            rb[j] = L.rb[j];
-            pr[j] = phys<T>(rb[j]);
+            rb[j] = R.L[l].rb[j];
+            pr[j] = R.L[l].pr[j];
         }
     };
     T vr[8], vi[8];
@@ -119,31 +127,38 @@ __global__ void __launch_bounds__(kMaxThreads) k_lowstage(T *__restrict__ a, uin
             for (uint32_t c = t; c < TN; c += blockDim.x) tile[phys<T>(c)] = src[c];
         }
         __syncthreads();
-        set_layout(R.L[0]);
+        set_layout(0);
         read_regs();
         for (int g = 0; g < R.count; ++g) {
             const Op<T> &op = R.op[g];
             if (op.layout >= 0) {                         // the same for the whole CTA
                 write_regs();                             // own slots: no barrier needed before
                 __syncthreads();
-                set_layout(R.L[op.layout]);
+                set_layout(op.layout);
                 read_regs();
             }
             if ((base & op.need) != op.need) continue;    // the same for the whole CTA
             T m[8];
 #pragma unroll
             for (int j = 0; j < 8; ++j) m[j] = op.m[j];
-            switch (op.kind) {
-            case OP_PHASE: apply_phase(vr, vi, m[0], m[1], tb, rb, op.set); break;
-            case OP_1Q + 0: apply_pairs<T, 1, 0, 1>(vr, vi, m, tb, rb, op.set); break;
-            case OP_1Q + 1: apply_pairs<T, 2, 0, 2>(vr, vi, m, tb, rb, op.set); break;
-            case OP_1Q + 2: apply_pairs<T, 4, 0, 4>(vr, vi, m, tb, rb, op.set); break;
-            case OP_EX + 0: apply_pairs<T, 3, 1, 2>(vr, vi, m, tb, rb, op.set); break;
-            case OP_EX + 1: apply_pairs<T, 5, 1, 4>(vr, vi, m, tb, rb, op.set); break;
-            case OP_EX + 2: apply_pairs<T, 6, 2, 4>(vr, vi, m, tb, rb, op.set); break;
-            case OP_EX + 3: apply_pairs<T, 3, 2, 1>(vr, vi, m, tb, rb, op.set); break;
-            case OP_EX + 4: apply_pairs<T, 5, 4, 1>(vr, vi, m, tb, rb, op.set); break;
-            default: apply_pairs<T, 6, 4, 2>(vr, vi, m, tb, rb, op.set); break;
+            const bool pred = op.set != 0;
+            switch (op.kind + (pred ? 16 : 0)) {
+            case OP_PHASE:
+            case OP_PHASE + 16: apply_phase(vr, vi, m[0], m[1], tb, rb, op.set); break;
+#define QS_LOW_PAIR_CASES(P, OFF)                                                             \
+            case OFF + OP_1Q + 0: apply_pairs<T, 1, 0, 1, P>(vr, vi, m, tb, rb, op.set); break; \
+            case OFF + OP_1Q + 1: apply_pairs<T, 2, 0, 2, P>(vr, vi, m, tb, rb, op.set); break; \
+            case OFF + OP_1Q + 2: apply_pairs<T, 4, 0, 4, P>(vr, vi, m, tb, rb, op.set); break; \
+            case OFF + OP_EX + 0: apply_pairs<T, 3, 1, 2, P>(vr, vi, m, tb, rb, op.set); break; \
+            case OFF + OP_EX + 1: apply_pairs<T, 5, 1, 4, P>(vr, vi, m, tb, rb, op.set); break; \
+            case OFF + OP_EX + 2: apply_pairs<T, 6, 2, 4, P>(vr, vi, m, tb, rb, op.set); break; \
+            case OFF + OP_EX + 3: apply_pairs<T, 3, 2, 1, P>(vr, vi, m, tb, rb, op.set); break; \
+            case OFF + OP_EX + 4: apply_pairs<T, 5, 4, 1, P>(vr, vi, m, tb, rb, op.set); break; \
+            case OFF + OP_EX + 5: apply_pairs<T, 6, 4, 2, P>(vr, vi, m, tb, rb, op.set); break;
+            QS_LOW_PAIR_CASES(false, 0)
+            QS_LOW_PAIR_CASES(true, 16)
+#undef QS_LOW_PAIR_CASES
+            default: break;
             }
         }
         write_regs();
@@ -171,7 +186,8 @@ int launch_run(qs_state *s, const std::vector<qs_prim> &run, int K)
     Run<T> R;
     plan_run(run, K, &R);
     const uint64_t tiles = s->N >> K;
-    const size_t smem = sizeof(typename vec2<T>::type) << K;
+    // the tile, then per layout each thread's (tile offset, slot)
+    const size_t smem = (sizeof(typename vec2<T>::type) << K) + sizeof(uint2) * R.nlayouts * (1u << (K - kRegBits));
     const unsigned grid = grid_for(tiles, 1, 16);
     k_lowstage<T><<<grid, 1u << (K - kRegBits), smem, s->stream>>>(static_cast<T *>(s->amp), tiles, K, R);
     QS_LAUNCH_CHECK("k_lowstage");

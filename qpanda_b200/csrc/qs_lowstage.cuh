@@ -56,6 +56,7 @@ enum : uint8_t { OP_PHASE = 0, OP_1Q = 1, OP_EX = 4 };
 
 struct Layout {
     uint16_t rb[kRegBits];                   // tile offset (a power of two) of register index bit j
+    uint16_t pr[kRegBits];                   // phys(rb[j]): its shared-memory slot offset
     uint16_t tb[kLowBits - kRegBits];        // tile offset of thread index bit k (K - 3 of them used)
 };
 
@@ -124,7 +125,10 @@ inline Layout make_layout(const std::vector<int> &regs, int K)
 {
     Layout L;
     memset(&L, 0, sizeof(L));
-    for (int j = 0; j < kRegBits; ++j) L.rb[j] = (uint16_t)(1u << regs[j]);
+    for (int j = 0; j < kRegBits; ++j) {
+        L.rb[j] = (uint16_t)(1u << regs[j]);
+        L.pr[j] = (uint16_t)phys<T>(L.rb[j]);
+    }
     std::vector<int> rest, order;
     for (int b = 0; b < K; ++b)
         if (b != regs[0] && b != regs[1] && b != regs[2]) rest.push_back(b);

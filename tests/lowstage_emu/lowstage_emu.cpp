@@ -128,7 +128,7 @@ int emulate_run(std::vector<cd> &a, int n, const std::vector<qs_prim> &run, Stat
         }
         for (int j = 0; j < kRegBits; ++j) {
             rb[j] = L.rb[j];
-            pr[j] = phys<T>(rb[j]);
+            pr[j] = L.pr[j];                          // the kernel's slot offsets, from the plan
         }
     };
     auto access = [&](bool write) -> int {
