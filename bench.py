@@ -847,10 +847,12 @@ def secondary_summaries(args, gpu_id):
                 "build_s": ln["config"]["build_s"], "clocks": ln["clocks"]}
 
     def req():
-        ln = requests_line(quiet, 2000, 20, gpu_id=gpu_id, budget_gb=100)
+        ln = requests_line(args, 2000, 20, gpu_id=gpu_id, budget_gb=100)
         return {"workload": "requests", "served": ln["config"]["served"], "failed": ln["failed"],
                 "circuits_per_s": ln["value"], "latency_s": ln["latency_s"], "service_s": ln["service_s"],
                 "subsample": "every 20th of the first 2000 requests of the trace (0.1 of its rate), real time",
+                "cpu_reference_circuits_per_s": (ln.get("cpu_baseline") or {}).get("value"),
+                "cpu_sample": (ln.get("cpu_baseline") or {}).get("sample"),
                 "clocks": ln["clocks"]}
 
     keep("circuit20_c128", c20)
@@ -1084,6 +1086,9 @@ def requests_line(args, n_requests, every, gpu_id=None, rank=0, budget_gb=120):
             nl = FusionPlan(q, circuits.random_layers(q, req["depth"], req["seed"])).num_launches()
             alg_bytes += 2 * 8 * (1 << q) * nl
     peak, peak_kind = peaks()
+    cpu = None
+    if not getattr(args, "no_cpu_baseline", False):
+        cpu = requests_cpu_baseline(sample)
     return {
             "metric": "request loop: circuits/s with p50/p99 latency", "value": n_ok / makespan,
             "unit": "circuits/s", "n_gpus": 1, "steps": 1, "warmup": 2, "ms_per_step": makespan * 1e3,
@@ -1106,8 +1111,40 @@ def requests_line(args, n_requests, every, gpu_id=None, rank=0, budget_gb=120):
             "e2e": {"value": n_ok / makespan, "unit": "circuits/s",
                     "h2d_bytes_per_step": None, "d2h_bytes_per_step": None,
                     "includes": "host circuit generation, submission in real time, shots to the host"},
+            "cpu_baseline": cpu,
             "clocks": clk,
     }
+
+
+def requests_cpu_baseline(sample, max_q=22, max_n=6):
+    """The reference CPU backend (oracle/_ref, -fopenmp, complex128) on the
+    largest served requests of at most max_q qubits (max_n of them, states
+    beyond the host caches), each circuit simulated once; extrapolated to the
+    whole served sample by gate x amplitude work.  A lower bound on the
+    reference's own cost: its shot loop re-simulates the circuit per shot."""
+    from qpanda_b200 import circuits
+    try:
+        from oracle.pyoracle import RefState
+        small = sorted((r for r in sample if r["qubits"] <= max_q), key=lambda r: -r["qubits"])[:max_n]
+        t0 = time.perf_counter()
+        work_s = 0
+        for r in small:
+            g = circuits.random_layers(r["qubits"], r["depth"], r["seed"])
+            st = RefState(r["qubits"], omp=True)
+            st.apply(g)
+            work_s += len(g) << r["qubits"]
+        secs = time.perf_counter() - t0
+        work_all = sum((len(circuits.random_layers(r["qubits"], r["depth"], r["seed"])) << r["qubits"])
+                       for r in sample)
+        return {"value": len(sample) / (secs * work_all / max(work_s, 1)), "unit": "circuits/s",
+                "cores": os.cpu_count(), "kind": "reference",
+                "sample": (f"reference CPUQuantumGates.cpp (-fopenmp, {os.cpu_count()} threads, complex128) on "
+                           f"the {len(small)} largest of the {len(sample)} served requests of <= {max_q} qubits, each "
+                           f"circuit once: {secs:.2f} s, extrapolated by gate x amplitude "
+                           f"work ({work_all / max(work_s, 1):.0f}x; the reference re-simulates per shot, so its "
+                           "shots requests cost more)")}
+    except Exception as ex:
+        return {"value": None, "unit": "circuits/s", "kind": "reference", "sample": f"unavailable: {ex}"}
 
 
 def run_requests(args):

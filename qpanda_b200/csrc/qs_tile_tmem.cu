@@ -368,6 +368,15 @@ __device__ __forceinline__ void split_store(uint32_t taddr, const float (&y)[64]
     }
 }
 
+// Sum of squares of a row in four independent chains (fixed order).
+__device__ __forceinline__ float sum_squares(const float (&y)[64])
+{
+    float t[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+    for (int i = 0; i < 64; ++i) t[i & 3] = fmaf(y[i], y[i], t[i & 3]);
+    return (t[0] + t[1]) + (t[2] + t[3]);
+}
+
 // Between two blocks: the thread's 32 results (y[2j], y[2j+1] = register j)
 // to their slots of the staging buffer (xw ^ wcol[j]), a barrier of the group,
 // then its row of the next block from slots xr ^ rcol[j].  8-byte accesses;
@@ -511,12 +520,7 @@ __global__ void __launch_bounds__(kCtaThreads, 1) k_tile_tmem(const float *amp, 
                     asm volatile("ld.shared.v2.f32 {%0,%1}, [%2];" : "=f"(y[2 * j]), "=f"(y[2 * j + 1]) : "r"(a));
                 }
             }
-            if (want_in) {
-                float ss = 0.f;
-#pragma unroll
-                for (int i = 0; i < 64; ++i) ss = fmaf(y[i], y[i], ss);
-                acc_in += (double)ss;
-            }
+            if (want_in) acc_in += (double)sum_squares(y);
             split_store(tlane, y);
         }
         asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
@@ -548,10 +552,6 @@ __global__ void __launch_bounds__(kCtaThreads, 1) k_tile_tmem(const float *amp, 
                 if (b + 2 == L.nsub && tile + stride < P.tiles) copy_tile(amp, tnext, L, stage, g_t, cs_t);
             } else {
                 const uint64_t obase = store_base(tile, tbase, P.W) | orow;
-                float t = 0.f;
-#pragma unroll
-                for (int i = 0; i < 64; ++i) t = fmaf(y[i], y[i], t);
-                acc_out += (double)t;
                 if (L.vec_out) {
 #pragma unroll
                     for (int j = 0; j < 16; ++j)
@@ -562,6 +562,7 @@ __global__ void __launch_bounds__(kCtaThreads, 1) k_tile_tmem(const float *amp, 
                     for (int j = 0; j < 32; ++j)
                         *reinterpret_cast<float2 *>(out + 2 * (obase | L.o_col[j])) = make_float2(y[2 * j], y[2 * j + 1]);
                 }
+                acc_out += (double)sum_squares(y);                      // after the stores are issued
             }
             asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
         }
