@@ -230,7 +230,8 @@ typedef struct qs_plan_opts {
                               tiles are contiguous (loads stream, stores scatter; measured slower) */
     int threads_per_row;   /* tiled passes: 1 = each of a lane's 128 threads owns a row of the tile (default);
                               2 = 256 threads per lane, two per row, each with 16 of its 32 columns
-                              (measured 3-4 % slower) */
+                              (measured slower on both tiled kernels: 3-4 % with the tile in shared
+                              memory, 20 % with it in tensor memory, where 64 registers a thread spill) */
     int tile_in_tmem;      /* tiled passes: 1 = the tile is the MMAs' A operand in tensor memory and the
                               block matrices the B operand in shared memory (default), for every pass
                               with position 0 in its tile; other passes, and 0, keep the tile in

@@ -856,7 +856,7 @@ extern "C" int qs_plan_apply_range(qs_state *s, qs_plan *P, size_t first, size_t
             d.in_parts = u ? nullptr : norm;
             d.out_parts = norm + GT * (1 + u % 2);
             r = QS_ERR_UNSUPPORTED;
-            if (P->opts.tile_in_tmem && d.threads_per_row == 1) r = qs_launch_tiled_tmem(s, &d, flag);
+            if (P->opts.tile_in_tmem) r = qs_launch_tiled_tmem(s, &d, flag);
             if (r == QS_ERR_UNSUPPORTED) r = qs_launch_tiled(s, &d, flag);
             if (r) return r;
         }

@@ -219,8 +219,14 @@ namespace {
 using namespace qs_tile;
 
 constexpr int kGroups = 4;                       // lane groups (tiles in flight) per CTA
-constexpr int kGroupThreads = 128;
-constexpr int kCtaThreads = kGroups * kGroupThreads;
+// TPR threads per tile row: 128 * TPR threads per group, each with 32 / TPR of
+// its row's 32 columns (TPR = 2: two warps on each quarter of the TMEM lanes).
+template <int TPR>
+struct TShape {
+    static constexpr int kGroupThreads = 128 * TPR;
+    static constexpr int kCtaThreads = kGroups * kGroupThreads;
+    static constexpr int kRegs = 32 / TPR;       // complex columns per thread
+};
 constexpr uint32_t kOffB = 0;                    // 3 blocks x (hi, lo) x 8 KB
 constexpr uint32_t kOffStage = qs_tmem::kMaxSub * 2 * kB;
 constexpr uint32_t kOffMisc = kOffStage + kGroups * kStage;
@@ -246,11 +252,13 @@ struct TParams {
     double *out_parts;
 };
 
+template <int TPR>
 __device__ __forceinline__ void group_bar(int id)
 {
-    asm volatile("bar.sync %0, %1;" :: "r"(id), "r"(kGroupThreads) : "memory");
+    asm volatile("bar.sync %0, %1;" :: "r"(id), "r"(TShape<TPR>::kGroupThreads) : "memory");
 }
 
+template <int TPR>
 __device__ __forceinline__ bool group_bar_or(int id, bool v)
 {
     uint32_t r;
@@ -259,7 +267,7 @@ __device__ __forceinline__ bool group_bar_or(int id, bool v)
         "setp.ne.u32 p, %1, 0;\n\t"
         "bar.red.or.pred q, %2, %3, p;\n\t"
         "selp.u32 %0, 1, 0, q;\n\t}\n"
-        : "=r"(r) : "r"((uint32_t)v), "r"(id), "r"(kGroupThreads) : "memory");
+        : "=r"(r) : "r"((uint32_t)v), "r"(id), "r"(TShape<TPR>::kGroupThreads) : "memory");
     return r != 0;
 }
 
@@ -281,7 +289,7 @@ __device__ __forceinline__ uint64_t tbase_of(uint64_t tile, const TLayout &L)
 __device__ void load_b_perm(uint8_t *dst, const uint16_t *mat, const TLayout &L, float scale)
 {
     const int total = L.nsub * 64 * 32;
-    for (int it = threadIdx.x; it < total; it += kCtaThreads) {
+    for (int it = threadIdx.x; it < total; it += blockDim.x) {
         const int b = it >> 11, np = (it >> 5) & 63, cp = it & 31;
         const uint32_t n = 2 * qs_tmem::tmem_matrix_index((uint32_t)np >> 1, L.mperm[b]) + (np & 1);
         const uint32_t k = 2 * qs_tmem::tmem_matrix_index((uint32_t)cp, L.mperm[b]);
@@ -353,55 +361,63 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float *y)
     for (int i = 0; i < 32; ++i) y[i] = __uint_as_float(r[i]);
 }
 
-// Row values (32 complex = 64 floats, y[2j] real, y[2j+1] imaginary) as BF16
-// hi/lo pairs into the thread's TMEM lane: hi at columns a..a+31, lo at
-// a+32..a+63, in two halves of 16 columns (fewer values live at once).
-__device__ __forceinline__ void split_store(uint32_t taddr, const float (&y)[64])
+// The thread's row values (32 / TPR complex, y[2j] real, y[2j+1] imaginary:
+// its columns c0 .. c0 + 32 / TPR - 1) as BF16 hi/lo pairs into its TMEM
+// lane: hi at columns a + c0.., lo at a + 32 + c0.., 16 columns at a time.
+template <int TPR>
+__device__ __forceinline__ void split_store(uint32_t taddr, const float (&y)[64 / TPR], uint32_t c0)
 {
 #pragma unroll
-    for (int h = 0; h < 2; ++h) {
+    for (int h = 0; h < 2 / TPR; ++h) {
         uint32_t hv[16], lv[16];
 #pragma unroll
         for (int j = 0; j < 16; ++j) split_pair(y[32 * h + 2 * j], y[32 * h + 2 * j + 1], hv[j], lv[j]);
-        tmem_st16(taddr + 16 * h, hv);
-        tmem_st16(taddr + 32 + 16 * h, lv);
+        tmem_st16(taddr + c0 + 16 * h, hv);
+        tmem_st16(taddr + 32 + c0 + 16 * h, lv);
     }
 }
 
-// Sum of squares of a row in four independent chains (fixed order).
-__device__ __forceinline__ float sum_squares(const float (&y)[64])
+// Sum of squares in four independent chains (fixed order).
+template <int NV>
+__device__ __forceinline__ float sum_squares(const float (&y)[NV])
 {
     float t[4] = {0.f, 0.f, 0.f, 0.f};
 #pragma unroll
-    for (int i = 0; i < 64; ++i) t[i & 3] = fmaf(y[i], y[i], t[i & 3]);
+    for (int i = 0; i < NV; ++i) t[i & 3] = fmaf(y[i], y[i], t[i & 3]);
     return (t[0] + t[1]) + (t[2] + t[3]);
 }
 
-// Between two blocks: the thread's 32 results (y[2j], y[2j+1] = register j)
+// Between two blocks: the thread's results (y[2j], y[2j+1] = its register j)
 // to their slots of the staging buffer (xw ^ wcol[j]), a barrier of the group,
-// then its row of the next block from slots xr ^ rcol[j].  8-byte accesses;
-// the swizzle makes each half warp's 16 accesses hit distinct banks.
-__device__ __forceinline__ void exchange_through(float (&y)[64], uint32_t stage, uint32_t xw, uint32_t xr,
+// then its part of the next block's row from slots xr ^ rcol[j].  8-byte
+// accesses; the swizzle makes each half warp's 16 accesses hit distinct
+// banks.  xw / xr include the thread's column base (the tables are linear).
+template <int TPR>
+__device__ __forceinline__ void exchange_through(float (&y)[64 / TPR], uint32_t stage, uint32_t xw, uint32_t xr,
                                                  const uint16_t *wcol, const uint16_t *rcol, int bar_id)
 {
 #pragma unroll
-    for (int j = 0; j < 32; ++j)
+    for (int j = 0; j < 32 / TPR; ++j)
         asm volatile("st.shared.v2.f32 [%0], {%1, %2};"
                      :: "r"(stage + ((xw ^ wcol[j]) << 3)), "f"(y[2 * j]), "f"(y[2 * j + 1]) : "memory");
-    group_bar(bar_id);
+    group_bar<TPR>(bar_id);
 #pragma unroll
-    for (int j = 0; j < 32; ++j)
+    for (int j = 0; j < 32 / TPR; ++j)
         asm volatile("ld.shared.v2.f32 {%0, %1}, [%2];"
                      : "=f"(y[2 * j]), "=f"(y[2 * j + 1]) : "r"(stage + ((xr ^ rcol[j]) << 3)) : "memory");
 }
 
 // The group's copies of a tile: chunk c = 128 k + t (tile indices 2c, 2c+1,
-// adjacent in memory) to stage chunk c ^ cf_t ^ cf_k[k].
+// adjacent in memory) to stage chunk c ^ cf_t ^ cf_k[k]; with TPR = 2 the
+// group's 256 threads take chunks 256 kk + t (k = 2 kk + bit 7 of t, that bit
+// folded into g_t / cs_t by the caller: the tables are linear in k).
+template <int TPR>
 __device__ __forceinline__ void copy_tile(const float *amp, uint64_t base, const TLayout &L, uint32_t stage,
                                           uint64_t g_t, uint32_t cs_t)
 {
 #pragma unroll
-    for (int k = 0; k < 16; ++k) {
+    for (int kk = 0; kk < 16 / TPR; ++kk) {
+        const int k = TPR * kk;
         const float *src = amp + 2 * (base | g_t | L.gk[k]);
         const uint32_t dst = stage + ((cs_t ^ ((uint32_t)k << 7) ^ L.cf_k[k]) << 4);
         asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" :: "r"(dst), "l"(src) : "memory");
@@ -409,11 +425,16 @@ __device__ __forceinline__ void copy_tile(const float *amp, uint64_t base, const
     asm volatile("cp.async.commit_group;" ::: "memory");
 }
 
-__global__ void __launch_bounds__(kCtaThreads, 1) k_tile_tmem(const float *amp, float *out, TParams P)
+template <int TPR>
+__global__ void __launch_bounds__(TShape<TPR>::kCtaThreads, 1) k_tile_tmem(const float *amp, float *out, TParams P)
 {
+    using S = TShape<TPR>;
+    constexpr int kV = 64 / TPR;                     // floats per thread per row
     extern __shared__ __align__(1024) uint8_t smem[];
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int grp = tid >> 7, ltid = tid & 127, wq = ltid >> 5;
+    const int grp = tid / S::kGroupThreads, ltid = tid % S::kGroupThreads, wq = (ltid >> 5) & 3;
+    const int half = TPR == 2 ? ltid >> 7 : 0;       // which 16 of a row's 32 columns (TPR = 2)
+    const int c0 = 16 * half;
     if (smem_u32(smem) & 1023u) {
         if (tid == 0) atomicExch(P.err, 2);
         return;
@@ -483,11 +504,18 @@ __global__ void __launch_bounds__(kCtaThreads, 1) k_tile_tmem(const float *amp, 
             xw0 ^= L.xw_warp[0][v]; xr0 ^= L.xr_warp[0][v];
             xw1 ^= L.xw_warp[1][v]; xr1 ^= L.xr_warp[1][v];
         }
+    if (TPR == 2 && half) {                          // the thread's columns 16.. (every table is linear)
+        xrow ^= L.s_col[16];
+        orow |= L.o_col[16];
+        xw0 ^= L.xw_col[0][16]; xr0 ^= L.xr_col[0][16];
+        xw1 ^= L.xw_col[1][16]; xr1 ^= L.xr_col[1][16];
+    }
     uint64_t g_t = 0;
-    uint32_t cs_t = (uint32_t)ltid;
+    uint32_t cs_t = (uint32_t)ltid;                  // TPR = 2: bit 7 of ltid is bit 0 of k
 #pragma unroll
     for (int b = 0; b < 7; ++b)
         if ((ltid >> b) & 1) { g_t |= L.g_bit[b]; cs_t ^= L.cf_bit[b]; }
+    if (TPR == 2 && (ltid >> 7)) { g_t |= L.gk[1]; cs_t ^= L.cf_k[1]; }
 
     const bool want_in = P.in_parts != nullptr;
     uint32_t phase = 0;
@@ -497,17 +525,17 @@ __global__ void __launch_bounds__(kCtaThreads, 1) k_tile_tmem(const float *amp, 
     uint64_t tile = (uint64_t)blockIdx.x * kGroups + grp;
     const uint64_t step = tbase_of(stride, L);
     uint64_t tbase = tbase_of(tile, L);
-    if (tile < P.tiles) copy_tile(amp, tbase, L, stage, g_t, cs_t);
+    if (tile < P.tiles) copy_tile<TPR>(amp, tbase, L, stage, g_t, cs_t);
     for (; tile < P.tiles; tile += stride) {
         const uint64_t tnext = tile_base_advance(tbase, step, L.tmask);
         asm volatile("cp.async.wait_group 0;" ::: "memory");
-        group_bar(bar_id);
-        float y[64];
+        group_bar<TPR>(bar_id);
+        float y[kV];
         {
-            // gather the thread's block-0 row
+            // gather the thread's part of its block-0 row
             if (L.pair_in) {
 #pragma unroll
-                for (int j = 0; j < 16; ++j) {
+                for (int j = 0; j < 16 / TPR; ++j) {
                     const uint32_t a = stage + ((xrow ^ L.s_col[2 * j]) << 3);
                     asm volatile("ld.shared.v4.f32 {%0,%1,%2,%3}, [%4];"
                                  : "=f"(y[4 * j]), "=f"(y[4 * j + 1]), "=f"(y[4 * j + 2]), "=f"(y[4 * j + 3])
@@ -515,51 +543,51 @@ __global__ void __launch_bounds__(kCtaThreads, 1) k_tile_tmem(const float *amp, 
                 }
             } else {
 #pragma unroll
-                for (int j = 0; j < 32; ++j) {
+                for (int j = 0; j < 32 / TPR; ++j) {
                     const uint32_t a = stage + ((xrow ^ L.s_col[j]) << 3);
                     asm volatile("ld.shared.v2.f32 {%0,%1}, [%2];" : "=f"(y[2 * j]), "=f"(y[2 * j + 1]) : "r"(a));
                 }
             }
             if (want_in) acc_in += (double)sum_squares(y);
-            split_store(tlane, y);
+            split_store<TPR>(tlane, y, c0);
         }
         asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
         asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-        group_bar(bar_id);
+        group_bar<TPR>(bar_id);
         if (ltid == 0) issue_ts(tgrp + 64, tgrp, smem_u32(smem + kOffB), smem_u32(smem + kOffB + kB), mb);
         // a one-block pass needs the staging buffer no more: the next tile's copies
-        if (L.nsub == 1 && tile + stride < P.tiles) copy_tile(amp, tnext, L, stage, g_t, cs_t);
+        if (L.nsub == 1 && tile + stride < P.tiles) copy_tile<TPR>(amp, tnext, L, stage, g_t, cs_t);
 
         for (int b = 0; b < L.nsub; ++b) {
             const bool ok = mbar_wait(mb, phase);
             phase ^= 1;
-            if (group_bar_or(bar_id, !ok)) { failed = true; break; }
+            if (group_bar_or<TPR>(bar_id, !ok)) { failed = true; break; }
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             const uint32_t dreg = (b & 1) ? 0u : 64u;                    // this block's accumulator
-            tmem_ld32(tlane + dreg, y);
-            tmem_ld32(tlane + dreg + 32, y + 32);
+#pragma unroll
+            for (int q = 0; q < 2 / TPR; ++q) tmem_ld32(tlane + dreg + 2 * c0 + 32 * q, y + 32 * q);
             asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
             if (b + 1 < L.nsub) {
-                exchange_through(y, stage, b ? xw1 : xw0, b ? xr1 : xr0, L.xw_col[b], L.xr_col[b], bar_id);
-                split_store(tlane + dreg, y);                            // the next block's A
+                exchange_through<TPR>(y, stage, b ? xw1 : xw0, b ? xr1 : xr0, L.xw_col[b], L.xr_col[b], bar_id);
+                split_store<TPR>(tlane + dreg, y, c0);                   // the next block's A
                 asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
                 asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-                group_bar(bar_id);                                       // also: every exchange read is done
+                group_bar<TPR>(bar_id);                                  // also: every exchange read is done
                 if (ltid == 0)
                     issue_ts(tgrp + (dreg ^ 64u), tgrp + dreg, smem_u32(smem + kOffB + (2 * (b + 1)) * kB),
                              smem_u32(smem + kOffB + (2 * (b + 1) + 1) * kB), mb);
                 // after the last exchange the staging buffer is free: the next tile's copies
-                if (b + 2 == L.nsub && tile + stride < P.tiles) copy_tile(amp, tnext, L, stage, g_t, cs_t);
+                if (b + 2 == L.nsub && tile + stride < P.tiles) copy_tile<TPR>(amp, tnext, L, stage, g_t, cs_t);
             } else {
                 const uint64_t obase = store_base(tile, tbase, P.W) | orow;
                 if (L.vec_out) {
 #pragma unroll
-                    for (int j = 0; j < 16; ++j)
+                    for (int j = 0; j < 16 / TPR; ++j)
                         *reinterpret_cast<float4 *>(out + 2 * (obase | L.o_col[2 * j])) =
                             make_float4(y[4 * j], y[4 * j + 1], y[4 * j + 2], y[4 * j + 3]);
                 } else {
 #pragma unroll
-                    for (int j = 0; j < 32; ++j)
+                    for (int j = 0; j < 32 / TPR; ++j)
                         *reinterpret_cast<float2 *>(out + 2 * (obase | L.o_col[j])) = make_float2(y[2 * j], y[2 * j + 1]);
                 }
                 acc_out += (double)sum_squares(y);                      // after the stores are issued
@@ -576,7 +604,7 @@ __global__ void __launch_bounds__(kCtaThreads, 1) k_tile_tmem(const float *amp, 
             ai += __shfl_xor_sync(0xffffffffu, ai, o);
             ao += __shfl_xor_sync(0xffffffffu, ao, o);
         }
-        constexpr int kWarps = kCtaThreads / 32;
+        constexpr int kWarps = S::kCtaThreads / 32;
         double *red = reinterpret_cast<double *>(smem + kOffStage);      // group 0's staging buffer
         __syncthreads();                     // every copy of every group has landed
         if (lane == 0) { red[warp] = ai; red[kWarps + warp] = ao; }
@@ -588,7 +616,7 @@ __global__ void __launch_bounds__(kCtaThreads, 1) k_tile_tmem(const float *amp, 
             if (P.out_parts) P.out_parts[blockIdx.x] = b;
         }
         if (blockIdx.x == 0)                 // partials past this grid read as zero
-            for (int i = (int)gridDim.x + tid; i < P.nparts; i += kCtaThreads) {
+            for (int i = (int)gridDim.x + tid; i < P.nparts; i += S::kCtaThreads) {
                 if (P.in_parts) P.in_parts[i] = 0.0;
                 if (P.out_parts) P.out_parts[i] = 0.0;
             }
@@ -654,9 +682,14 @@ int qs_launch_tiled_tmem(qs_state *s, const qs_tiled_desc *d, int *err_dev)
         return qs_fail(QS_ERR_ARG, "tiled pass: set both buffers, and distinct, or neither");
     if (d->has_write && !d->amp_out)
         return qs_fail(QS_ERR_ARG, "tiled pass: remapped results need a separate output buffer");
-    QS_CUDA_TRY(cudaFuncSetAttribute(k_tile_tmem, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes));
     const unsigned grid = (unsigned)qs_tmem_grid(s);
-    k_tile_tmem<<<grid, kCtaThreads, kSmemBytes, s->stream>>>(in, out, P);
+    if (d->threads_per_row == 2) {
+        QS_CUDA_TRY(cudaFuncSetAttribute(k_tile_tmem<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes));
+        k_tile_tmem<2><<<grid, TShape<2>::kCtaThreads, kSmemBytes, s->stream>>>(in, out, P);
+    } else {
+        QS_CUDA_TRY(cudaFuncSetAttribute(k_tile_tmem<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes));
+        k_tile_tmem<1><<<grid, TShape<1>::kCtaThreads, kSmemBytes, s->stream>>>(in, out, P);
+    }
     QS_LAUNCH_CHECK("k_tile_tmem");
     return QS_OK;
 }
