@@ -254,7 +254,7 @@ __global__ void __launch_bounds__(kThreads, BShape<SUB>::kCtasPerSm) k_batch(Bat
                             }
                     } else {
                         const uint64_t obase = tbase | gCl;
-                        float t = 0.f;
+                        float t4[4] = {0.f, 0.f, 0.f, 0.f};                  // four chains, fixed order
                         float zt[kMaxZZ];
 #pragma unroll
                         for (int i = 0; i < kMaxZZ; ++i) zt[i] = 0.f;
@@ -266,14 +266,14 @@ __global__ void __launch_bounds__(kThreads, BShape<SUB>::kCtasPerSm) k_batch(Bat
                                 const uint64_t g = obase | L.gl[8 * q + e];
                                 *reinterpret_cast<float2 *>(C.amp + 2 * g) = make_float2(re, im);
                                 const float pr = fmaf(re, re, im * im);
-                                t += pr;
+                                t4[e & 3] += pr;
                                 if (last_pass) {
                                     const uint32_t par = (uint32_t)(g ^ (g >> 1));   // bit i: x_i xor x_{i+1}
 #pragma unroll
                                     for (int i = 0; i < kMaxZZ; ++i) zt[i] += ((par >> i) & 1u) ? -pr : pr;
                                 }
                             }
-                        acc_out += (double)t;
+                        acc_out += (double)((t4[0] + t4[1]) + (t4[2] + t4[3]));
                         if (last_pass)
 #pragma unroll
                             for (int i = 0; i < kMaxZZ; ++i) zz[i] += (double)zt[i];

@@ -233,12 +233,9 @@ __global__ void __launch_bounds__(Shape<SUB, TPR>::kCtaThreads, 1) k_fused_tile(
                         a_store_at(aHi, aLo, tp ^ L.scat[b][j0 + 8 * q + e], __uint_as_float(y[q][2 * e]),
                                    __uint_as_float(y[q][2 * e + 1]));
             } else {
-                float t = 0.f;
                 const uint64_t obase = store_base(tile, tbase, P.W) | gCl;
 #pragma unroll
                 for (int q = 0; q < kQ; ++q) {
-#pragma unroll
-                    for (int e = 0; e < 16; ++e) t = fmaf(__uint_as_float(y[q][e]), __uint_as_float(y[q][e]), t);
                     if (L.vecl) {
 #pragma unroll
                         for (int e = 0; e < 8; e += 2) {
@@ -254,7 +251,13 @@ __global__ void __launch_bounds__(Shape<SUB, TPR>::kCtaThreads, 1) k_fused_tile(
                         }
                     }
                 }
-                acc_out += (double)t;
+                float t4[4] = {0.f, 0.f, 0.f, 0.f};               // after the stores are issued
+#pragma unroll
+                for (int q = 0; q < kQ; ++q)
+#pragma unroll
+                    for (int e = 0; e < 16; ++e)
+                        t4[e & 3] = fmaf(__uint_as_float(y[q][e]), __uint_as_float(y[q][e]), t4[e & 3]);
+                acc_out += (double)((t4[0] + t4[1]) + (t4[2] + t4[3]));
             }
             asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
         }
