@@ -218,7 +218,7 @@ def _one_by_one(sv, gates):
 
 
 @pytest.mark.parametrize("dt", ["c128", "c64"])
-@pytest.mark.parametrize("n", [9, 12, 18])
+@pytest.mark.parametrize("n", [5, 6, 9, 10, 12, 18])
 def test_staged_low_qubit_runs_match_gate_by_gate(need_gpu, dt, n):
     """qs_gates_apply runs consecutive gates on the lowest qubits through
     shared memory in one pass (qs_lowstage.cu): the same state as the gates
