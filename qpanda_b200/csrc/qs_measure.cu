@@ -214,6 +214,12 @@ k_marginal(const T *__restrict__ a, MargParams P, double *__restrict__ part)
     }
     typedef typename vec2<T>::type V;
     const V *pa = reinterpret_cast<const V *>(a);
+    // fewer bins than threads: thread t sums fixed positions of every chunk
+    // (bin t / tpbt, terms u = t % tpbt + k tpbt) into a register, and the
+    // threads of a bin combine once at the end
+    const int tpbt = nb < kThreads ? kThreads / nb : 1;
+    const int mb = t / tpbt, msub = t % tpbt;
+    double mine = 0;
     __syncthreads();
     for (uint64_t r = 0; r < P.R; ++r) {
         uint64_t uidx = g * P.R + r, hu = 0;
@@ -245,18 +251,20 @@ k_marginal(const T *__restrict__ a, MargParams P, double *__restrict__ part)
                 acc[b] += s;
             }
         } else {
-            const int tpbt = kThreads / nb;          // threads per bin
-            const int b = t / tpbt, sub = t % tpbt;
             double s = 0;
-            for (int u = sub; u < tpb; u += tpbt) s += p[tabM[b] | tabU[u]];
-            red[t] = s;
-            __syncthreads();
-            for (int w = tpbt >> 1; w > 0; w >>= 1) {
-                if (sub < w) red[t] += red[t + w];
-                __syncthreads();
-            }
-            if (sub == 0) acc[b] += red[t];
+            for (int u = msub; u < tpb; u += tpbt) s += p[tabM[mb] | tabU[u]];
+            mine += s;
         }
+        __syncthreads();
+    }
+    if (nb < kThreads) {
+        red[t] = mine;
+        __syncthreads();
+        for (int w = tpbt >> 1; w > 0; w >>= 1) {
+            if (msub < w) red[t] += red[t + w];
+            __syncthreads();
+        }
+        if (msub == 0) acc[mb] = red[t];
         __syncthreads();
     }
     double *dst = part + g * (1ull << P.m);
@@ -420,17 +428,31 @@ k_inner(const Ta *__restrict__ a, const Tb *__restrict__ b, uint64_t N, double *
     typedef typename vec2<Tb>::type VB;
     const VA *pa = reinterpret_cast<const VA *>(a);
     const VB *pb = reinterpret_cast<const VB *>(b);
-    double re = 0, im = 0;
+    // four elements in flight per thread, two accumulator pairs (fixed order)
+    double re[2] = {0, 0}, im[2] = {0, 0};
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < N; i += stride) {
-        VA x = pa[i];
-        VB y = pb[i];
-        double xr = x.x, xi = x.y, yr = y.x, yi = y.y;
-        re += xr * yr + xi * yi;          // conj(x) * y
-        im += xr * yi - xi * yr;
+    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    for (; i + 3 * stride < N; i += 4 * stride) {
+        VA x[4];
+        VB y[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) { x[u] = pa[i + u * stride]; y[u] = pb[i + u * stride]; }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const double xr = x[u].x, xi = x[u].y, yr = y[u].x, yi = y[u].y;
+            re[u & 1] += xr * yr + xi * yi;          // conj(x) * y
+            im[u & 1] += xr * yi - xi * yr;
+        }
     }
-    double sre = block_sum(re);
-    double sim = block_sum(im);
+    for (; i < N; i += stride) {
+        const VA x = pa[i];
+        const VB y = pb[i];
+        const double xr = x.x, xi = x.y, yr = y.x, yi = y.y;
+        re[0] += xr * yr + xi * yi;
+        im[0] += xr * yi - xi * yr;
+    }
+    double sre = block_sum(re[0] + re[1]);
+    double sim = block_sum(im[0] + im[1]);
     if (threadIdx.x == 0) {
         partials[2 * blockIdx.x] = sre;
         partials[2 * blockIdx.x + 1] = sim;
@@ -447,7 +469,21 @@ k_diff(const Ta *__restrict__ a, const Tb *__restrict__ b, uint64_t N, double *p
     const VB *pb = reinterpret_cast<const VB *>(b);
     double mx = 0, ss = 0;
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < N; i += stride) {
+    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    for (; i + 3 * stride < N; i += 4 * stride) {            // four elements in flight
+        VA x[4];
+        VB y[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) { x[u] = pa[i + u * stride]; y[u] = pb[i + u * stride]; }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const double dr = (double)x[u].x - (double)y[u].x, di = (double)x[u].y - (double)y[u].y;
+            const double d2 = dr * dr + di * di;
+            ss += d2;
+            mx = fmax(mx, d2);
+        }
+    }
+    for (; i < N; i += stride) {
         VA x = pa[i];
         VB y = pb[i];
         double dr = (double)x.x - (double)y.x, di = (double)x.y - (double)y.y;
@@ -782,7 +818,7 @@ extern "C" int qs_inner(qs_state *a, qs_state *b, double *re, double *im)
     if (a->n != b->n) return qs_fail(QS_ERR_ARG, "qs_inner: qubit counts differ (%d vs %d)", a->n, b->n);
     // Order b's pending work before a's reduction.
     QS_CUDA_TRY(cudaStreamSynchronize(b->stream));
-    unsigned grid = grid_for(a->N, kThreads, 4);
+    unsigned grid = grid_for(a->N, kThreads, 8);
     double *part = reinterpret_cast<double *>(static_cast<char *>(a->scratch) + kPartOff);
     if (a->dtype == QS_C64 && b->dtype == QS_C64)
         k_inner<float, float><<<grid, kThreads, 0, a->stream>>>((const float *)a->amp, (const float *)b->amp, a->N, part);
@@ -809,7 +845,7 @@ extern "C" int qs_diff(qs_state *a, qs_state *b, double *max_abs, double *sum_sq
     if ((r = qs_check_state(b))) return r;
     if (a->n != b->n) return qs_fail(QS_ERR_ARG, "qs_diff: qubit counts differ (%d vs %d)", a->n, b->n);
     QS_CUDA_TRY(cudaStreamSynchronize(b->stream));
-    unsigned grid = grid_for(a->N, kThreads, 4);
+    unsigned grid = grid_for(a->N, kThreads, 8);
     double *part = reinterpret_cast<double *>(static_cast<char *>(a->scratch) + kPartOff);
     if (a->dtype == QS_C64 && b->dtype == QS_C64)
         k_diff<float, float><<<grid, kThreads, 0, a->stream>>>((const float *)a->amp, (const float *)b->amp, a->N, part);
