@@ -235,7 +235,9 @@ def test_staged_low_qubit_runs_match_gate_by_gate(need_gpu, dt, n):
         a.apply(g)
         _one_by_one(b, g)
         mx, _ = a.diff(b)
-        assert mx <= (1e-15 if dt == "c128" else 1e-7), mx
+        # FP32 rounding level (a few ulps of amplitudes up to ~0.5 on the
+        # narrow states; the two kernels may contract multiply-adds differently)
+        assert mx <= (1e-15 if dt == "c128" else 5e-7), mx
         o = OracleState(n)
         o.set_state(init)
         o.apply(g)
