@@ -720,15 +720,41 @@ static void tiled_pass_desc(const qs_plan *P, size_t u, bool last, int mode, std
         const int c_next = P->blocks[nx.first].q[0];
         const int c_last = P->blocks[pp.first + pp.count - 1].q[0];
         auto in_tile = [&](int q) { return ((tmask >> pos[q]) & 1) != 0; };
-        int head = -1;
-        if (in_tile(c_next) && ((next >> c_next) & 1)) head = c_next;
-        else if (in_tile(c_last) && ((next >> c_last) & 1)) head = c_last;
+        auto shared = [&](int q) { return ((next >> q) & 1) != 0; };
         std::vector<int> order;
-        if (head >= 0) order.push_back(head);
-        for (int l = 0; l < 12; ++l)
-            if (tq[l] != head && ((next >> tq[l]) & 1)) order.push_back(tq[l]);
-        for (int l = 0; l < 12; ++l)
-            if (!((next >> tq[l]) & 1)) order.push_back(tq[l]);
+        if (P->opts.tile_in_tmem) {
+            // k_tile_tmem: position 0 a column of this pass's last block (its
+            // results leave as 16-byte stores), shared with the next pass (whose
+            // loads then start at 0) - its block-0 column if possible; then the
+            // shared qubits outside the last block, which become that block's
+            // lanes (a warp's stores then cover consecutive positions), then
+            // the other shared ones, then the rest, lanes before columns
+            uint64_t lastcols = 0;
+            for (int j = 0; j < 5; ++j) lastcols |= 1ull << P->blocks[pp.first + pp.count - 1].q[j];
+            auto col = [&](int q) { return ((lastcols >> q) & 1) != 0; };
+            int head = -1;
+            if (in_tile(c_next) && shared(c_next) && col(c_next)) head = c_next;
+            for (int l = 0; l < 12 && head < 0; ++l)
+                if (shared(tq[l]) && col(tq[l])) head = tq[l];
+            if (head < 0 && in_tile(c_next) && shared(c_next)) head = c_next;
+            if (head >= 0) order.push_back(head);
+            for (int pass2 = 0; pass2 < 4; ++pass2)
+                for (int l = 0; l < 12; ++l) {
+                    const int q = tq[l];
+                    if (q == head) continue;
+                    const int cls = shared(q) ? (col(q) ? 1 : 0) : (col(q) ? 3 : 2);
+                    if (cls == pass2) order.push_back(q);
+                }
+        } else {
+            int head = -1;
+            if (in_tile(c_next) && shared(c_next)) head = c_next;
+            else if (in_tile(c_last) && shared(c_last)) head = c_last;
+            if (head >= 0) order.push_back(head);
+            for (int l = 0; l < 12; ++l)
+                if (tq[l] != head && shared(tq[l])) order.push_back(tq[l]);
+            for (int l = 0; l < 12; ++l)
+                if (!shared(tq[l])) order.push_back(tq[l]);
+        }
         for (int k = 0; k < 12; ++k) npos[order[k]] = k;
         for (int l = 0; l < 12; ++l) d.wtile[l] = npos[tq[l]];
         for (int p = 0, i = 0; p < n; ++p)

@@ -258,3 +258,27 @@ def test_tmem_conflict_free_on_the_bench_layouts(emu):
         err, took, left, gclash, cclash, xclash = run_tmem_emu(emu, n, g, random_state(n, 7), remap)
         assert err < 1e-10 and left == 0
         assert (gclash, cclash, xclash) == (0, 0, 0), (remap, gclash, cclash, xclash)
+
+
+def test_tmem_layout_shape_of_the_32q_bench_plan(emu):
+    """The remapped plan of the 32-qubit benchmark circuit (2 low qubits, the
+    tuned choice) puts a column of each pass's last block at write position 0
+    and its lanes just above, so that most passes store 16-byte vectors and a
+    warp's stores touch few 128-byte lines; the next pass's copies keep their
+    contiguous runs.  8 KB per warp and tile each way: 64 lines at best."""
+    E = emu
+    E.tmem_layout_stats.argtypes = [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_longlong),
+                                    C.POINTER(C.c_longlong)]
+    E.tmem_layout_stats.restype = C.c_int
+    n = 32
+    g = circuits.random_layers(n, 16, 20240601, iswap_frac=0.1)
+    p = FusionPlan(n, g, remap=1, low_qubits=2)
+    vec, st, cp = C.c_int(), C.c_longlong(), C.c_longlong()
+    assert E.tmem_layout_stats(p.handle, n, 1, C.byref(vec), C.byref(st), C.byref(cp)) == 0, \
+        E.tile_emu_error().decode()
+    passes = p.num_launches()
+    p.close()
+    assert passes == 32
+    assert vec.value >= 20, vec.value                       # 11 before the write order favoured the stores
+    assert st.value / passes <= 80, st.value / passes       # 120 lines per warp and tile before
+    assert cp.value / passes <= 72, cp.value / passes

@@ -24,6 +24,7 @@
 // runs; nvcc because the shared headers hold device helpers):
 //   nvcc -O2 -std=c++17 -x cu -shared -Xcompiler -fPIC tile_emu.cpp
 //        -I<csrc> -I<include> -L<lib> -lqsb200
+#include <algorithm>
 #include <complex>
 #include <cstdint>
 #include <cstdio>
@@ -552,5 +553,57 @@ extern "C" int tmem_emu_apply(const qs_plan *P, int n, double *state, int remap,
             if (hits[i] != 1) return fail("output amplitude not written exactly once", (long long)k, (long long)i);
     }
     memcpy(state, buf0.data(), N * sizeof(cd));
+    return 0;
+}
+
+// Memory shape of k_tile_tmem's accesses over a plan (no state needed): the
+// passes whose last block stores 16-byte vectors, and per warp and tile the
+// distinct 128-byte lines its store instructions and its copy instructions
+// touch (8 KB each way: 64 lines at best), summed over the passes.
+extern "C" int tmem_layout_stats(const qs_plan *P, int n, int remap, int *vec_out_passes, long long *store_lines,
+                                 long long *copy_lines)
+{
+    g_err[0] = 0;
+    const size_t npass = P->passes.size();
+    std::vector<qs_tiled_desc> descs;
+    std::vector<int> dst;
+    if (qs_plan_tiled_schedule(P, n, 0, npass, remap, descs, dst)) return fail("schedule failed");
+    *vec_out_passes = 0;
+    *store_lines = *copy_lines = 0;
+    for (size_t k = 0; k < npass; ++k) {
+        qs_tmem::TLayout L;
+        if (qs_tmem_layout_build(n, &descs[k], &L)) return fail("pass %lld: no tensor-memory layout", (long long)k);
+        *vec_out_passes += L.vec_out ? 1 : 0;
+        const int nj = L.vec_out ? 16 : 32;
+        for (int w = 0; w < 4; ++w) {
+            for (int j = 0; j < nj; ++j) {
+                std::vector<uint64_t> lines;
+                for (int l = 0; l < 32; ++l) {
+                    uint64_t o = L.o_col[L.vec_out ? 2 * j : j];
+                    for (int i = 0; i < 5; ++i)
+                        if ((l >> i) & 1) o |= L.o_lane[i];
+                    for (int v = 0; v < 2; ++v)
+                        if ((w >> v) & 1) o |= L.o_warp[v];
+                    lines.push_back(o >> 4);                     // 8-byte amplitudes, 128-byte lines
+                }
+                std::sort(lines.begin(), lines.end());
+                *store_lines += std::unique(lines.begin(), lines.end()) - lines.begin();
+            }
+            for (int k2 = 0; k2 < 16; ++k2) {
+                std::vector<uint64_t> lines;
+                for (int l = 0; l < 32; ++l) {
+                    const int t = 32 * w + l;
+                    uint64_t g = L.gk[k2];
+                    for (int b = 0; b < 7; ++b)
+                        if ((t >> b) & 1) g |= L.g_bit[b];
+                    lines.push_back(g >> 4);
+                }
+                std::sort(lines.begin(), lines.end());
+                *copy_lines += std::unique(lines.begin(), lines.end()) - lines.begin();
+            }
+        }
+    }
+    *store_lines /= 4;
+    *copy_lines /= 4;
     return 0;
 }
