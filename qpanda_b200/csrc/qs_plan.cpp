@@ -725,15 +725,22 @@ static void tiled_pass_desc(const qs_plan *P, size_t u, bool last, int mode, std
         if (P->opts.tile_in_tmem) {
             // k_tile_tmem: position 0 a column of this pass's last block (its
             // results leave as 16-byte stores), shared with the next pass (whose
-            // loads then start at 0) - its block-0 column if possible; then the
+            // loads then start at 0) - one of its block-0 columns if possible; then the
             // shared qubits outside the last block, which become that block's
             // lanes (a warp's stores then cover consecutive positions), then
             // the other shared ones, then the rest, lanes before columns
-            uint64_t lastcols = 0;
-            for (int j = 0; j < 5; ++j) lastcols |= 1ull << P->blocks[pp.first + pp.count - 1].q[j];
+            uint64_t lastcols = 0, nextcols = 0;
+            for (int j = 0; j < 5; ++j) {
+                lastcols |= 1ull << P->blocks[pp.first + pp.count - 1].q[j];
+                nextcols |= 1ull << P->blocks[nx.first].q[j];
+            }
             auto col = [&](int q) { return ((lastcols >> q) & 1) != 0; };
+            auto ncol = [&](int q) { return ((nextcols >> q) & 1) != 0; };
+            // position 0 in the last block's columns gives its 16-byte stores, in
+            // the next pass's block-0 columns that pass's 16-byte gathers
             int head = -1;
-            if (in_tile(c_next) && shared(c_next) && col(c_next)) head = c_next;
+            for (int l = 0; l < 12 && head < 0; ++l)
+                if (shared(tq[l]) && col(tq[l]) && ncol(tq[l])) head = tq[l];
             for (int l = 0; l < 12 && head < 0; ++l)
                 if (shared(tq[l]) && col(tq[l])) head = tq[l];
             if (head < 0 && in_tile(c_next) && shared(c_next)) head = c_next;
