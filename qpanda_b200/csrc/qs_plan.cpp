@@ -739,6 +739,16 @@ static void tiled_pass_desc(const qs_plan *P, size_t u, bool last, int mode, std
             // position 0 in the last block's columns gives its 16-byte stores, in
             // the next pass's block-0 columns that pass's 16-byte gathers
             int head = -1;
+            // a one-block pass reads and writes through one layout, whose
+            // register bit 0 is either read position 0 (16-byte gathers) or
+            // write position 0 (16-byte stores): when read position 0 is a
+            // column, write it at 0 too, or - not shared with the next pass -
+            // put a non-column there, so that the gather keeps its pairs
+            if (pp.count == 1 && col(tq[0])) {
+                if (shared(tq[0])) head = tq[0];
+                for (int l = 1; l < 12 && head < 0; ++l)
+                    if (shared(tq[l]) && !col(tq[l])) head = tq[l];
+            }
             for (int l = 0; l < 12 && head < 0; ++l)
                 if (shared(tq[l]) && col(tq[l]) && ncol(tq[l])) head = tq[l];
             for (int l = 0; l < 12 && head < 0; ++l)
