@@ -342,9 +342,11 @@ typedef struct qs_batch_opts {
     int use_graph;         /* capture the launch in a CUDA graph and replay it */
     int block_qubits;      /* fusion width: gates are grouped into blocks of at most 4 or 5 qubits
                               (default 5; applied as 5-qubit blocks either way) */
+    int tile_in_tmem;      /* with max_sub <= 2: 1 = the tile in tensor memory as the MMAs' A operand
+                              (k_batch_tmem, default), 0 = in shared memory (k_batch) */
 } qs_batch_opts;
 /* Defaults (2 blocks per pass, 3 low qubits, longest first, graph, 5-qubit
- * fusion).  Fill a qs_batch_opts with this call before changing fields: the
+ * fusion, the tile in tensor memory).  Fill a qs_batch_opts with this call before changing fields: the
  * struct may gain fields at its end. */
 int qs_batch_default_opts(qs_batch_opts *opts);
 /* Circuit c has n_qubits[c] qubits and gates[offsets[c] .. offsets[c+1]). */

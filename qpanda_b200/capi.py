@@ -383,7 +383,7 @@ class FusionPlan:
 
 class BatchOpts(C.Structure):
     _fields_ = [("max_sub", C.c_int), ("low_qubits", C.c_int), ("order", C.c_int), ("use_graph", C.c_int),
-                ("block_qubits", C.c_int)]
+                ("block_qubits", C.c_int), ("tile_in_tmem", C.c_int)]
 
 
 def _concat(circuits_list):

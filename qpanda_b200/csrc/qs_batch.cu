@@ -27,6 +27,10 @@
 #include "qs_plan_internal.h"
 #include "qs_prim.h"
 #include "qs_tile_core.cuh"
+#include "qs_tile_tmem.cuh"
+#include "qs_tile_tmem_dev.cuh"
+
+int qs_tmem_layout_build(int n, const qs_tiled_desc *d, qs_tmem::TLayout *L);
 
 namespace {
 
@@ -66,6 +70,7 @@ struct BatchCirc {
     const uint16_t *mats;        // the circuit's blocks, [2][64][64] BF16 each
     const Layout *layouts;       // its passes (Layout::pad = first block of the pass)
     const LoadMap *loads;        // their tile-order copy maps
+    const qs_tmem::TLayout *tlayouts;   // its passes' tensor-memory layouts (k_batch_tmem), or null
     double *zz;                  // nq - 1 outputs
     int32_t npass, nq, nq_eff, pad;
 };
@@ -321,6 +326,239 @@ __global__ void __launch_bounds__(kThreads, BShape<SUB>::kCtasPerSm) k_batch(Bat
     }
 }
 
+// The same sweep with the tile in tensor memory: k_tile_tmem's pass body
+// (qs_tile_tmem.cu: staging copies in tile order, the row gather, the tile as
+// the MMAs' A operand in TMEM, the exchange between blocks through the staging
+// buffer, the stores of the last block) run by one 128-thread CTA per circuit,
+// three CTAs per SM, passes of up to two blocks; what k_batch adds stays as it
+// is: the queue, |0...0> on the first pass without reading memory, the
+// previous pass's norm folded into the first block's matrix, and the
+// <Z_i Z_{i+1}> of the last pass's output.
+constexpr int kTmThreads = 128;
+constexpr int kTmCtasPerSm = 3;
+constexpr uint32_t kTmOffB = 0;                                      // 2 blocks x (hi, lo) x 8 KB
+constexpr uint32_t kTmOffStage = 2 * 2 * kB;                         // 32 KB of staging
+constexpr uint32_t kTmOffLayout = kTmOffStage + kStage;
+constexpr uint32_t kTmLayoutBytes = (sizeof(qs_tmem::TLayout) + 15) & ~15u;
+constexpr uint32_t kTmOffMisc = kTmOffLayout + kTmLayoutBytes;       // mbarrier 8, tmem 4, circuit 4
+constexpr uint32_t kTmSmemBytes = kTmOffMisc + 16;
+constexpr uint32_t kTmCols = 128;
+static_assert(kTmCtasPerSm * (kTmSmemBytes + 1024) <= 228 * 1024, "resident CTAs per SM");
+static_assert(kTmCtasPerSm * kTmCols <= 512, "TMEM columns per SM");
+static_assert((4 + 4 * kMaxZZ) * 8 <= kStage, "reductions fit the staging buffer");
+
+__global__ void __launch_bounds__(kTmThreads, kTmCtasPerSm) k_batch_tmem(BatchParams P)
+{
+    namespace D = qs_tmem_dev;
+    extern __shared__ __align__(1024) uint8_t smem[];
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    if (smem_u32(smem) & 1023u) {
+        if (tid == 0) atomicExch(P.err, 2);
+        return;
+    }
+    qs_tmem::TLayout &L = *reinterpret_cast<qs_tmem::TLayout *>(smem + kTmOffLayout);
+    const uint32_t stage = smem_u32(smem + kTmOffStage);
+    uint64_t *mbar = reinterpret_cast<uint64_t *>(smem + kTmOffMisc);
+    uint32_t *tmem_holder = reinterpret_cast<uint32_t *>(smem + kTmOffMisc + 8);
+    int32_t *s_circ = reinterpret_cast<int32_t *>(smem + kTmOffMisc + 12);
+    double *red = reinterpret_cast<double *>(smem + kTmOffStage);   // when no copy is in flight
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                     :: "r"(smem_u32(tmem_holder)), "r"(kTmCols));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(smem_u32(mbar)), "r"(1));
+        asm volatile("fence.mbarrier_init.release.cluster;");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tgrp = *tmem_holder;
+    const uint32_t tlane = tgrp + ((uint32_t)(warp * 32) << 16);
+    const uint32_t mb = smem_u32(mbar);
+    uint32_t phase = 0;
+    bool failed = false;
+
+    while (!failed) {
+        if (tid == 0) {
+            const int c = atomicAdd(P.head, 1);
+            *s_circ = c < P.ncirc ? P.order[c] : -1;
+        }
+        __syncthreads();
+        const int ci = *s_circ;
+        if (ci < 0) break;
+        const BatchCirc C = P.circ[ci];
+        const uint64_t tiles = 1ull << (C.nq_eff - 12);
+        const int nzz = C.nq - 1;
+        float scale = 1.0f;
+        double zz[kMaxZZ];
+#pragma unroll
+        for (int i = 0; i < kMaxZZ; ++i) zz[i] = 0.0;
+        double out_norm = 0.0;
+
+        for (int p = 0; p < C.npass && !failed; ++p) {
+            {
+                const uint32_t *src = reinterpret_cast<const uint32_t *>(C.tlayouts + p);
+                uint32_t *dst = reinterpret_cast<uint32_t *>(&L);
+                for (int i = tid; i < (int)(sizeof(qs_tmem::TLayout) / 4); i += kTmThreads) dst[i] = src[i];
+            }
+            __syncthreads();
+            D::load_b_perm(smem + kTmOffB, C.mats + (size_t)C.layouts[p].pad * 2 * 64 * 64, L, scale);
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            __syncthreads();
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            // per-thread parts of the gather, exchange, copy and store addresses
+            uint32_t xrow = 0, xw0 = 0, xr0 = 0;
+            uint64_t orow = 0, g_t = 0;
+            uint32_t cs_t = (uint32_t)tid;
+#pragma unroll
+            for (int i = 0; i < 5; ++i)
+                if ((lane >> i) & 1) {
+                    xrow ^= L.s_lane[i];
+                    orow |= L.o_lane[i];
+                    xw0 ^= L.xw_lane[0][i];
+                    xr0 ^= L.xr_lane[0][i];
+                }
+#pragma unroll
+            for (int v = 0; v < 2; ++v)
+                if ((warp >> v) & 1) {
+                    xrow ^= L.s_warp[v];
+                    orow |= L.o_warp[v];
+                    xw0 ^= L.xw_warp[0][v];
+                    xr0 ^= L.xr_warp[0][v];
+                }
+#pragma unroll
+            for (int b = 0; b < 7; ++b)
+                if ((tid >> b) & 1) { g_t |= L.g_bit[b]; cs_t ^= L.cf_bit[b]; }
+            const bool last_pass = p + 1 == C.npass;
+            double acc_out = 0;
+            const uint64_t step = D::tbase_of(1, L);
+            uint64_t tbase = 0;
+            if (p > 0) D::copy_tile<1>(C.amp, tbase, L, stage, g_t, cs_t);
+            for (uint64_t tile = 0; tile < tiles; ++tile) {
+                const uint64_t tnext = tile_base_advance(tbase, step, L.tmask);
+                float y[64];
+                if (p == 0) {
+                    // |0...0>: amplitude 0 is tile 0, the row with no row bits, column 0
+#pragma unroll
+                    for (int e = 0; e < 64; ++e) y[e] = 0.f;
+                    if (tile == 0 && tid == 0) y[0] = 1.f;
+                } else {
+                    asm volatile("cp.async.wait_group 0;" ::: "memory");
+                    __syncthreads();
+                    if (L.pair_in) {
+#pragma unroll
+                        for (int j = 0; j < 16; ++j)
+                            asm volatile("ld.shared.v4.f32 {%0,%1,%2,%3}, [%4];"
+                                         : "=f"(y[4 * j]), "=f"(y[4 * j + 1]), "=f"(y[4 * j + 2]), "=f"(y[4 * j + 3])
+                                         : "r"(stage + ((xrow ^ L.s_col[2 * j]) << 3)));
+                    } else {
+#pragma unroll
+                        for (int j = 0; j < 32; ++j)
+                            asm volatile("ld.shared.v2.f32 {%0,%1}, [%2];"
+                                         : "=f"(y[2 * j]), "=f"(y[2 * j + 1]) : "r"(stage + ((xrow ^ L.s_col[j]) << 3)));
+                    }
+                }
+                D::split_store<1>(tlane, y, 0u);
+                asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+                asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+                __syncthreads();
+                if (tid == 0) D::issue_ts(tgrp + 64, tgrp, smem_u32(smem + kTmOffB), smem_u32(smem + kTmOffB + kB), mb);
+                if (p > 0 && L.nsub == 1 && tile + 1 < tiles) D::copy_tile<1>(C.amp, tnext, L, stage, g_t, cs_t);
+                for (int b = 0; b < L.nsub; ++b) {
+                    const bool ok = mbar_wait(mb, phase);
+                    phase ^= 1;
+                    if (__syncthreads_or(!ok)) { failed = true; break; }
+                    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                    const uint32_t dreg = (b & 1) ? 0u : 64u;                // this block's accumulator
+                    D::tmem_ld32(tlane + dreg, y);
+                    D::tmem_ld32(tlane + dreg + 32, y + 32);
+                    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+                    if (b + 1 < L.nsub) {
+                        D::exchange_through<1, kTmThreads>(y, stage, xw0, xr0, L.xw_col[0], L.xr_col[0], 0);
+                        D::split_store<1>(tlane + dreg, y, 0u);              // the next block's A
+                        asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+                        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+                        __syncthreads();                                     // also: every exchange read is done
+                        if (tid == 0)
+                            D::issue_ts(tgrp + (dreg ^ 64u), tgrp + dreg, smem_u32(smem + kTmOffB + 2 * kB),
+                                        smem_u32(smem + kTmOffB + 3 * kB), mb);
+                        if (p > 0 && tile + 1 < tiles) D::copy_tile<1>(C.amp, tnext, L, stage, g_t, cs_t);
+                    } else {
+                        const uint64_t obase = tbase | orow;
+                        if (L.vec_out) {
+#pragma unroll
+                            for (int j = 0; j < 16; ++j)
+                                *reinterpret_cast<float4 *>(C.amp + 2 * (obase | L.o_col[2 * j])) =
+                                    make_float4(y[4 * j], y[4 * j + 1], y[4 * j + 2], y[4 * j + 3]);
+                        } else {
+#pragma unroll
+                            for (int j = 0; j < 32; ++j)
+                                *reinterpret_cast<float2 *>(C.amp + 2 * (obase | L.o_col[j])) =
+                                    make_float2(y[2 * j], y[2 * j + 1]);
+                        }
+                        acc_out += (double)D::sum_squares(y);
+                        if (last_pass) {
+                            float zt[kMaxZZ];
+#pragma unroll
+                            for (int i = 0; i < kMaxZZ; ++i) zt[i] = 0.f;
+#pragma unroll
+                            for (int j = 0; j < 32; ++j) {
+                                const uint64_t g = obase | L.o_col[j];
+                                const float pr = fmaf(y[2 * j], y[2 * j], y[2 * j + 1] * y[2 * j + 1]);
+                                const uint32_t par = (uint32_t)(g ^ (g >> 1));       // bit i: x_i xor x_{i+1}
+#pragma unroll
+                                for (int i = 0; i < kMaxZZ; ++i) zt[i] += ((par >> i) & 1u) ? -pr : pr;
+                            }
+#pragma unroll
+                            for (int i = 0; i < kMaxZZ; ++i) zz[i] += (double)zt[i];
+                        }
+                    }
+                    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+                }
+                if (failed) break;
+                tbase = tnext;
+            }
+            asm volatile("cp.async.wait_group 0;" ::: "memory");
+            // the pass's output norm (fixed order), and the next pass's scale
+            for (int o = 16; o > 0; o >>= 1) acc_out += __shfl_xor_sync(0xffffffffu, acc_out, o);
+            __syncthreads();
+            if (lane == 0) red[warp] = acc_out;
+            __syncthreads();
+            out_norm = red[0] + red[1] + red[2] + red[3];
+            scale = out_norm > 0 ? (float)(1.0 / sqrt(out_norm)) : 1.0f;
+            // this pass's stores must be visible to the next pass's loads
+            __threadfence();
+            __syncthreads();
+        }
+        if (failed) break;
+#pragma unroll
+        for (int i = 0; i < kMaxZZ; ++i)
+            for (int o = 16; o > 0; o >>= 1) zz[i] += __shfl_xor_sync(0xffffffffu, zz[i], o);
+        if (lane == 0)
+#pragma unroll
+            for (int i = 0; i < kMaxZZ; ++i) red[4 + warp * kMaxZZ + i] = zz[i];
+        __syncthreads();
+        for (int i = tid; i < nzz; i += kTmThreads)
+            C.zz[i] = (red[4 + i] + red[4 + kMaxZZ + i] + red[4 + 2 * kMaxZZ + i] + red[4 + 3 * kMaxZZ + i]) /
+                      out_norm;
+        __syncthreads();
+    }
+    if (failed) {
+        if (tid == 0) atomicExch(P.err, 1);
+        mbar_wait(mb, phase ^ 1);
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" :: "r"(tgrp), "r"(kTmCols));
+    }
+}
+
 }  // namespace
 
 // ------------------------------------------------------------------ host
@@ -336,6 +574,8 @@ struct qs_batch {
     void *d_mats = nullptr;              // all block matrices
     void *d_layouts = nullptr;           // layouts of the distinct plan structures
     void *d_loads = nullptr;             // their tile-order copy maps
+    void *d_tlayouts = nullptr;          // their tensor-memory layouts (k_batch_tmem)
+    bool use_tmem = false;
     void *d_circ = nullptr;              // BatchCirc[n]
     void *d_order = nullptr;
     double *d_zz = nullptr;
@@ -352,8 +592,8 @@ void batch_free(qs_batch *B)
 {
     if (B->graph_exec) cudaGraphExecDestroy(B->graph_exec);
     if (B->graph) cudaGraphDestroy(B->graph);
-    for (void *p : {B->d_states, B->d_mats, B->d_layouts, B->d_loads, B->d_circ, B->d_order, (void *)B->d_zz,
-                    (void *)B->d_head})
+    for (void *p : {B->d_states, B->d_mats, B->d_layouts, B->d_loads, B->d_tlayouts, B->d_circ, B->d_order,
+                    (void *)B->d_zz, (void *)B->d_head})
         if (p) cudaFree(p);
     delete B;
 }
@@ -380,6 +620,7 @@ extern "C" int qs_batch_default_opts(qs_batch_opts *o)
     o->order = QS_BATCH_LONGEST_FIRST;
     o->use_graph = 1;
     o->block_qubits = 5;
+    o->tile_in_tmem = 1;
     return QS_OK;
 }
 
@@ -449,6 +690,9 @@ extern "C" int qs_batch_create(int n_circ, const int *n_qubits, const qs_gate *g
     protos.assign(np, nullptr);
     std::vector<std::vector<Layout>> p_layouts(np);
     std::vector<std::vector<LoadMap>> p_loads(np);
+    std::vector<std::vector<qs_tmem::TLayout>> p_tl(np);
+    std::vector<char> tl_ok(np, 1);
+    bool want_tmem = o.tile_in_tmem && o.max_sub <= 2;
     std::vector<int> prc(np, QS_OK);
     std::vector<std::string> perr(np);
     if (!r)
@@ -469,6 +713,18 @@ extern "C" int qs_batch_create(int n_circ, const int *n_qubits, const qs_gate *g
                 L.pad = (int32_t)pass.first;
                 p_layouts[pi].push_back(L);
                 p_loads[pi].push_back(M);
+                if (want_tmem && tl_ok[pi]) {
+                    // the same pass for k_batch_tmem: in place, natural layout
+                    qs_tiled_desc d;
+                    memset(&d, 0, sizeof(d));
+                    for (int t = 0; t < 12; ++t) d.T[t] = pass.T[t];
+                    d.nsub = (int)pass.count;
+                    for (size_t b = 0; b < pass.count; ++b)
+                        for (int j = 0; j < 5; ++j) d.qpos[b][j] = qpos[b][j];
+                    qs_tmem::TLayout TL;
+                    if (qs_tmem_layout_build(pp->n, &d, &TL) == QS_OK) p_tl[pi].push_back(TL);
+                    else tl_ok[pi] = 0;                         // this structure stays on k_batch
+                }
             }
             if (rr) perr[pi] = qs_last_error();
             prc[pi] = rr;
@@ -486,11 +742,15 @@ extern "C" int qs_batch_create(int n_circ, const int *n_qubits, const qs_gate *g
     // ---- device memory
     std::vector<Layout> layouts;                      // per proto, concatenated
     std::vector<LoadMap> loads;                       // their tile-order copy maps
+    std::vector<qs_tmem::TLayout> tlayouts;           // and tensor-memory layouts (same indices)
     std::vector<size_t> layout_first(np);
+    for (int pi = 0; pi < np && want_tmem; ++pi) want_tmem = tl_ok[pi] != 0;   // one kernel for the batch
+    B->use_tmem = want_tmem;
     for (int pi = 0; pi < np && !r; ++pi) {
         layout_first[pi] = layouts.size();
         layouts.insert(layouts.end(), p_layouts[pi].begin(), p_layouts[pi].end());
         loads.insert(loads.end(), p_loads[pi].begin(), p_loads[pi].end());
+        if (want_tmem) tlayouts.insert(tlayouts.end(), p_tl[pi].begin(), p_tl[pi].end());
     }
     std::vector<size_t> mat_off(n_circ);
     size_t mat_total = 0;
@@ -515,6 +775,8 @@ extern "C" int qs_batch_create(int n_circ, const int *n_qubits, const qs_gate *g
         if (e == cudaSuccess) e = cudaMalloc(&B->d_mats, std::max<size_t>(hm.size() * 2, 16));
         if (e == cudaSuccess) e = cudaMalloc(&B->d_layouts, std::max<size_t>(layouts.size() * sizeof(Layout), 16));
         if (e == cudaSuccess) e = cudaMalloc(&B->d_loads, std::max<size_t>(loads.size() * sizeof(LoadMap), 16));
+        if (e == cudaSuccess && want_tmem)
+            e = cudaMalloc(&B->d_tlayouts, std::max<size_t>(tlayouts.size() * sizeof(qs_tmem::TLayout), 16));
         if (e == cudaSuccess) e = cudaMalloc(&B->d_circ, sizeof(BatchCirc) * n_circ);
         if (e == cudaSuccess) e = cudaMalloc(&B->d_order, sizeof(int32_t) * n_circ);
         if (e == cudaSuccess) e = cudaMalloc((void **)&B->d_zz, std::max<size_t>(B->zz_count, 1) * sizeof(double));
@@ -524,6 +786,9 @@ extern "C" int qs_batch_create(int n_circ, const int *n_qubits, const qs_gate *g
             e = cudaMemcpy(B->d_layouts, layouts.data(), layouts.size() * sizeof(Layout), cudaMemcpyHostToDevice);
         if (e == cudaSuccess && !loads.empty())
             e = cudaMemcpy(B->d_loads, loads.data(), loads.size() * sizeof(LoadMap), cudaMemcpyHostToDevice);
+        if (e == cudaSuccess && want_tmem && !tlayouts.empty())
+            e = cudaMemcpy(B->d_tlayouts, tlayouts.data(), tlayouts.size() * sizeof(qs_tmem::TLayout),
+                           cudaMemcpyHostToDevice);
         if (e != cudaSuccess) r = qs_cuda_fail(e, "qs_batch_create: device memory");
     }
     if (!r) {
@@ -534,6 +799,8 @@ extern "C" int qs_batch_create(int n_circ, const int *n_qubits, const qs_gate *g
             bc.mats = static_cast<const uint16_t *>(B->d_mats) + mat_off[c];
             bc.layouts = static_cast<const Layout *>(B->d_layouts) + layout_first[proto_id[c]];
             bc.loads = static_cast<const LoadMap *>(B->d_loads) + layout_first[proto_id[c]];
+            bc.tlayouts = want_tmem ? static_cast<const qs_tmem::TLayout *>(B->d_tlayouts) + layout_first[proto_id[c]]
+                                    : nullptr;
             bc.zz = B->d_zz + B->zz_off[c];
             bc.npass = (int32_t)pp->passes.size();
             bc.nq = B->nq[c];
@@ -569,7 +836,10 @@ int batch_launch(qs_batch *B, cudaStream_t st)
     P.ncirc = B->n;
     P.head = B->d_head;
     P.err = B->d_head + 1;
-    if (B->opts.max_sub <= 2) {
+    if (B->use_tmem) {
+        const unsigned grid = (unsigned)std::min(B->n, QS_SM_COUNT * kTmCtasPerSm);
+        k_batch_tmem<<<grid, kTmThreads, kTmSmemBytes, st>>>(P);
+    } else if (B->opts.max_sub <= 2) {
         const unsigned grid = (unsigned)std::min(B->n, QS_SM_COUNT * BShape<2>::kCtasPerSm);
         k_batch<2><<<grid, kThreads, BShape<2>::kSmemBytes, st>>>(P);
     } else {
@@ -588,6 +858,7 @@ extern "C" int qs_batch_run(qs_batch *B, void *stream)
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     QS_CUDA_TRY(cudaFuncSetAttribute(k_batch<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, BShape<2>::kSmemBytes));
     QS_CUDA_TRY(cudaFuncSetAttribute(k_batch<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, BShape<3>::kSmemBytes));
+    QS_CUDA_TRY(cudaFuncSetAttribute(k_batch_tmem, cudaFuncAttributeMaxDynamicSharedMemorySize, kTmSmemBytes));
     if (!B->opts.use_graph) return batch_launch(B, st);
     if (!B->graph_exec) {
         // capture once on a private stream; replay on the caller's stream
@@ -770,14 +1041,15 @@ extern "C" int qs_batch_autotune_cached(int n_circ, const int *n_qubits, const q
         char line[256];
         while (fgets(line, sizeof(line), f)) {
             unsigned long long k = 0;
-            int ms, lq, order, bq;
+            int ms, lq, order, bq, tm;
             double t;
-            if (sscanf(line, "%llx %d %d %d %d %lf", &k, &ms, &lq, &order, &bq, &t) == 6 && k == key) {
+            if (sscanf(line, "%llx %d %d %d %d %d %lf", &k, &ms, &lq, &order, &bq, &tm, &t) == 7 && k == key) {
                 qs_batch_default_opts(best);
                 best->max_sub = ms;
                 best->low_qubits = lq;
                 best->order = order;
                 best->block_qubits = bq;
+                best->tile_in_tmem = tm;
                 if (best_ms) *best_ms = t;
                 if (from_cache) *from_cache = 1;
                 fclose(f);
@@ -792,8 +1064,8 @@ extern "C" int qs_batch_autotune_cached(int n_circ, const int *n_qubits, const q
     if (best_ms) *best_ms = t;
     FILE *f = fopen(cache_path, "a");
     if (!f) return qs_fail(QS_ERR_IO, "qs_batch_autotune_cached: cannot write %s", cache_path);
-    fprintf(f, "%016llx %d %d %d %d %.6f\n", (unsigned long long)key, best->max_sub, best->low_qubits, best->order,
-            best->block_qubits, t);
+    fprintf(f, "%016llx %d %d %d %d %d %.6f\n", (unsigned long long)key, best->max_sub, best->low_qubits,
+            best->order, best->block_qubits, best->tile_in_tmem, t);
     fclose(f);
     return QS_OK;
 }

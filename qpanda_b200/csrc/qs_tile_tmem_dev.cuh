@@ -47,7 +47,7 @@ __device__ __forceinline__ uint64_t tbase_of(uint64_t tile, const TLayout &L)
 // column order (register bit p = matrix bit mperm[b][p], for rows and
 // columns alike); block 0's scaled by `scale` (hi + lo recombined, scaled,
 // split again).
-__device__ void load_b_perm(uint8_t *dst, const uint16_t *mat, const TLayout &L, float scale)
+__device__ inline void load_b_perm(uint8_t *dst, const uint16_t *mat, const TLayout &L, float scale)
 {
     const int total = L.nsub * 64 * 32;
     for (int it = threadIdx.x; it < total; it += blockDim.x) {

@@ -113,3 +113,20 @@ def test_fusion_width_4_and_tuning_cache(need_gpu, tmp_path):
                                                                       o2.order)
     assert o1.block_qubits in (4, 5)
     assert len(cache.read_text().splitlines()) == 1
+
+
+@pytest.mark.parametrize("tmem", [1, 0])
+def test_batch_tile_in_tensor_or_shared_memory(need_gpu, tmem):
+    """The batched kernels with the tile in tensor memory (k_batch_tmem, the
+    default for passes of up to two blocks) and in shared memory (k_batch)
+    both give the oracle's <ZZ> and states, with both fusion widths."""
+    sweep = small_sweep(4, count=16)
+    for bq in (5, 4):
+        b = Batch(sweep, tile_in_tmem=tmem, block_qubits=bq)
+        b.run()
+        zz = b.zz()
+        for k, (q, g) in enumerate(sweep):
+            ref_zz, ref_state = oracle_zz(q, g)
+            assert np.abs(zz[k] - ref_zz).max() < TOL, (k, q, bq)
+            assert np.abs(b.state(k) - ref_state).max() < TOL, (k, q, bq)
+        b.close()
