@@ -966,11 +966,14 @@ def vqe_line(args, steps, warmup, tune_stride=16, gpu_id=None, rank=0):
                    "layers": "U{4..12}", "seed": SWEEP_SEED, "outputs": "all <Z_i Z_{i+1}>",
                    "launch": "one persistent kernel, CUDA graph replay",
                    "autotuned": {"block_qubits": opts.block_qubits, "max_sub": opts.max_sub,
-                                 "low_qubits": opts.low_qubits, "order": opts.order, "sample_ms": tune_ms,
+                                 "low_qubits": opts.low_qubits, "order": opts.order,
+                                 "tile_in_tmem": opts.tile_in_tmem, "sample_ms": tune_ms,
                                  "tune_s": tune_s, "stride": None if args.no_autotune else tune_stride,
                                  "cache": None if args.no_autotune else cache, "from_cache": hit},
                    "build_s": build_s, "l2": "21 GB of states >> L2"},
-        "roofline": {"bound": "hbm", "kernel": "k_batch", "achieved": alg / step_s / 1e9, "peak": peak,
+        "roofline": {"bound": "hbm",
+                     "kernel": "k_batch_tmem" if (opts.tile_in_tmem and opts.max_sub <= 2) else "k_batch",
+                     "achieved": alg / step_s / 1e9, "peak": peak,
                      "unit": "GB/s", "frac": alg / step_s / 1e9 / peak, "peak_source": peak_kind,
                      "traffic": None, "algorithmic_bytes_per_launch": alg, "launch_s": step_s},
         "zz_checksum": float(sum(float(np.sum(z)) for z in zz)),
@@ -1104,7 +1107,8 @@ def requests_line(args, n_requests, every, gpu_id=None, rank=0, budget_gb=120):
                           "mean": float(lats.mean())},
             "service_s": {"p50": float(np.percentile(svcs, 50)), "p99": float(np.percentile(svcs, 99))},
             "failed": len(sample) - n_ok,
-            "roofline": {"bound": "hbm", "kernel": "k_fused_tile (all requests)", "achieved": alg_bytes / makespan / 1e9,
+            "roofline": {"bound": "hbm", "kernel": "fused tiled passes (all requests)",
+                         "achieved": alg_bytes / makespan / 1e9,
                          "peak": peak, "unit": "GB/s", "frac": alg_bytes / makespan / 1e9 / peak,
                          "peak_source": peak_kind, "traffic": None, "algorithmic_bytes_per_launch": alg_bytes,
                          "launch_s": makespan},
