@@ -275,12 +275,14 @@ k_marginal(const T *__restrict__ a, MargParams P, double *__restrict__ part)
     }
 }
 
-// The same marginal when every chunk bit is measured (P.ulo == 0, chunks of
-// 4096): each bin is one amplitude of each chunk, so a thread owns fixed
-// chunk positions and adds their |a|^2 in registers, chunk after chunk -
-// the order k_marginal adds them in, so the bins are bit-identical - with
-// 16-byte loads (two complex64 or one complex128 amplitude each), two
-// chunks' loads in flight before their first use, and no shared memory.
+// The same marginal on chunks of 4096 (states of 12 qubits and more): a
+// thread owns fixed chunk positions and adds their |a|^2 in registers, chunk
+// after chunk, with 16-byte loads (two complex64 or one complex128 amplitude
+// each) and two chunks' loads in flight before their first use.  When every
+// chunk bit is measured (P.ulo == 0) each position is a bin - the order
+// k_marginal adds them in, so the bins are bit-identical - and no shared
+// memory is used; otherwise the CTA folds its 4096 position sums into the
+// 2^mlo bins once, at the end, in a fixed order.
 template <typename T>
 __global__ void __launch_bounds__(kThreads)
 k_marginal_direct(const T *__restrict__ a, MargParams P, double *__restrict__ part)
@@ -338,12 +340,52 @@ k_marginal_direct(const T *__restrict__ a, MargParams P, double *__restrict__ pa
         add(v0);
     }
     double *dst = part + g * (1ull << P.m);
+    if (P.ulo == 0) {                                         // every chunk position is a bin
 #pragma unroll
-    for (int i = 0; i < kLoads * kApl; ++i) {
-        const int l = (t + (i / kApl) * kThreads) * kApl + (i % kApl);   // chunk position
+        for (int i = 0; i < kLoads * kApl; ++i) {
+            const int l = (t + (i / kApl) * kThreads) * kApl + (i % kApl);   // chunk position
+            uint64_t oi = out_hi;
+            for (int b = 0; b < P.mlo; ++b) oi |= (uint64_t)((l >> P.mlo_pos[b]) & 1) << P.mlo_out[b];
+            dst[oi] = acc[i];
+        }
+        return;
+    }
+    // some chunk bits unmeasured: fold the 4096 position sums into the 2^mlo
+    // bins once per CTA, in a fixed order (shared memory: 4096 + kThreads doubles)
+    extern __shared__ double fold[];
+    double *red = fold + 4096;
+#pragma unroll
+    for (int i = 0; i < kLoads * kApl; ++i) fold[(t + (i / kApl) * kThreads) * kApl + (i % kApl)] = acc[i];
+    __syncthreads();
+    const int nb = 1 << P.mlo, tpb = 1 << P.ulo;
+    auto position = [&](int b, int u) {
+        uint32_t l = 0;
+        for (int r = 0; r < P.mlo; ++r) l |= (uint32_t)((b >> r) & 1) << P.mlo_pos[r];
+        for (int r = 0; r < P.ulo; ++r) l |= (uint32_t)((u >> r) & 1) << P.ulo_pos[r];
+        return l;
+    };
+    auto out_index = [&](int b) {
         uint64_t oi = out_hi;
-        for (int b = 0; b < P.mlo; ++b) oi |= (uint64_t)((l >> P.mlo_pos[b]) & 1) << P.mlo_out[b];
-        dst[oi] = acc[i];
+        for (int r = 0; r < P.mlo; ++r) oi |= (uint64_t)((b >> r) & 1) << P.mlo_out[r];
+        return oi;
+    };
+    if (nb >= kThreads) {
+        for (int b = t; b < nb; b += kThreads) {
+            double sum = 0;
+            for (int u = 0; u < tpb; ++u) sum += fold[position(b, u)];
+            dst[out_index(b)] = sum;
+        }
+    } else {
+        const int tpbt = kThreads / nb, b = t / tpbt, sub = t % tpbt;
+        double sum = 0;
+        for (int u = sub; u < tpb; u += tpbt) sum += fold[position(b, u)];
+        red[t] = sum;
+        __syncthreads();
+        for (int w = tpbt >> 1; w > 0; w >>= 1) {
+            if (sub < w) red[t] += red[t + w];
+            __syncthreads();
+        }
+        if (sub == 0) dst[out_index(b)] = red[t];
     }
 }
 
@@ -638,8 +680,11 @@ int marginal_launch(qs_state *s, const MargParams &P, double *dev_out, double *p
     if (G == 1) part = dev_out;
     uint64_t ctas = ohi * G;
     if (ctas > 0x7fffffffull) return qs_fail(QS_ERR_UNSUPPORTED, "qs_probs: too many output bins");
-    if (P.ulo == 0 && P.c == 12) {
-        k_marginal_direct<T><<<(unsigned)ctas, kThreads, 0, s->stream>>>(static_cast<const T *>(s->amp), P, part);
+    if (P.c == 12) {
+        // chunk positions accumulated in registers; folded into bins at the end
+        // when some chunk bits are unmeasured (4096 + kThreads doubles of shared memory)
+        const size_t fold_b = P.ulo == 0 ? 0 : (4096 + kThreads) * sizeof(double);
+        k_marginal_direct<T><<<(unsigned)ctas, kThreads, fold_b, s->stream>>>(static_cast<const T *>(s->amp), P, part);
         QS_LAUNCH_CHECK("k_marginal_direct");
     } else {
         size_t smem = marginal_smem(P);
