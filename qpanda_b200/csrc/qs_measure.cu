@@ -283,7 +283,7 @@ k_marginal(const T *__restrict__ a, MargParams P, double *__restrict__ part)
 // k_marginal adds them in, so the bins are bit-identical - and no shared
 // memory is used; otherwise the CTA folds its 4096 position sums into the
 // 2^mlo bins once, at the end, in a fixed order.
-template <typename T>
+template <typename T, bool FOLD>
 __global__ void __launch_bounds__(kThreads)
 k_marginal_direct(const T *__restrict__ a, MargParams P, double *__restrict__ part)
 {
@@ -340,7 +340,7 @@ k_marginal_direct(const T *__restrict__ a, MargParams P, double *__restrict__ pa
         add(v0);
     }
     double *dst = part + g * (1ull << P.m);
-    if (P.ulo == 0) {                                         // every chunk position is a bin
+    if constexpr (!FOLD) {                                    // every chunk position is a bin
 #pragma unroll
         for (int i = 0; i < kLoads * kApl; ++i) {
             const int l = (t + (i / kApl) * kThreads) * kApl + (i % kApl);   // chunk position
@@ -683,8 +683,11 @@ int marginal_launch(qs_state *s, const MargParams &P, double *dev_out, double *p
     if (P.c == 12) {
         // chunk positions accumulated in registers; folded into bins at the end
         // when some chunk bits are unmeasured (4096 + kThreads doubles of shared memory)
-        const size_t fold_b = P.ulo == 0 ? 0 : (4096 + kThreads) * sizeof(double);
-        k_marginal_direct<T><<<(unsigned)ctas, kThreads, fold_b, s->stream>>>(static_cast<const T *>(s->amp), P, part);
+        if (P.ulo == 0)
+            k_marginal_direct<T, false><<<(unsigned)ctas, kThreads, 0, s->stream>>>(static_cast<const T *>(s->amp), P, part);
+        else
+            k_marginal_direct<T, true><<<(unsigned)ctas, kThreads, (4096 + kThreads) * sizeof(double), s->stream>>>(
+                static_cast<const T *>(s->amp), P, part);
         QS_LAUNCH_CHECK("k_marginal_direct");
     } else {
         size_t smem = marginal_smem(P);
