@@ -459,7 +459,7 @@ def run_b200(args):
                   "dominant_kernel": odom, "dominant_gbs": o_ach, "dominant_frac": o_ach / peak,
                   "kernels": kernel_table(okinds)}
     # the plain path as a caller gets it: qs_gates_apply, whose runs of gates
-    # on the low qubits go through shared memory in one pass each
+    # on one tile's qubits go through shared memory in one pass each
     staged_s = None
     if other == "plain" or path == "plain":
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -473,8 +473,9 @@ def run_b200(args):
             other_line["circuit_s_per_gate_launches"] = ot
             other_line["circuit_s"] = ot = staged_s
             other_line["hbm_gbs_effective"] = circuits.gate_bytes(gates, n, amp_b) / ot / 1e9
-            other_line["note"] = ("circuit_s: qs_gates_apply (runs of gates on qubits 0..9 staged in shared "
-                                  "memory, one pass each); kernels: the same gates one launch each")
+            other_line["note"] = ("circuit_s: qs_gates_apply (runs of consecutive gates whose targets share "
+                                  "one tile's 10 qubits staged in shared memory and registers, one pass each); "
+                                  "kernels: the same gates one launch each")
 
     # fidelity of the fused complex64 run against the complex128 per-gate path
     # (the FP64 oracle on the GPU) at 30 qubits on the same circuit structure

@@ -11,6 +11,7 @@
 #include <vector>
 
 #include "qs_common.cuh"
+#include "qs_lowstage.cuh"
 #include "qs_prim.h"
 
 int qs_copy_in(qs_state *s, const void *host, int host_dtype);
@@ -298,45 +299,35 @@ extern "C" int qs_gate_apply(qs_state *s, const qs_gate *g)
 
 // qs_lowstage.cu
 int qs_lowstage_bits(int n);
-bool qs_lowstage_fits(const qs_prim &p, int n);
-int qs_lowstage_max_run();
-double qs_lowstage_traffic(const qs_prim &p, int dtype);
-int qs_launch_lowstage(qs_state *s, const std::vector<qs_prim> &run);
+void qs_lowstage_passes(const std::vector<qs_prim> &prims, int n, int dtype, bool stage_all,
+                        std::vector<qs_low::Pass> &out);
+int qs_launch_lowstage(qs_state *s, const std::vector<qs_prim> &run, uint64_t qmask);
 
-// Gate by gate, except that runs of consecutive gates whose target bits lie
-// in the lowest qubits go through shared memory in one pass each
-// (qs_lowstage.cu) when that moves fewer bytes than the gates would one by
-// one: same arithmetic per amplitude, fewer passes over HBM.
+// Gate by gate, except that runs of consecutive gates whose targets lie
+// within one tile's 10 qubits go through shared memory and registers in one
+// pass each (qs_lowstage.cu) when that moves fewer bytes than the gates would
+// one by one: same arithmetic per amplitude, fewer passes over HBM.
 extern "C" int qs_gates_apply(qs_state *s, const qs_gate *g, size_t count)
 {
     int r = qs_check_state(s);
     if (r) return r;
     if (count && !g) return qs_fail(QS_ERR_ARG, "qs_gates_apply: null gate list");
+    std::vector<qs_prim> prims(count);
+    for (size_t i = 0; i < count; ++i)
+        if ((r = qs_lower_gate(s->n, &g[i], &prims[i]))) return r;
+    std::vector<qs_low::Pass> passes;
+    qs_lowstage_passes(prims, s->n, s->dtype, false, passes);
     std::vector<qs_prim> run;
-    auto flush = [&]() -> int {
-        int rc = QS_OK;
-        double per_gate = 0;
-        for (const qs_prim &p : run) per_gate += qs_lowstage_traffic(p, s->dtype);
-        if (run.size() > 1 && per_gate > 1.0) {
-            rc = qs_launch_lowstage(s, run);
+    for (const qs_low::Pass &ps : passes) {
+        if (ps.qmask) {
+            run.assign(prims.begin() + ps.first, prims.begin() + ps.first + ps.count);
+            r = qs_launch_lowstage(s, run, ps.qmask);
         } else {
-            for (size_t k = 0; k < run.size() && !rc; ++k) rc = qs_launch_prim(s, run[k]);
+            r = qs_launch_prim(s, prims[ps.first]);
         }
-        run.clear();
-        return rc;
-    };
-    for (size_t i = 0; i < count; ++i) {
-        qs_prim p;
-        if ((r = qs_lower_gate(s->n, &g[i], &p))) return r;
-        if (qs_lowstage_fits(p, s->n)) {
-            run.push_back(p);
-            if ((int)run.size() == qs_lowstage_max_run() && (r = flush())) return r;
-        } else {
-            if ((r = flush())) return r;
-            if ((r = qs_launch_prim(s, p))) return r;
-        }
+        if (r) return r;
     }
-    return flush();
+    return QS_OK;
 }
 
 extern "C" int qs_pmeasure(qs_state *s, const int *qubits, int m, uint64_t *idx_out, double *p_out, int *count)

@@ -1,23 +1,28 @@
-// qs_lowstage.cu - the per-gate path with the low-stride qubits staged in
-// shared memory.
+// qs_lowstage.cu - the per-gate path with runs of gates staged in shared
+// memory and registers.
 //
-// A gate whose target bits (the pair it mixes, or none for a phase) lie below
-// qubit K (= 10) mixes amplitudes inside aligned runs of 2^K.  A run of such
-// gates - consecutive in the gate list; their controls and phase masks may
-// include any qubits - is applied in one pass: each CTA loads a 2^K-amplitude
-// tile (16-byte loads) into shared memory and each of its 2^(K-3) threads
-// takes 8 of the tile's amplitudes into registers.  Which 3 tile bits index a
+// A gate whose target bits (the pair it mixes, or none for a phase) lie in a
+// set Q of K (= 10) qubits mixes amplitudes inside the tiles of Q: the 2^K
+// amplitudes that agree on every other qubit.  A run of such gates -
+// consecutive in the gate list, their targets together within K qubits
+// (qubit 0, and 1 for complex64, always in Q; the rest of Q the lowest
+// qubits left); their controls and phase masks may include any qubits - is
+// applied in one pass: each CTA loads a tile (16-byte copies; qubits 0..2 in
+// Q make them whole 32- or 64-byte runs of the state) into shared memory and
+// each of its 2^(K-3) threads takes 8 of the tile's amplitudes into
+// registers.  Which 3 tile bits index a
 // thread's registers (its *layout*) is chosen on the host per stretch of the
 // run so that every gate's target bits are register bits when it is applied:
 // the gate then mixes register pairs of one thread, with no shared-memory
 // traffic and no barrier.  Only when the next gate needs other register bits
 // do the amplitudes go back through shared memory (8 stores, a barrier, 8
-// loads per thread).  A gate whose controls or mask bits at or above K are not
-// all set in the tile's base leaves the tile alone; controls and mask bits
-// below K are a per-amplitude predicate.  The per-amplitude arithmetic is
-// k_pair's and k_phase's (qs_gates.cu), so the state after the run is the
-// state after the gates one by one.  Gates on higher targets keep the
-// streaming kernels, whose pair-index remapping handles any stride.
+// loads per thread).  A gate whose controls or mask bits outside Q are not
+// all set in the tile's base leaves the tile alone; controls and mask bits in
+// Q are a per-amplitude predicate.  The per-amplitude arithmetic is k_pair's
+// and k_phase's (qs_gates.cu), so the state after the run is the state after
+// the gates one by one.  A run that would not save traffic (a lone gate, a
+// pair of controlled phases) keeps the streaming kernels, whose pair-index
+// remapping handles any stride.
 //
 // The layouts, the shared-memory swizzle (every access phase on distinct
 // banks) and the planner are in qs_lowstage.cuh.
@@ -111,20 +116,25 @@ __global__ void __launch_bounds__(kMaxThreads) k_lowstage(T *__restrict__ a, uin
 #pragma unroll
         for (int r = 0; r < 8; ++r) tile[pt ^ reg_off(r, pr)] = V{vr[r], vi[r]};
     };
+    // the thread's part of every copy offset (its chunks differ in the bits above)
+    const uint64_t cto = copy_thread_off<T>(t, K, R.qoff);
     for (uint64_t tl = blockIdx.x; tl < tiles; tl += gridDim.x) {
-        const uint64_t base = tl << K;
+        const uint64_t base = tile_base(tl, K, R.qpos);
         // HBM -> shared memory, 16-byte chunks
         if constexpr (sizeof(T) == 4) {
-            const float4 *src = reinterpret_cast<const float4 *>(a) + (base >> 1);
+            const float4 *src = reinterpret_cast<const float4 *>(a);
             float4 *dst = reinterpret_cast<float4 *>(lsm);
-            for (uint32_t c = t; c < TN / 2; c += blockDim.x) {
-                const float4 v = src[c];
+            uint32_t k = 0;
+            for (uint32_t c = t; c < TN / 2; c += blockDim.x, ++k) {
+                const float4 v = src[(base | cto | copy_chunk_off<T>(k, K, R.qoff)) >> 1];
                 const uint32_t p = phys<T>(2 * c);
                 dst[p >> 1] = (p & 1) ? make_float4(v.z, v.w, v.x, v.y) : v;
             }
         } else {
-            const double2 *src = reinterpret_cast<const double2 *>(a) + base;
-            for (uint32_t c = t; c < TN; c += blockDim.x) tile[phys<T>(c)] = src[c];
+            const double2 *src = reinterpret_cast<const double2 *>(a);
+            uint32_t k = 0;
+            for (uint32_t c = t; c < TN; c += blockDim.x, ++k)
+                tile[phys<T>(c)] = src[base | cto | copy_chunk_off<T>(k, K, R.qoff)];
         }
         __syncthreads();
         set_layout(0);
@@ -165,26 +175,30 @@ __global__ void __launch_bounds__(kMaxThreads) k_lowstage(T *__restrict__ a, uin
         __syncthreads();
         // shared memory -> HBM
         if constexpr (sizeof(T) == 4) {
-            float4 *dst = reinterpret_cast<float4 *>(a) + (base >> 1);
+            float4 *dst = reinterpret_cast<float4 *>(a);
             const float4 *src = reinterpret_cast<const float4 *>(lsm);
-            for (uint32_t c = t; c < TN / 2; c += blockDim.x) {
+            uint32_t k = 0;
+            for (uint32_t c = t; c < TN / 2; c += blockDim.x, ++k) {
                 const uint32_t p = phys<T>(2 * c);
                 const float4 v = src[p >> 1];
-                dst[c] = (p & 1) ? make_float4(v.z, v.w, v.x, v.y) : v;
+                dst[(base | cto | copy_chunk_off<T>(k, K, R.qoff)) >> 1] = (p & 1) ? make_float4(v.z, v.w, v.x, v.y) : v;
             }
         } else {
-            double2 *dst = reinterpret_cast<double2 *>(a) + base;
-            for (uint32_t c = t; c < TN; c += blockDim.x) dst[c] = tile[phys<T>(c)];
+            double2 *dst = reinterpret_cast<double2 *>(a);
+            uint32_t k = 0;
+            for (uint32_t c = t; c < TN; c += blockDim.x, ++k)
+                dst[base | cto | copy_chunk_off<T>(k, K, R.qoff)] = tile[phys<T>(c)];
         }
         __syncthreads();
     }
 }
 
 template <typename T>
-int launch_run(qs_state *s, const std::vector<qs_prim> &run, int K)
+int launch_run(qs_state *s, const std::vector<qs_prim> &run, const TileMap &M)
 {
+    const int K = M.K;
     Run<T> R;
-    plan_run(run, K, &R);
+    plan_run_on(run, M, s->n, &R);
     const uint64_t tiles = s->N >> K;
     // the tile, then per layout each thread's (tile offset, slot)
     const size_t smem = (sizeof(typename vec2<T>::type) << K) + sizeof(uint2) * R.nlayouts * (1u << (K - kRegBits));
@@ -200,18 +214,8 @@ int launch_run(qs_state *s, const std::vector<qs_prim> &run, int K)
 // this small).
 int qs_lowstage_bits(int n) { return n < kMinLowBits ? 0 : n < kLowBits ? n : kLowBits; }
 
-// Whether primitive p can join a staged run on an n-qubit state: its target
-// bits below the tile width (controls and phase masks may be anywhere).
-bool qs_lowstage_fits(const qs_prim &p, int n)
-{
-    const int K = qs_lowstage_bits(n);
-    if (!K) return false;
-    const uint64_t low = (1ull << K) - 1;
-    if (p.kind == QS_PRIM_PHASE) return true;
-    return ((p.holes & ~p.cmask) & ~low) == 0 && (p.off0 & ~low) == 0 && (p.off1 & ~low) == 0;
-}
-
-int qs_lowstage_max_run() { return kMaxRun; }
+// The qubits a primitive mixes (none for a phase): they must be tile qubits.
+static uint64_t prim_targets(const qs_prim &p) { return p.kind == QS_PRIM_PHASE ? 0 : (p.off0 | p.off1); }
 
 // HBM traffic of primitive p on the per-gate kernels, in full passes over the
 // state: the amplitudes it touches, counted in whole 32-byte sectors (4
@@ -232,12 +236,63 @@ double qs_lowstage_traffic(const qs_prim &p, int dtype)
     return 1.0 / (double)(1ull << halvings);
 }
 
-// Apply a run of primitives that all fit (qs_lowstage_fits) in one pass.
-int qs_launch_lowstage(qs_state *s, const std::vector<qs_prim> &run)
+// The passes of a lowered gate list on an n-qubit state of dtype: runs of
+// consecutive primitives whose targets, with the qubits of a 64-byte run of
+// the state (0..2 for complex64, 0..1 for complex128), fit K =
+// qs_lowstage_bits(n) qubits - at most kMaxRun each - staged in one
+// pass on the tile of those qubits and the lowest others (K in all), when
+// that moves fewer bytes than the gates one by one would, or when `stage_all`
+// (the CPU emulation's coverage); otherwise each primitive on its own.
+void qs_lowstage_passes(const std::vector<qs_prim> &prims, int n, int dtype, bool stage_all,
+                        std::vector<Pass> &out)
+{
+    out.clear();
+    const int K = qs_lowstage_bits(n);
+    if (!K) {
+        for (size_t i = 0; i < prims.size(); ++i) out.push_back({i, 1, 0});
+        return;
+    }
+    const uint64_t all = n >= 64 ? ~0ull : (1ull << n) - 1;
+    const uint64_t seed = (dtype == QS_C64 ? 7ull : 3ull) & all;
+    size_t first = 0;
+    uint64_t q = seed;
+    auto close = [&](size_t end) {
+        const size_t count = end - first;
+        if (!count) return;
+        double per_gate = 0;
+        for (size_t i = first; i < end; ++i) per_gate += qs_lowstage_traffic(prims[i], dtype);
+        if (stage_all || (count > 1 && per_gate > 1.0)) {
+            uint64_t m = q;
+            for (int b = 0; b < n && __builtin_popcountll(m) < K; ++b) m |= 1ull << b;
+            out.push_back({first, count, m});
+        } else {
+            for (size_t i = first; i < end; ++i) out.push_back({i, 1, 0});
+        }
+        first = end;
+        q = seed;
+    };
+    for (size_t i = 0; i < prims.size(); ++i) {
+        const uint64_t t = prim_targets(prims[i]);
+        if ((int)(i - first) == kMaxRun || __builtin_popcountll(q | t) > K) close(i);
+        q |= t;
+    }
+    close(prims.size());
+}
+
+// Apply a run of primitives whose targets lie in the qubits of qmask (K =
+// qs_lowstage_bits(n) of them, qubit 0 among them: a 16-byte copy then holds
+// two tile neighbours) in one pass.
+int qs_launch_lowstage(qs_state *s, const std::vector<qs_prim> &run, uint64_t qmask)
 {
     if (run.empty()) return QS_OK;
     if ((int)run.size() > kMaxRun) return qs_fail(QS_ERR_ARG, "staged run of %zu gates (at most %d)", run.size(), kMaxRun);
     const int K = qs_lowstage_bits(s->n);
     if (!K) return qs_fail(QS_ERR_ARG, "staged run on a %d-qubit state (at least %d qubits)", s->n, kMinLowBits);
-    return s->dtype == QS_C64 ? launch_run<float>(s, run, K) : launch_run<double>(s, run, K);
+    if (__builtin_popcountll(qmask) != K || !(qmask & 1ull) || (s->n < 64 && (qmask >> s->n)))
+        return qs_fail(QS_ERR_ARG, "staged run: tile qubits 0x%llx (%d of them, with qubit 0)",
+                       (unsigned long long)qmask, K);
+    for (const qs_prim &p : run)
+        if (prim_targets(p) & ~qmask) return qs_fail(QS_ERR_ARG, "staged run: a gate's targets are not tile qubits");
+    const TileMap M = {K, qmask};
+    return s->dtype == QS_C64 ? launch_run<float>(s, run, M) : launch_run<double>(s, run, M);
 }

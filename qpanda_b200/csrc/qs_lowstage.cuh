@@ -1,9 +1,17 @@
-// qs_lowstage.cuh - the plan of a staged low-qubit run (k_lowstage,
-// qs_lowstage.cu): register layouts, the shared-memory swizzle and the op
-// list.  Host code plus the two index helpers the kernel shares; included by
-// the kernel and by the CPU emulation of its index arithmetic.
+// qs_lowstage.cuh - the plan of a staged run (k_lowstage, qs_lowstage.cu):
+// the tile's qubits, register layouts, the shared-memory swizzle and the op
+// list.  Host code plus the index helpers the kernel shares; included by the
+// kernel and by the CPU emulation of its index arithmetic.
 //
-// A CTA owns a 2^K-amplitude tile; each of its 2^(K-3) threads holds 8
+// A tile is the 2^K amplitudes that agree on every qubit outside a set Q of K
+// qubits (qubit 0 always among them, and qubit 1 for complex64, so that the
+// copies move whole 32-byte sectors); tile bit k is the k-th qubit of Q in
+// ascending order.  A run is planned on its gates with every mask carried by
+// the tile map (the qubits of Q -> bits 0..K-1, the others -> K, K+1, ... in
+// ascending order), so below K every mask speaks of tile bits; a gate's
+// controls outside Q are a per-tile condition, in the state's own bits.
+//
+// A CTA owns a tile; each of its 2^(K-3) threads holds 8
 // amplitudes in registers.  A layout names the tile bit behind each of the 3
 // register index bits and each thread index bit: thread t's register r holds
 // tile index  tb(t) | rb(r),  tb / rb the deposits of t / r's bits at those
@@ -75,7 +83,76 @@ struct Run {
     int nlayouts;
     Layout L[kMaxRun + 1];
     Op<T> op[kMaxRun];
+    uint64_t qoff[kLowBits];     // 2^q of the tile's qubit q behind tile bit k
+    int8_t qpos[kLowBits];       // the tile's qubits, ascending
 };
+
+// The tile's qubits: the set bits of qmask (K of them), ascending.
+struct TileMap {
+    int K;
+    uint64_t qmask;
+};
+
+// A mask in the state's bits -> tile-map order (see the top of this file).
+inline uint64_t map_bits(uint64_t m, const TileMap &M, int n)
+{
+    uint64_t out = 0;
+    int lo = 0, hi = M.K;
+    for (int q = 0; q < n; ++q) {
+        const int to = ((M.qmask >> q) & 1) ? lo++ : hi++;
+        if ((m >> q) & 1) out |= 1ull << to;
+    }
+    return out;
+}
+
+// The inverse of map_bits.
+inline uint64_t unmap_bits(uint64_t m, const TileMap &M, int n)
+{
+    uint64_t out = 0;
+    int lo = 0, hi = M.K;
+    for (int q = 0; q < n; ++q) {
+        const int from = ((M.qmask >> q) & 1) ? lo++ : hi++;
+        if ((m >> from) & 1) out |= 1ull << q;
+    }
+    return out;
+}
+
+// State offset of tile tl's first amplitude: tl's bits spread over the
+// qubits outside the tile (zeros inserted at the tile's qubits).
+__host__ __device__ __forceinline__ uint64_t tile_base(uint64_t tl, int K, const int8_t *qpos)
+{
+    for (int j = 0; j < K; ++j) {
+        const uint64_t low = (1ull << qpos[j]) - 1;
+        tl = ((tl & ~low) << 1) | (tl & low);
+    }
+    return tl;
+}
+
+// The copies between the state and shared memory: thread t's chunk k is the
+// tile's chunk c = t + k 2^(K-3), a 16-byte vector (two complex64 amplitudes,
+// tile indices 2c and 2c + 1; or one complex128, tile index c).  Its state
+// offset from the tile base is copy_thread_off(t) | copy_chunk_off(k): the
+// thread's bits land on tile bits 1.. (complex64) or 0.. (complex128), k's on
+// the 2 (3) tile bits above them.
+template <typename T>
+__host__ __device__ __forceinline__ uint64_t copy_thread_off(uint32_t t, int K, const uint64_t *qoff)
+{
+    const int first = sizeof(T) == 4 ? 1 : 0;
+    uint64_t o = 0;
+    for (int j = 0; j < K - kRegBits; ++j)
+        if ((t >> j) & 1u) o |= qoff[first + j];
+    return o;
+}
+
+template <typename T>
+__host__ __device__ __forceinline__ uint64_t copy_chunk_off(uint32_t k, int K, const uint64_t *qoff)
+{
+    const int kb = sizeof(T) == 4 ? 2 : 3;
+    uint64_t o = 0;
+    for (int j = 0; j < kb; ++j)
+        if ((k >> j) & 1u) o |= qoff[K - kb + j];
+    return o;
+}
 
 template <typename T>
 __host__ __device__ constexpr int bank_row_bits() { return sizeof(T) == 4 ? 4 : 3; }
@@ -218,5 +295,37 @@ inline void plan_run(const std::vector<qs_prim> &run, int K, Run<T> *R)
         }
     }
 }
+
+// The plan of a run on the tile of qubits M.qmask of an n-qubit state: the
+// run's masks carried by the tile map, planned by plan_run, each op's
+// per-tile condition carried back to the state's bits.
+template <typename T>
+inline void plan_run_on(const std::vector<qs_prim> &run, const TileMap &M, int n, Run<T> *R)
+{
+    std::vector<qs_prim> loc(run);
+    for (qs_prim &p : loc) {
+        p.holes = map_bits(p.holes, M, n);
+        p.cmask = map_bits(p.cmask, M, n);
+        p.off0 = map_bits(p.off0, M, n);
+        p.off1 = map_bits(p.off1, M, n);
+    }
+    plan_run(loc, M.K, R);
+    for (int g = 0; g < R->count; ++g) R->op[g].need = unmap_bits(R->op[g].need, M, n);
+    int k = 0;
+    for (int q = 0; q < n && k < M.K; ++q)
+        if ((M.qmask >> q) & 1) {
+            R->qpos[k] = (int8_t)q;
+            R->qoff[k] = 1ull << q;
+            ++k;
+        }
+}
+
+// The passes of a lowered gate list (qs_lowstage_passes, qs_lowstage.cu):
+// prims [first, first + count) as one staged pass on the tile of qubits
+// qmask, or, with qmask 0, one per-gate launch each.
+struct Pass {
+    size_t first, count;
+    uint64_t qmask;
+};
 
 }  // namespace qs_low

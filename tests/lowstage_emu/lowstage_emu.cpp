@@ -1,11 +1,14 @@
 // lowstage_emu.cpp - CPU emulation of the staged low-qubit runs, for tests.
 //
 // Applies a gate list to a complex128 host state the way qs_gates_apply does
-// on the GPU: gates lowered by the library (qs_lower_gate), consecutive gates
-// that fit a staged tile (qs_lowstage_fits) collected into runs of up to
-// qs_low::kMaxRun, and each run moved exactly as k_lowstage
+// on the GPU: gates lowered by the library (qs_lower_gate), split into passes
+// by the library (qs_lowstage_passes: runs of consecutive gates whose targets
+// fit one tile's qubits), and each run moved exactly as k_lowstage
 // (qpanda_b200/csrc/qs_lowstage.cu) moves it: the plan from the library's own
-// planner (qs_low::plan_run), the 16-byte copies into the swizzled tile, each
+// planner (qs_low::plan_run_on), the tile bases and 16-byte copy offsets in
+// the state (qs_low::tile_base, copy_thread_off, copy_chunk_off: every
+// amplitude of the state copied in exactly once and out exactly once per
+// run), the copies into the swizzled tile, each
 // thread's 8 registers at  thread_off ^ reg_off  through phys, the register
 // pairs of every op kind, the predicates on low controls and masks, the
 // tile-uniform skip on high ones, and the round trips through shared memory
@@ -15,8 +18,8 @@
 // register write-back, every slot read exactly once per register read, and
 // the bank conflicts of every access phase (counted, not assumed: 16 lanes of
 // 8-byte accesses, or 8 lanes of 16-byte ones, on the slots they touch).
-// Runs are staged whatever their size (the library stages only runs that
-// save traffic); gates that do not fit are applied directly.
+// Runs are staged whatever their size (stage_all: the library stages only
+// runs that save traffic).
 //
 // Built by tests/test_lowstage_emulation.py against the library (host code
 // only runs; nvcc because the shared header holds device helpers):
@@ -32,7 +35,8 @@
 #include "qs_prim.h"
 
 int qs_lowstage_bits(int n);
-bool qs_lowstage_fits(const qs_prim &p, int n);
+void qs_lowstage_passes(const std::vector<qs_prim> &prims, int n, int dtype, bool stage_all,
+                        std::vector<qs_low::Pass> &out);
 
 namespace {
 
@@ -93,13 +97,17 @@ long long conflicts(const std::vector<int64_t> &slot_of_lane, int per_phase, int
 }
 
 template <typename T>
-int emulate_run(std::vector<cd> &a, int n, const std::vector<qs_prim> &run, Stats &st)
+int emulate_run(std::vector<cd> &a, int n, const std::vector<qs_prim> &run, uint64_t qmask, Stats &st)
 {
     using namespace qs_low;
     const int K = qs_lowstage_bits(n);
     if (K < kMinLowBits || K > kLowBits) return fail("tile width %lld out of range", K);
+    if (__builtin_popcountll(qmask) != K || !(qmask & 1) || (qmask >> n)) return fail("tile qubits 0x%llx", (long long)qmask);
+    for (const qs_prim &p : run)
+        if (p.kind == QS_PRIM_PAIR && ((p.off0 | p.off1) & ~qmask)) return fail("a gate's targets are not tile qubits");
     Run<T> R;
-    plan_run(run, K, &R);
+    const TileMap M = {K, qmask};
+    plan_run_on(run, M, n, &R);
     if (R.count != (int)run.size() || R.nlayouts < 1 || R.nlayouts > kMaxRun + 1) return fail("bad plan");
     const uint32_t TN = 1u << K;
     const int tbits = K - kRegBits;
@@ -151,7 +159,29 @@ int emulate_run(std::vector<cd> &a, int n, const std::vector<qs_prim> &run, Stat
         }
         return 0;
     };
-    for (uint64_t base = 0; base < a.size(); base += TN) {
+    // state offset of tile index i (the copies' view): chunk c = t + k threads
+    // of thread t holds tile indices 2c, 2c + 1 (complex64) or c (complex128)
+    std::vector<uint64_t> off(TN);
+    for (uint32_t t = 0; t < threads; ++t)
+        for (uint32_t k = 0; k < (sizeof(T) == 4 ? 4u : 8u); ++k) {
+            const uint64_t o = copy_thread_off<T>(t, K, R.qoff) | copy_chunk_off<T>(k, K, R.qoff);
+            const uint32_t c = t + k * threads;
+            if (sizeof(T) == 4) {
+                if (o & 1) return fail("16-byte copy at an odd amplitude (thread %lld, chunk %lld)", t, k);
+                off[2 * c] = o;
+                off[2 * c + 1] = o | 1;
+            } else {
+                off[c] = o;
+            }
+        }
+    std::vector<uint8_t> touched(a.size(), 0);
+    const uint64_t tiles = a.size() >> K;
+    for (uint64_t tl = 0; tl < tiles; ++tl) {
+        const uint64_t base = tile_base(tl, K, R.qpos);
+        for (uint32_t i = 0; i < TN; ++i) {
+            const uint64_t at = base | off[i];
+            if (at >= a.size() || touched[at]++) return fail("amplitude %lld copied twice or out of range", (long long)at);
+        }
         // HBM -> shared memory
         std::fill(wr.begin(), wr.end(), 0);
         if (sizeof(T) == 4) {
@@ -159,8 +189,8 @@ int emulate_run(std::vector<cd> &a, int n, const std::vector<qs_prim> &run, Stat
             for (uint32_t c = 0; c < TN / 2; ++c) {
                 const uint32_t p = phys<T>(2 * c);
                 const uint32_t s0 = (p >> 1) * 2;              // the float4 slot pair
-                slot[s0] = (p & 1) ? a[base + 2 * c + 1] : a[base + 2 * c];
-                slot[s0 + 1] = (p & 1) ? a[base + 2 * c] : a[base + 2 * c + 1];
+                slot[s0] = (p & 1) ? a[base | off[2 * c + 1]] : a[base | off[2 * c]];
+                slot[s0 + 1] = (p & 1) ? a[base | off[2 * c]] : a[base | off[2 * c + 1]];
                 if (wr[s0]++ || wr[s0 + 1]++) return fail("copy slot %lld written twice", s0);
                 lanes.push_back(p >> 1);
             }
@@ -170,7 +200,7 @@ int emulate_run(std::vector<cd> &a, int n, const std::vector<qs_prim> &run, Stat
             for (uint32_t c = 0; c < TN; ++c) {
                 const uint32_t s = phys<T>(c);
                 if (s >= TN || wr[s]++) return fail("copy slot %lld written twice", s);
-                slot[s] = a[base + c];
+                slot[s] = a[base | off[c]];
                 lanes.push_back(s);
             }
             st.copy_conflicts += conflicts(lanes, 8, 8);
@@ -219,8 +249,10 @@ int emulate_run(std::vector<cd> &a, int n, const std::vector<qs_prim> &run, Stat
         for (uint32_t i = 0; i < TN; ++i)
             if (wr[i] != 1) return fail("slot %lld not written back", i);
         // shared memory -> HBM
-        for (uint32_t i = 0; i < TN; ++i) a[base + i] = slot[phys<T>(i)];
+        for (uint32_t i = 0; i < TN; ++i) a[base | off[i]] = slot[phys<T>(i)];
     }
+    for (uint64_t i = 0; i < a.size(); ++i)
+        if (touched[i] != 1) return fail("amplitude %lld not in exactly one tile", (long long)i);
     ++st.runs;
     return 0;
 }
@@ -239,30 +271,53 @@ extern "C" int lowstage_emu_apply(double *amp, int n, const void *gates, int cou
     memcpy(a.data(), amp, sizeof(cd) * a.size());
     const qs_gate *g = static_cast<const qs_gate *>(gates);
     Stats st = {0, 0, 0, 0};
-    std::vector<qs_prim> run;
-    auto flush = [&]() -> int {
-        int r = 0;
-        if (!run.empty())
-            r = dtype == QS_C64 ? emulate_run<float>(a, n, run, st) : emulate_run<double>(a, n, run, st);
-        run.clear();
-        return r;
-    };
-    for (int i = 0; i < count; ++i) {
-        qs_prim p;
-        if (qs_lower_gate(n, &g[i], &p)) return fail("gate %lld does not lower", i);
-        if (qs_lowstage_fits(p, n)) {
-            run.push_back(p);
-            if ((int)run.size() == qs_low::kMaxRun && flush()) return 1;
-        } else {
-            if (flush()) return 1;
-            apply_direct(a, p);
+    std::vector<qs_prim> prims(count);
+    for (int i = 0; i < count; ++i)
+        if (qs_lower_gate(n, &g[i], &prims[i])) return fail("gate %lld does not lower", i);
+    std::vector<qs_low::Pass> passes;
+    qs_lowstage_passes(prims, n, dtype, true, passes);
+    size_t next = 0;
+    for (const qs_low::Pass &ps : passes) {
+        if (ps.first != next || ps.count < 1 || (int)ps.count > qs_low::kMaxRun)
+            return fail("passes do not cover the gate list in order (at %lld)", (long long)next);
+        next = ps.first + ps.count;
+        if (!ps.qmask) {
+            apply_direct(a, prims[ps.first]);
+            continue;
         }
+        std::vector<qs_prim> run(prims.begin() + ps.first, prims.begin() + ps.first + ps.count);
+        if (dtype == QS_C64 ? emulate_run<float>(a, n, run, ps.qmask, st)
+                            : emulate_run<double>(a, n, run, ps.qmask, st))
+            return 1;
     }
-    if (flush()) return 1;
+    if (next != (size_t)count) return fail("passes end at %lld", (long long)next);
     memcpy(amp, a.data(), sizeof(cd) * a.size());
     stats[0] = st.reg_conflicts;
     stats[1] = st.copy_conflicts;
     stats[2] = st.layout_switches;
     stats[3] = st.runs;
+    return 0;
+}
+
+// The passes qs_gates_apply makes for a gate list: out[0] staged passes,
+// out[1] per-gate launches, out[2] gates in staged passes.  Returns 0 or 1.
+extern "C" int lowstage_emu_passes(int n, const void *gates, int count, int dtype, long long *out)
+{
+    g_err[0] = 0;
+    const qs_gate *g = static_cast<const qs_gate *>(gates);
+    std::vector<qs_prim> prims(count);
+    for (int i = 0; i < count; ++i)
+        if (qs_lower_gate(n, &g[i], &prims[i])) return fail("gate %lld does not lower", i);
+    std::vector<qs_low::Pass> passes;
+    qs_lowstage_passes(prims, n, dtype, false, passes);
+    out[0] = out[1] = out[2] = 0;
+    for (const qs_low::Pass &ps : passes) {
+        if (ps.qmask) {
+            ++out[0];
+            out[2] += (long long)ps.count;
+        } else {
+            ++out[1];
+        }
+    }
     return 0;
 }

@@ -218,13 +218,15 @@ def _one_by_one(sv, gates):
 
 
 @pytest.mark.parametrize("dt", ["c128", "c64"])
-@pytest.mark.parametrize("n", [5, 6, 9, 10, 12, 18])
-def test_staged_low_qubit_runs_match_gate_by_gate(need_gpu, dt, n):
-    """qs_gates_apply runs consecutive gates on the lowest qubits through
-    shared memory in one pass (qs_lowstage.cu): the same state as the gates
-    one by one on the streaming kernels, and the oracle's within the usual
-    bar.  Random layers (rotations on qubits 0.. in order), the QFT (long runs
-    of controlled phases) and every gate kind with control lists."""
+@pytest.mark.parametrize("n", [5, 6, 9, 10, 12, 18, 20])
+def test_staged_runs_match_gate_by_gate(need_gpu, dt, n):
+    """qs_gates_apply runs consecutive gates whose targets share one tile's
+    10 qubits (any qubits, with the lowest ones) through shared memory and
+    registers in one pass (qs_lowstage.cu): the same state as the gates one
+    by one on the streaming kernels, and the oracle's within the usual bar.
+    Random layers (rotations on every qubit, CNOT / iSWAP on random pairs),
+    the QFT (long runs of controlled phases) and every gate kind with control
+    lists."""
     from tests.golden.make_golden import every_gate_circuit
     for g in (circuits.random_layers(n, 4, 70 + n, iswap_frac=0.3), circuits.qft(n),
               every_gate_circuit(n, 5 + n)):

@@ -1,8 +1,9 @@
-"""CPU check of the staged low-qubit runs' index arithmetic (no GPU).
+"""CPU check of the staged runs' index arithmetic (no GPU).
 
 tests/lowstage_emu/lowstage_emu.cpp moves every run of a gate list exactly as
-k_lowstage does - the library's own planner (register layouts, op kinds),
-the swizzled 16-byte copies, each thread's register slots, the round trips
+k_lowstage does - the library's own passes and planner (tile qubits, register
+layouts, op kinds), the tile bases and copy offsets in the state, the
+swizzled 16-byte copies, each thread's register slots, the round trips
 through shared memory at every layout switch - with FP64 arithmetic.  The
 result must match the oracle to rounding, every shared-memory slot must be
 written and read exactly once per phase, and no access phase may hit a bank
@@ -40,6 +41,8 @@ def emu(tmp_path_factory):
     E.lowstage_emu_apply.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_longlong)]
     E.lowstage_emu_apply.restype = C.c_int
     E.lowstage_emu_error.restype = C.c_char_p
+    E.lowstage_emu_passes.argtypes = [C.c_int, C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_longlong)]
+    E.lowstage_emu_passes.restype = C.c_int
     return E
 
 
@@ -93,3 +96,36 @@ def test_rotation_layer_needs_three_layout_switches(emu):
     err, (reg_conf, copy_conf, switches, runs) = run_emu(emu, n, g, C64)
     assert err < TOL[C64] and reg_conf == 0 and copy_conf == 0
     assert runs == 1 and switches == 3, (runs, switches)
+
+
+@pytest.mark.parametrize("dtype", [C64, C128])
+def test_runs_on_any_qubits(emu, dtype):
+    """Runs whose gates act on high qubits stage tiles of those qubits plus
+    the lowest ones: every amplitude copied in and out exactly once per run,
+    the oracle's state, no bank conflicts."""
+    n = 14
+    for k, g in enumerate((circuits.random_layers(n, 3, 500 + dtype, iswap_frac=0.3),
+                           every_gate_circuit(n, 77 + dtype))):
+        err, (reg_conf, copy_conf, switches, runs) = run_emu(emu, n, g, dtype)
+        assert err < TOL[dtype], (k, err)
+        assert runs > 0 and copy_conf == 0 and reg_conf == 0, (k, runs, copy_conf, reg_conf)
+
+
+def passes_of(E, n, g, dtype):
+    g = np.ascontiguousarray(g)
+    out = (C.c_longlong * 3)()
+    assert E.lowstage_emu_passes(n, g.ctypes.data, len(g), dtype, out) == 0, E.lowstage_emu_error().decode()
+    return list(out)
+
+
+def test_benchmark_circuits_run_in_few_passes(emu):
+    """The per-gate path's passes over the state (qs_gates_apply): the
+    20-qubit complex128 circuit (600 gates), the 32-qubit complex64 circuit
+    (768 gates) and the 28-qubit QFT (420 gates) each stage nearly every gate,
+    in runs of up to 24 whose targets share one tile."""
+    for n, g, dtype, most in ((20, circuits.random_layers(20, 20, 20240601), C128, 70),
+                              (32, circuits.random_layers(32, 16, 20240601, iswap_frac=0.1), C64, 110),
+                              (28, circuits.qft(28), C64, 25)):
+        staged, single, in_staged = passes_of(emu, n, g, dtype)
+        assert staged + single <= most, (n, staged, single)
+        assert in_staged >= 0.99 * len(g), (n, in_staged, len(g))
