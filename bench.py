@@ -1241,7 +1241,7 @@ def qft_line(args, n, steps, warmup, gpu_id=None):
         ss = statistics.mean(staged)
         out[dt] = {"circuit_s": cs, "hbm_gbs_effective": circuits.gate_bytes(gates, n, amp_b) / cs / 1e9,
                    "kernels": table, "staged_circuit_s": ss,
-                   "staged_note": "qs_gates_apply: runs of gates on qubits 0..9 in one shared-memory pass each"}
+                   "staged_note": "qs_gates_apply: runs of consecutive gates whose targets share one tile's 10 qubits, one staged pass each"}
         states[dt] = sv
     clk = clocks.stop() if clocks else None
     a, d = states["c64"], states["c128"]
