@@ -64,6 +64,35 @@ __device__ __forceinline__ void apply_pairs(T (&vr)[8], T (&vi)[8], const T (&m)
     }
 }
 
+// The pairs (r, r | B) of a 1-qubit gate with a diagonal matrix (FLIP =
+// false: x' = m00 x, y' = m11 y) or an anti-diagonal one (FLIP: x' = m01 y,
+// y' = m10 x): cmul_add2's arithmetic with the zero entries' products, exact
+// zeros there, left out.
+template <typename T, int B, bool FLIP, bool PRED>
+__device__ __forceinline__ void apply_sparse(T (&vr)[8], T (&vi)[8], const T (&m)[8], uint32_t tb,
+                                             const uint32_t (&rb)[kRegBits], uint32_t set)
+{
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+        if (r & B) continue;
+        if (PRED && ((tb | reg_off(r, rb)) & set) != set) continue;
+        const T ar = vr[r], ai = vi[r], br = vr[r | B], bi = vi[r | B];
+        // each output in the form cmul_add2 gives it when its first operand
+        // (r0) or its second (r1) is the zero entry
+        if (FLIP) {
+            vr[r] = fma(-m[3], bi, m[2] * br);
+            vi[r] = fma(m[3], br, m[2] * bi);
+            vr[r | B] = m[4] * ar - m[5] * ai;
+            vi[r | B] = m[4] * ai + m[5] * ar;
+        } else {
+            vr[r] = m[0] * ar - m[1] * ai;
+            vi[r] = m[0] * ai + m[1] * ar;
+            vr[r | B] = fma(-m[7], bi, m[6] * br);
+            vi[r | B] = fma(m[7], br, m[6] * bi);
+        }
+    }
+}
+
 template <typename T>
 __device__ __forceinline__ void apply_phase(T (&vr)[8], T (&vi)[8], T pr, T pi, uint32_t tb,
                                             const uint32_t (&rb)[kRegBits], uint32_t set)
@@ -152,9 +181,9 @@ __global__ void __launch_bounds__(kMaxThreads) k_lowstage(T *__restrict__ a, uin
 #pragma unroll
             for (int j = 0; j < 8; ++j) m[j] = op.m[j];
             const bool pred = op.set != 0;
-            switch (op.kind + (pred ? 16 : 0)) {
+            switch (op.kind + (pred ? OP_KINDS : 0)) {
             case OP_PHASE:
-            case OP_PHASE + 16: apply_phase(vr, vi, m[0], m[1], tb, rb, op.set); break;
+            case OP_PHASE + OP_KINDS: apply_phase(vr, vi, m[0], m[1], tb, rb, op.set); break;
 #define QS_LOW_PAIR_CASES(P, OFF)                                                             \
             case OFF + OP_1Q + 0: apply_pairs<T, 1, 0, 1, P>(vr, vi, m, tb, rb, op.set); break; \
             case OFF + OP_1Q + 1: apply_pairs<T, 2, 0, 2, P>(vr, vi, m, tb, rb, op.set); break; \
@@ -164,9 +193,15 @@ __global__ void __launch_bounds__(kMaxThreads) k_lowstage(T *__restrict__ a, uin
             case OFF + OP_EX + 2: apply_pairs<T, 6, 2, 4, P>(vr, vi, m, tb, rb, op.set); break; \
             case OFF + OP_EX + 3: apply_pairs<T, 3, 2, 1, P>(vr, vi, m, tb, rb, op.set); break; \
             case OFF + OP_EX + 4: apply_pairs<T, 5, 4, 1, P>(vr, vi, m, tb, rb, op.set); break; \
-            case OFF + OP_EX + 5: apply_pairs<T, 6, 4, 2, P>(vr, vi, m, tb, rb, op.set); break;
+            case OFF + OP_EX + 5: apply_pairs<T, 6, 4, 2, P>(vr, vi, m, tb, rb, op.set); break; \
+            case OFF + OP_DIAG + 0: apply_sparse<T, 1, false, P>(vr, vi, m, tb, rb, op.set); break; \
+            case OFF + OP_DIAG + 1: apply_sparse<T, 2, false, P>(vr, vi, m, tb, rb, op.set); break; \
+            case OFF + OP_DIAG + 2: apply_sparse<T, 4, false, P>(vr, vi, m, tb, rb, op.set); break; \
+            case OFF + OP_FLIP + 0: apply_sparse<T, 1, true, P>(vr, vi, m, tb, rb, op.set); break; \
+            case OFF + OP_FLIP + 1: apply_sparse<T, 2, true, P>(vr, vi, m, tb, rb, op.set); break; \
+            case OFF + OP_FLIP + 2: apply_sparse<T, 4, true, P>(vr, vi, m, tb, rb, op.set); break;
             QS_LOW_PAIR_CASES(false, 0)
-            QS_LOW_PAIR_CASES(true, 16)
+            QS_LOW_PAIR_CASES(true, OP_KINDS)
 #undef QS_LOW_PAIR_CASES
             default: break;
             }

@@ -59,8 +59,11 @@ constexpr int kMaxThreads = 1 << (kLowBits - kRegBits);
 // op kinds: a phase; a pair on register bit k (1 + k); an exchange pair whose
 // members have register bit ja and jb set, (ja, jb) = (0,1), (0,2), (1,2),
 // (1,0), (2,0), (2,1) (4 .. 9) - both orders, so that the arithmetic is
-// k_pair's operand for operand
-enum : uint8_t { OP_PHASE = 0, OP_1Q = 1, OP_EX = 4 };
+// k_pair's operand for operand; a pair on register bit k whose matrix is
+// diagonal (10 + k: RZ, a phase on the target) or anti-diagonal (13 + k: X,
+// Y, the CNOT and Toffoli targets), which skip the products with its zero
+// entries (k_pair adds them as exact zeros)
+enum : uint8_t { OP_PHASE = 0, OP_1Q = 1, OP_EX = 4, OP_DIAG = 10, OP_FLIP = 13, OP_KINDS = 16 };
 
 struct Layout {
     uint16_t rb[kRegBits];                   // tile offset (a power of two) of register index bit j
@@ -280,7 +283,10 @@ inline void plan_run(const std::vector<qs_prim> &run, int K, Run<T> *R)
             p.need = q.cmask & ~low;
             p.set = (uint32_t)(q.cmask & low);
             if (q.off0 == 0) {
-                p.kind = (uint8_t)(OP_1Q + reg_of(__builtin_ctzll(q.off1)));
+                const int rk = reg_of(__builtin_ctzll(q.off1));
+                const bool diag = q.m[2] == 0 && q.m[3] == 0 && q.m[4] == 0 && q.m[5] == 0;
+                const bool flip = q.m[0] == 0 && q.m[1] == 0 && q.m[6] == 0 && q.m[7] == 0;
+                p.kind = (uint8_t)((diag ? OP_DIAG : flip ? OP_FLIP : OP_1Q) + rk);
             } else {
                 static const int8_t ex_kind[3][3] = {{0, 0, 1}, {3, 0, 2}, {4, 5, 0}};
                 p.kind = (uint8_t)(OP_EX + ex_kind[reg_of(__builtin_ctzll(q.off0))][reg_of(__builtin_ctzll(q.off1))]);

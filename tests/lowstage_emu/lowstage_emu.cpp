@@ -222,6 +222,14 @@ int emulate_run(std::vector<cd> &a, int n, const std::vector<qs_prim> &run, uint
             } else if (op.kind < OP_EX) {
                 HB = B1 = 1 << (op.kind - OP_1Q);
                 B0 = 0;
+            } else if (op.kind >= OP_DIAG && op.kind < OP_FLIP + 3) {
+                // the full 2x2 on the pair: its zero entries must be zeros
+                const bool flip = op.kind >= OP_FLIP;
+                HB = B1 = 1 << (op.kind - (flip ? OP_FLIP : OP_DIAG));
+                B0 = 0;
+                const int z0 = flip ? 0 : 2, z1 = flip ? 6 : 4;
+                if (op.m[z0] != 0 || op.m[z0 + 1] != 0 || op.m[z1] != 0 || op.m[z1 + 1] != 0)
+                    return fail("op %lld: nonzero entries off its sparse pattern", g);
             } else {
                 static const int ex[6][2] = {{1, 2}, {1, 4}, {2, 4}, {2, 1}, {4, 1}, {4, 2}};
                 if (op.kind - OP_EX >= 6) return fail("bad op kind %lld", op.kind);
