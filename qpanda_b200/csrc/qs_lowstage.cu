@@ -112,9 +112,10 @@ __global__ void __launch_bounds__(kMaxThreads) k_lowstage(T *__restrict__ a, uin
     typedef typename vec2<T>::type V;
     extern __shared__ __align__(16) unsigned char lsm[];
     V *tile = reinterpret_cast<V *>(lsm);
-    const uint32_t TN = 1u << K;
     const int tbits = K - kRegBits;
     const uint32_t t = threadIdx.x;
+    // 16-byte chunks per thread: the tile's 2^K amplitudes over 2^(K-3) threads
+    constexpr uint32_t kChunks = sizeof(T) == 4 ? 4 : 8;
     // per layout, this thread's tile offset and its slot: computed once per CTA
     uint2 *lt = reinterpret_cast<uint2 *>(lsm + (sizeof(V) << K));
     for (int l = 0; l < R.nlayouts; ++l) {
@@ -149,21 +150,26 @@ __global__ void __launch_bounds__(kMaxThreads) k_lowstage(T *__restrict__ a, uin
     const uint64_t cto = copy_thread_off<T>(t, K, R.qoff);
     for (uint64_t tl = blockIdx.x; tl < tiles; tl += gridDim.x) {
         const uint64_t base = tile_base(tl, K, R.qpos);
-        // HBM -> shared memory, 16-byte chunks
+        // HBM -> shared memory, 16-byte chunks: all of a thread's chunks
+        // loaded before any is stored (their loads in flight together)
         if constexpr (sizeof(T) == 4) {
             const float4 *src = reinterpret_cast<const float4 *>(a);
             float4 *dst = reinterpret_cast<float4 *>(lsm);
-            uint32_t k = 0;
-            for (uint32_t c = t; c < TN / 2; c += blockDim.x, ++k) {
-                const float4 v = src[(base | cto | copy_chunk_off<T>(k, K, R.qoff)) >> 1];
-                const uint32_t p = phys<T>(2 * c);
-                dst[p >> 1] = (p & 1) ? make_float4(v.z, v.w, v.x, v.y) : v;
+            float4 v[kChunks];
+#pragma unroll
+            for (uint32_t k = 0; k < kChunks; ++k) v[k] = src[(base | cto | copy_chunk_off<T>(k, K, R.qoff)) >> 1];
+#pragma unroll
+            for (uint32_t k = 0; k < kChunks; ++k) {
+                const uint32_t p = phys<T>(2 * (t + k * blockDim.x));
+                dst[p >> 1] = (p & 1) ? make_float4(v[k].z, v[k].w, v[k].x, v[k].y) : v[k];
             }
         } else {
             const double2 *src = reinterpret_cast<const double2 *>(a);
-            uint32_t k = 0;
-            for (uint32_t c = t; c < TN; c += blockDim.x, ++k)
-                tile[phys<T>(c)] = src[base | cto | copy_chunk_off<T>(k, K, R.qoff)];
+            double2 v[kChunks];
+#pragma unroll
+            for (uint32_t k = 0; k < kChunks; ++k) v[k] = src[base | cto | copy_chunk_off<T>(k, K, R.qoff)];
+#pragma unroll
+            for (uint32_t k = 0; k < kChunks; ++k) tile[phys<T>(t + k * blockDim.x)] = v[k];
         }
         __syncthreads();
         set_layout(0);
@@ -212,17 +218,17 @@ __global__ void __launch_bounds__(kMaxThreads) k_lowstage(T *__restrict__ a, uin
         if constexpr (sizeof(T) == 4) {
             float4 *dst = reinterpret_cast<float4 *>(a);
             const float4 *src = reinterpret_cast<const float4 *>(lsm);
-            uint32_t k = 0;
-            for (uint32_t c = t; c < TN / 2; c += blockDim.x, ++k) {
-                const uint32_t p = phys<T>(2 * c);
+#pragma unroll
+            for (uint32_t k = 0; k < kChunks; ++k) {
+                const uint32_t p = phys<T>(2 * (t + k * blockDim.x));
                 const float4 v = src[p >> 1];
                 dst[(base | cto | copy_chunk_off<T>(k, K, R.qoff)) >> 1] = (p & 1) ? make_float4(v.z, v.w, v.x, v.y) : v;
             }
         } else {
             double2 *dst = reinterpret_cast<double2 *>(a);
-            uint32_t k = 0;
-            for (uint32_t c = t; c < TN; c += blockDim.x, ++k)
-                dst[base | cto | copy_chunk_off<T>(k, K, R.qoff)] = tile[phys<T>(c)];
+#pragma unroll
+            for (uint32_t k = 0; k < kChunks; ++k)
+                dst[base | cto | copy_chunk_off<T>(k, K, R.qoff)] = tile[phys<T>(t + k * blockDim.x)];
         }
         __syncthreads();
     }
