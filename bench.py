@@ -1225,8 +1225,8 @@ def qft_line(args, n, steps, warmup, gpu_id=None):
             table[kind_of[op]] = {"launches_per_circuit": len(ts) // steps, "mean_ms": t * 1e3,
                                   "gbs": gbs, "frac": gbs / peak}
         cs = statistics.mean(circ)
-        # the same gates through qs_gates_apply: runs on the low qubits staged
-        # in shared memory, one pass each (the state it leaves is the one above)
+        # the same gates through qs_gates_apply: runs of gates that share one
+        # tile's qubits staged, one pass each (the state it leaves is the one above)
         staged = []
         for k in range(warmup + steps):
             sv.set_state(host)
@@ -1390,6 +1390,9 @@ def run_kernels(args):
     run = circuits.make_gates([("RY", (q,), 0.2 * q) for q in range(10)])
     timed("k_lowstage: 10 rotations on qubits 0..9 (one pass)",
           lambda: check(L.qs_gates_apply(h, C.c_void_p(run.ctypes.data), len(run))), 2 * S * N)
+    run_hi = circuits.make_gates([("RY", (q,), 0.2 * q) for q in range(n - 7, n)])
+    timed(f"k_lowstage: 7 rotations on qubits {n - 7}..{n - 1} (one pass; tile qubits 0..2 and {n - 7}..{n - 1})",
+          lambda: check(L.qs_gates_apply(h, C.c_void_p(run_hi.ctypes.data), len(run_hi))), 2 * S * N)
     qs20 = np.arange(20, dtype=np.int32)
     dev = torch.empty(1 << 20, dtype=torch.float64, device="cuda")
     timed("k_marginal_direct: qubits 0..19 (the sampler's first levels)",
