@@ -433,7 +433,8 @@ def run_b200(args):
     clk = clocks.stop()
     barrier(ws)
     elapsed = max_over_ranks(start.elapsed_time(end) / 1e3, ws, device=f"cuda:{local}")
-    launches = args.steps * (1 + (nb if path == "fused" else ng))
+    # fused: reset, the passes, and the plan's closing norm check (k_norm_fix)
+    launches = args.steps * (1 + (nb + 1 if path == "fused" else ng))
     circuit_s = elapsed / args.steps
 
     peak, peak_kind = peaks()
@@ -453,7 +454,7 @@ def run_b200(args):
     ot = timed_steps(L, h, gates, plan, 1, stream, torch, okinds, other)[0]
     odom = max(okinds, key=lambda k: sum(okinds[k]))
     o_ach = dom_bytes / statistics.mean(okinds[odom]) / 1e9
-    other_line = {"circuit_s": ot, "launches": (nb if other == "fused" else ng) + 1,
+    other_line = {"circuit_s": ot, "launches": (nb + 1 if other == "fused" else ng) + 1,
                   "hbm_gbs_effective": ((nb * dom_bytes) if other == "fused"
                                         else circuits.gate_bytes(gates, n, amp_b)) / ot / 1e9,
                   "dominant_kernel": odom, "dominant_gbs": o_ach, "dominant_frac": o_ach / peak,

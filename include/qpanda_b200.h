@@ -271,9 +271,14 @@ int qs_plan_block(const qs_plan *plan, size_t i, int *k, int *qubits, double *ma
  * without tiled passes or i out of range.  No reference counterpart:
  * introspection of this backend's fusion plan. */
 int qs_plan_pass(const qs_plan *plan, size_t i, int *n_blocks, int *tile_qubits, int *block_qubits);
-/* Apply every block in order (asynchronous, on the state's stream). */
+/* Apply every block in order (asynchronous, on the state's stream).  The
+ * norm is kept to the input's: each pass rescales by the drift of the one
+ * before, and after the last pass the state is rescaled on the device when
+ * its norm differs from the input's by more than 2^-21 relative. */
 int qs_plan_apply(qs_state *s, qs_plan *plan);
-/* Apply launches (passes) [first, first + count) only (for timing or interleaving). */
+/* Apply launches (passes) [first, first + count) only (for timing or
+ * interleaving); a range that ends at the plan's last pass ends with the
+ * closing rescale. */
 int qs_plan_apply_range(qs_state *s, qs_plan *plan, size_t first, size_t count);
 /* Synchronize and report whether a bounded wait inside a fused pass expired
  * since the last qs_plan_apply (QS_ERR_STATE) - a watchdog, not expected. */

@@ -28,7 +28,12 @@
 // partial per CTA).  The truncating FP32 accumulation of the tensor cores
 // loses ~3e-7 of the norm per pass, always in the same direction; the next
 // pass rescales its input by sqrt(N0 / N_prev), N0 being the input norm of the
-// plan's first pass, so the drift does not build up over a circuit.
+// plan's first pass, so the drift does not build up over a circuit.  That
+// leaves the last pass's own drift, which the split products' rounding makes
+// coherent when a circuit undoes an earlier one (a plan and then its inverse
+// lost 1.3e-5 of the norm at 32 qubits); k_norm_fix, launched after a plan's
+// last pass, scales the state by sqrt(N0 / N_last) when the two differ by
+// more than 2^-21 relative, deciding on the device.
 #include <cuda_bf16.h>
 
 #include "qs_common.cuh"
@@ -321,7 +326,52 @@ __global__ void __launch_bounds__(kThreads, 4) k_fused_tc(float *__restrict__ am
     }
 }
 
+// Every CTA sums the two sets of partials in the same fixed order and gets
+// the same factor; nothing is written when the norms agree within kNormTol.
+constexpr double kNormTol = 1.0 / (1 << 21);
+constexpr int kFixThreads = 256;
+
+__global__ void __launch_bounds__(kFixThreads) k_norm_fix(float4 *amp, uint64_t n4, const double *n0p,
+                                                          const double *nlp, int nparts)
+{
+    __shared__ float s_c;
+    if (threadIdx.x < 32) {
+        double a = 0.0, b = 0.0;
+        for (int i = threadIdx.x; i < nparts; i += 32) { a += n0p[i]; b += nlp[i]; }
+        for (int o = 16; o > 0; o >>= 1) {
+            a += __shfl_xor_sync(0xffffffffu, a, o);
+            b += __shfl_xor_sync(0xffffffffu, b, o);
+        }
+        if (threadIdx.x == 0) s_c = (a > 0.0 && b > 0.0 && fabs(b / a - 1.0) > kNormTol) ? (float)sqrt(a / b) : 0.f;
+    }
+    __syncthreads();
+    const float c = s_c;
+    if (c == 0.f) return;
+    const uint64_t stride = (uint64_t)gridDim.x * kFixThreads;
+    uint64_t i = (uint64_t)blockIdx.x * kFixThreads + threadIdx.x;
+    for (; i + 3 * stride < n4; i += 4 * stride) {
+        float4 v[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) v[k] = amp[i + k * stride];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) amp[i + k * stride] = make_float4(v[k].x * c, v[k].y * c, v[k].z * c, v[k].w * c);
+    }
+    for (; i < n4; i += stride) {
+        const float4 v = amp[i];
+        amp[i] = make_float4(v.x * c, v.y * c, v.z * c, v.w * c);
+    }
+}
+
 }  // namespace
+
+int qs_launch_norm_fix(qs_state *s, const double *norm0, const double *last_out, int nparts)
+{
+    if (s->dtype != QS_C64) return QS_OK;
+    k_norm_fix<<<QS_SM_COUNT * 4, kFixThreads, 0, s->stream>>>(static_cast<float4 *>(s->amp), s->N / 2, norm0,
+                                                              last_out, nparts);
+    QS_LAUNCH_CHECK("k_norm_fix");
+    return QS_OK;
+}
 
 int qs_fused_grid(const qs_state *s)
 {

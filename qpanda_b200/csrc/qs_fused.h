@@ -19,6 +19,12 @@ struct qs_fused_desc {
 // CTAs of one fused pass on s (the number of norm partials per pass).
 int qs_fused_grid(const qs_state *s);
 
+// After a plan's last pass: scales the state by sqrt(sum(norm0) /
+// sum(last_out)) when the two sums (nparts partials each) differ by more than
+// 2^-21 relative, decided on the device; complex64 states only (no-op
+// otherwise).
+int qs_launch_norm_fix(qs_state *s, const double *norm0, const double *last_out, int nparts);
+
 // Launch one block on a complex64 state (n >= 12) on the state's stream.
 // err_dev: device int set to 1 if a bounded wait inside the kernel expired.
 int qs_launch_fused(qs_state *s, const qs_fused_desc *d, int *err_dev);

@@ -903,6 +903,9 @@ extern "C" int qs_plan_apply_range(qs_state *s, qs_plan *P, size_t first, size_t
             if (r == QS_ERR_UNSUPPORTED) r = qs_launch_tiled(s, &d, flag);
             if (r) return r;
         }
+        // the rescale of each pass leaves only the last pass's drift
+        if (count && first + count == plan_launches(P))
+            return qs_launch_norm_fix(s, norm, norm + GT * (1 + (first + count - 1) % 2), GT);
         return QS_OK;
     }
     for (size_t b = first; b < first + count; ++b) {
@@ -915,6 +918,8 @@ extern "C" int qs_plan_apply_range(qs_state *s, qs_plan *P, size_t first, size_t
         d.out_parts = norm + G * (1 + b % 2);
         if ((r = qs_launch_fused(s, &d, flag))) return r;
     }
+    if (count && first + count == plan_launches(P))
+        return qs_launch_norm_fix(s, norm, norm + G * (1 + (first + count - 1) % 2), G);
     return QS_OK;
 }
 
