@@ -393,8 +393,9 @@ int qs_batch_autotune_cached(int n_circuits, const int *n_qubits, const qs_gate 
  * reference has no counterpart (it caps programs at 30 qubits,
  * QPandaAPI.cpp:87).
  * A process holds some of the shards (ranks[0..n_ranks), on the current
- * device): two local shards swap with device copies; a shard whose partner is
- * elsewhere calls `exchange` for each piece (at most 256 MB) of its half:
+ * device): two local shards swap in place with one kernel; a shard whose
+ * partner is elsewhere swaps with it over peer memory (qs_sharded_set_peer)
+ * or calls `exchange` for each piece (at most 256 MB) of its half:
  * send `bytes` of device memory at `send` to shard `partner`, receive as many
  * from it into `recv` (distinct device buffers of the library), and return 0
  * once `recv` holds them - e.g. an NCCL send/receive pair on `stream`
@@ -407,6 +408,21 @@ int qs_sharded_create(int n_qubits, int n_global, int dtype, const int *ranks, i
                       qs_exchange_fn exchange, void *ctx, qs_sharded **out);
 /* Apply gate records (logical qubits); synchronous at every swap. */
 int qs_sharded_apply(qs_sharded *s, const qs_gate *gates, size_t count);
+/* Peer swaps with shard `partner`, whose amplitudes this process can address
+ * at `partner_amp`: a peer GPU's buffer (peer access enabled) or an IPC
+ * mapping (cudaIpcOpenMemHandle) of another process's shard, 16-byte aligned
+ * (qs_device_ptr of that shard, exported by its owner).  A swap with that
+ * partner then runs as one kernel on each side that reads and writes both
+ * halves in place - over NVLink when the partner is another GPU - with no
+ * staging buffer, packing or exchange call: the side with the rank bit 0
+ * swaps the first half of the rows, the other side the second.  Before and
+ * after each such swap this side calls barrier(ctx, shard, partner), which
+ * returns 0 once the partner has made the same call (this side's earlier work
+ * on its shard is complete before the first call, its part of the swap before
+ * the second).  Replaces the exchange function for that partner.  The
+ * reference has no counterpart. */
+typedef int (*qs_barrier_fn)(void *ctx, int shard, int partner);
+int qs_sharded_set_peer(qs_sharded *s, int partner, void *partner_amp, qs_barrier_fn barrier, void *ctx);
 /* The local shard with these rank bits (a qs_state of n - g qubits). */
 int qs_sharded_shard(qs_sharded *s, int rank, qs_state **shard);
 /* pos[q] = physical position of logical qubit q (n entries). */

@@ -12,13 +12,16 @@
 // p = 1 - b and receives the partner's half with local bit p = b into the same
 // place.  The schedule is the one qpanda_b200/sharded.py computes.
 //
-// Transport: two local shards swap halves with device copies (cudaMemcpy2D
-// for a strided half) through one staging buffer; a shard whose partner lives
-// in another process packs its half into a staging buffer and hands both
-// buffers to the caller's exchange function (NCCL send/receive, peer copies,
-// MPI ...), in chunks of at most 256 MB, then unpacks what it received.  The
-// reference has no counterpart: it caps programs at 30 qubits
-// (QPandaAPI.cpp:87).
+// Transport: two local shards swap halves in place with one kernel
+// (qs_swap.cu: each element pair read and written once, no staging); a
+// partner whose shard this process can address (a peer GPU's buffer, or an
+// IPC mapping of another process's shard, registered with
+// qs_sharded_set_peer) is swapped with the same kernel over NVLink, each side
+// taking half of the rows between two calls of the caller's barrier; any
+// other partner's half goes through the caller's exchange function (NCCL
+// send/receive, MPI ...): packed into a staging buffer in chunks of at most
+// 256 MB, and what comes back unpacked.  The reference has no counterpart: it
+// caps programs at 30 qubits (QPandaAPI.cpp:87).
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -27,6 +30,7 @@
 
 #include "qs_common.cuh"
 #include "qs_prim.h"
+#include "qs_swap.h"
 
 namespace {
 
@@ -119,8 +123,16 @@ int schedule(int n, int g, const qs_gate *gates, size_t count, std::vector<int> 
 
 }  // namespace
 
+struct qs_sharded_peer {
+    int partner = -1;
+    void *amp = nullptr;                     // the partner shard's amplitudes, addressable here
+    qs_barrier_fn barrier = nullptr;
+    void *ctx = nullptr;
+};
+
 struct qs_sharded {
     int n = 0, g = 0, L = 0, dtype = QS_C64;
+    std::vector<qs_sharded_peer> peers;
     std::vector<int> ranks;                  // rank bits of the local shards
     std::vector<qs_state *> shards;
     std::vector<int> pos;
@@ -193,23 +205,52 @@ int piece_copy(char *dst, size_t dpitch, const char *src, size_t spitch, const P
 
 int swap_local_pair(qs_sharded *S, qs_state *s0, qs_state *s1, int p)
 {
-    // s0 has rank bit 0: its half p = 1 goes to s1, s1's half p = 0 comes back
+    // s0 has rank bit 0: its half p = 1 trades places with s1's half p = 0
     const Half a = half_of(S, s0, p, 1), b = half_of(S, s1, p, 0);
-    std::vector<Piece> pcs;
-    pieces_of(a, pcs);
-    int r = ensure_stage(S, std::min(kChunkBytes, a.width * a.rows));
-    if (r) return r;
     cudaStream_t st = s0->stream;
     QS_CUDA_TRY(cudaStreamSynchronize(s1->stream));
-    char *tmp = static_cast<char *>(S->stage[0]);
-    for (const Piece &c : pcs) {
-        if ((r = piece_copy(tmp, c.w, piece_base(a, c), a.pitch, c, st))) return r;
-        if ((r = piece_copy(piece_base(a, c), a.pitch, piece_base(b, c), b.pitch, c, st))) return r;
-        if ((r = piece_copy(piece_base(b, c), b.pitch, tmp, c.w, c, st))) return r;
-    }
+    int r = qs_launch_swap_halves(a.base, b.base, a.width, a.pitch, 0, a.rows, 0, a.width, st);
+    if (r) return r;
     QS_CUDA_TRY(cudaStreamSynchronize(st));
     S->bytes += 2 * a.width * a.rows;
     return QS_OK;
+}
+
+// The partner's shard is addressable from here: this side swaps its share of
+// the element pairs (the rank-bit-0 side the first half of the rows, or of the
+// single row) in place, between two barriers with the partner.
+int swap_peer(qs_sharded *S, size_t i, int j, int p, const qs_sharded_peer &peer)
+{
+    qs_state *s = S->shards[i];
+    const int rank = S->ranks[i], partner = rank ^ (1 << j);
+    const int b = (rank >> j) & 1;
+    const Half mine = half_of(S, s, p, 1 - b);
+    char *theirs = static_cast<char *>(peer.amp) + (b ? mine.width : 0);
+    size_t r0 = 0, nr = mine.rows, c0 = 0, w = mine.width;
+    if (mine.rows >= 2) {
+        nr = mine.rows / 2;
+        r0 = b ? nr : 0;
+    } else {
+        w = mine.width / 2;
+        c0 = b ? w : 0;
+    }
+    QS_CUDA_TRY(cudaStreamSynchronize(s->stream));
+    if (peer.barrier(peer.ctx, rank, partner))
+        return qs_fail(QS_ERR_STATE, "sharded: barrier with shard %d before a swap failed", partner);
+    int r = qs_launch_swap_halves(mine.base, theirs, mine.width, mine.pitch, r0, nr, c0, w, s->stream);
+    if (r) return r;
+    QS_CUDA_TRY(cudaStreamSynchronize(s->stream));
+    if (peer.barrier(peer.ctx, rank, partner))
+        return qs_fail(QS_ERR_STATE, "sharded: barrier with shard %d after a swap failed", partner);
+    S->bytes += 2 * nr * w;
+    return QS_OK;
+}
+
+const qs_sharded_peer *find_peer(const qs_sharded *S, int partner)
+{
+    for (const qs_sharded_peer &q : S->peers)
+        if (q.partner == partner) return &q;
+    return nullptr;
 }
 
 int swap_remote(qs_sharded *S, size_t i, int j, int p)
@@ -300,17 +341,45 @@ extern "C" int qs_sharded_apply(qs_sharded *S, const qs_gate *gates, size_t coun
             if (it != S->ranks.end()) {
                 if (rank & (1 << st.j)) continue;      // the pair is handled from its rank-bit-0 member
                 r = swap_local_pair(S, S->shards[i], S->shards[it - S->ranks.begin()], st.p);
+            } else if (const qs_sharded_peer *pe = find_peer(S, partner)) {
+                r = swap_peer(S, i, st.j, st.p, *pe);
             } else if (S->exchange) {
                 r = swap_remote(S, i, st.j, st.p);
             } else {
-                r = qs_fail(QS_ERR_ARG, "sharded: shard %d's partner %d is not local and no exchange was given",
-                            rank, partner);
+                r = qs_fail(QS_ERR_ARG, "sharded: shard %d's partner %d is not local, not a peer, and no exchange "
+                            "was given", rank, partner);
             }
             if (r) return r;
         }
         ++S->swaps;
     }
     S->pos = pos;
+    return QS_OK;
+}
+
+extern "C" int qs_sharded_set_peer(qs_sharded *S, int partner, void *partner_amp, qs_barrier_fn barrier,
+                                   void *ctx)
+{
+    if (!S || !partner_amp || !barrier) return qs_fail(QS_ERR_ARG, "qs_sharded_set_peer: null argument");
+    if (partner < 0 || partner >= (1 << S->g))
+        return qs_fail(QS_ERR_ARG, "qs_sharded_set_peer: shard %d out of range", partner);
+    if (std::find(S->ranks.begin(), S->ranks.end(), partner) != S->ranks.end())
+        return qs_fail(QS_ERR_ARG, "qs_sharded_set_peer: shard %d is local", partner);
+    if ((uintptr_t)partner_amp % 16)
+        return qs_fail(QS_ERR_ARG, "qs_sharded_set_peer: shard %d's amplitudes are not 16-byte aligned", partner);
+    for (qs_sharded_peer &q : S->peers)
+        if (q.partner == partner) {
+            q.amp = partner_amp;
+            q.barrier = barrier;
+            q.ctx = ctx;
+            return QS_OK;
+        }
+    qs_sharded_peer q;
+    q.partner = partner;
+    q.amp = partner_amp;
+    q.barrier = barrier;
+    q.ctx = ctx;
+    S->peers.push_back(q);
     return QS_OK;
 }
 

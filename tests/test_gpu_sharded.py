@@ -1,7 +1,11 @@
 """GPU: a sharded state with its shards in one process on one GPU (the
 exchange as device copies), against the oracle on the whole state.  Ranks on
 separate GPUs exchange through NCCL with the same code (NcclExchanger), which
-tests/test_sharded.py runs on gloo ranks; this pool gives one GPU per run."""
+tests/test_sharded.py runs on gloo ranks; this pool gives one GPU per run.
+The C ABI's driver is tested with all shards local (in-place swap kernel),
+with one qs_sharded per host thread exchanging through a caller function,
+and with peer swaps over the partner's memory (one in-place kernel per side,
+the partner's buffer standing in for a peer GPU's)."""
 import numpy as np
 import pytest
 
@@ -118,6 +122,9 @@ def mailbox(tmp_path_factory):
     E.mailbox_run.restype = C.c_int
     E.mailbox_run.argtypes = [C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_size_t, C.c_void_p,
                               C.POINTER(C.c_int), C.POINTER(C.c_size_t)]
+    E.peer_run.restype = C.c_int
+    E.peer_run.argtypes = [C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_size_t, C.c_void_p,
+                           C.POINTER(C.c_int), C.POINTER(C.c_size_t), C.POINTER(C.c_size_t)]
     return E
 
 
@@ -143,4 +150,45 @@ def test_c_abi_sharded_exchange_function(need_gpu, mailbox, n, g_bits, dt, tol):
     assert swaps.value > 0
     shards = np.split(out.astype(np.complex128), 1 << g_bits)
     got = gather_logical(shards, n, g_bits, list(pos))
+    assert np.abs(got - _sharded_reference(n, gates)).max() < tol
+
+
+@pytest.mark.parametrize("dt,tol", [("c128", 1e-12), ("c64", 1e-5)])
+@pytest.mark.parametrize("n,g_bits", [(14, 1), (15, 2), (13, 3)])
+def test_c_abi_sharded_peer_swaps(need_gpu, mailbox, n, g_bits, dt, tol):
+    """One qs_sharded per shard in its own host thread, every other shard
+    registered as a peer (qs_sharded_set_peer): each swap is one in-place
+    kernel per side over the partner's memory (a peer GPU's, or an IPC mapping,
+    in a multi-GPU job; another buffer of this GPU here), the rank-bit-0 side
+    taking the first half of the rows, or of the single row when the swapped
+    position is the top local one.  The result equals the oracle's and, bit for
+    bit, the exchange-function path's; each side moves half of its half-slice
+    per swap, both ways."""
+    import ctypes as C
+
+    from qpanda_b200.capi import QS_C64, QS_C128
+    gates = np.ascontiguousarray(_circuit(n, 190 + n))
+    code = QS_C64 if dt == "c64" else QS_C128
+    npdt = np.complex64 if dt == "c64" else np.complex128
+    outs = []
+    for run in ("peer", "mailbox"):
+        out = np.empty((1 << g_bits) << (n - g_bits), dtype=npdt)
+        pos = np.empty(n, dtype=np.int32)
+        swaps, moved = C.c_size_t(), C.c_size_t()
+        if run == "peer":
+            rc = mailbox.peer_run(n, g_bits, code, gates.ctypes.data, len(gates), out.ctypes.data,
+                                  pos.ctypes.data_as(C.POINTER(C.c_int)), C.byref(swaps), C.byref(moved))
+            assert rc == 0, rc
+            assert swaps.value > 0
+            amp = 8 if dt == "c64" else 16
+            assert moved.value == swaps.value * (amp << (n - g_bits)) // 2, (moved.value, swaps.value)
+        else:
+            rc = mailbox.mailbox_run(n, g_bits, code, gates.ctypes.data, len(gates), out.ctypes.data,
+                                     pos.ctypes.data_as(C.POINTER(C.c_int)), C.byref(swaps))
+            assert rc == 0, rc
+        outs.append((out, list(pos)))
+    (a, pa), (b, pb) = outs
+    assert pa == pb and np.array_equal(a, b)
+    shards = np.split(a.astype(np.complex128), 1 << g_bits)
+    got = gather_logical(shards, n, g_bits, pa)
     assert np.abs(got - _sharded_reference(n, gates)).max() < tol
