@@ -31,7 +31,7 @@ def _newer(src_list, target):
 
 
 CXX = os.environ.get("CXX_HOST", "g++")
-CXXFLAGS = ["-O2", "-std=c++17", "-fPIC", "-Wall", "-I" + os.path.join(ROOT, "include"),
+CXXFLAGS = ["-O3", "-std=c++17", "-fPIC", "-Wall", "-I" + os.path.join(ROOT, "include"),
             "-I/usr/local/cuda/include"]
 
 

@@ -35,25 +35,6 @@ uint64_t remap(uint64_t mask, const int *q, int k)
     return r;
 }
 
-// Apply a primitive (already remapped to local bit positions) to a k-qubit vector.
-void apply_local(const qs_prim &p, cd *v, int k)
-{
-    const uint64_t N = 1ull << k;
-    if (p.kind == QS_PRIM_PHASE) {
-        cd ph(p.m[0], p.m[1]);
-        for (uint64_t i = 0; i < N; ++i)
-            if ((i & p.holes) == p.holes) v[i] *= ph;
-        return;
-    }
-    cd m00(p.m[0], p.m[1]), m01(p.m[2], p.m[3]), m10(p.m[4], p.m[5]), m11(p.m[6], p.m[7]);
-    for (uint64_t i = 0; i < N; ++i) {
-        if ((i & p.holes) != p.cmask) continue;     // base: hole bits zero except controls
-        cd a = v[i | p.off0], b = v[i | p.off1];
-        v[i | p.off0] = m00 * a + m01 * b;
-        v[i | p.off1] = m10 * a + m11 * b;
-    }
-}
-
 uint16_t bf16_bits(float f)
 {
     uint32_t u;
@@ -257,23 +238,72 @@ Groups closure_groups(const std::vector<size_t> &idx, const std::vector<uint64_t
 }
 
 // Block unitary: qubits q[0..4] ascending (global), gates applied in order.
+// U starts as the identity and each gate acts on its rows, all 32 columns at
+// once (column c gets exactly the operations the gates would apply to e_c), in
+// plain real arithmetic: each gate's masks are mapped to the block once, and
+// no complex multiply goes through the library's checked routine.
 void block_unitary(PlanBlock &B, const std::vector<qs_prim> &prim)
 {
-    B.U.assign(32 * 32, cd(0, 0));
-    std::vector<cd> col(32);
-    for (int c = 0; c < 32; ++c) {
-        std::fill(col.begin(), col.end(), cd(0, 0));
-        col[c] = 1;
-        for (size_t gi : B.gates) {
-            qs_prim lp = prim[gi];
-            lp.holes = remap(lp.holes, B.q, 5);
-            lp.cmask = remap(lp.cmask, B.q, 5);
-            lp.off0 = remap(lp.off0, B.q, 5);
-            lp.off1 = remap(lp.off1, B.q, 5);
-            apply_local(lp, col.data(), 5);
+    double re[32][32], im[32][32];
+    for (int r = 0; r < 32; ++r)
+        for (int c = 0; c < 32; ++c) {
+            re[r][c] = r == c ? 1.0 : 0.0;
+            im[r][c] = 0.0;
         }
-        for (int r = 0; r < 32; ++r) B.U[r * 32 + c] = col[r];
+    for (size_t gi : B.gates) {
+        const qs_prim &p = prim[gi];
+        const uint64_t holes = remap(p.holes, B.q, 5);
+        if (p.kind == QS_PRIM_PHASE) {
+            const double pr = p.m[0], pi = p.m[1];
+            for (int r = 0; r < 32; ++r) {
+                if ((r & holes) != holes) continue;
+                for (int c = 0; c < 32; ++c) {
+                    const double a = re[r][c], b = im[r][c];
+                    re[r][c] = a * pr - b * pi;
+                    im[r][c] = a * pi + b * pr;
+                }
+            }
+            continue;
+        }
+        const uint64_t cmask = remap(p.cmask, B.q, 5), off0 = remap(p.off0, B.q, 5), off1 = remap(p.off1, B.q, 5);
+        const double *m = p.m;                       // m00, m01, m10, m11 as (re, im)
+        // a plain exchange of the two rows (NOT, CNOT, SWAP, Toffoli, CSWAP):
+        // the products with 1 and 0 below would give exactly the swapped rows
+        const bool exchange = m[0] == 0 && m[1] == 0 && m[6] == 0 && m[7] == 0 && m[2] == 1 && m[3] == 0 &&
+                              m[4] == 1 && m[5] == 0;
+        const bool diagonal = m[2] == 0 && m[3] == 0 && m[4] == 0 && m[5] == 0;
+        for (int i = 0; i < 32; ++i) {
+            if ((i & holes) != cmask) continue;
+            double *ar = re[i | off0], *ai = im[i | off0], *br = re[i | off1], *bi = im[i | off1];
+            if (exchange) {
+                for (int c = 0; c < 32; ++c) {
+                    std::swap(ar[c], br[c]);
+                    std::swap(ai[c], bi[c]);
+                }
+                continue;
+            }
+            if (diagonal) {                          // RZ and the like: the zero products add nothing
+                for (int c = 0; c < 32; ++c) {
+                    const double xr = ar[c], xi = ai[c], yr = br[c], yi = bi[c];
+                    ar[c] = m[0] * xr - m[1] * xi;
+                    ai[c] = m[0] * xi + m[1] * xr;
+                    br[c] = m[6] * yr - m[7] * yi;
+                    bi[c] = m[6] * yi + m[7] * yr;
+                }
+                continue;
+            }
+            for (int c = 0; c < 32; ++c) {
+                const double xr = ar[c], xi = ai[c], yr = br[c], yi = bi[c];
+                ar[c] = (m[0] * xr - m[1] * xi) + (m[2] * yr - m[3] * yi);
+                ai[c] = (m[0] * xi + m[1] * xr) + (m[2] * yi + m[3] * yr);
+                br[c] = (m[4] * xr - m[5] * xi) + (m[6] * yr - m[7] * yi);
+                bi[c] = (m[4] * xi + m[5] * xr) + (m[6] * yi + m[7] * yr);
+            }
+        }
     }
+    B.U.resize(32 * 32);
+    for (int r = 0; r < 32; ++r)
+        for (int c = 0; c < 32; ++c) B.U[r * 32 + c] = cd(re[r][c], im[r][c]);
 }
 
 // Widen a mask to `want` qubits with the lowest free qubits of `pool`.
@@ -1026,7 +1056,12 @@ int qs_plan_rebind(const qs_plan *proto, const qs_gate *gates, size_t count, qs_
     P->opts = proto->opts;
     P->gates.assign(gates, gates + count);
     P->passes = proto->passes;
-    P->blocks = proto->blocks;
+    P->blocks.resize(proto->blocks.size());
+    for (size_t b = 0; b < proto->blocks.size(); ++b) {    // the structure; unitaries are rebuilt below
+        P->blocks[b].k = proto->blocks[b].k;
+        std::copy(proto->blocks[b].q, proto->blocks[b].q + 5, P->blocks[b].q);
+        P->blocks[b].gates = proto->blocks[b].gates;
+    }
     std::vector<qs_prim> prim;
     std::vector<uint64_t> mask;
     int r = lower_all(P, prim, mask);
