@@ -19,6 +19,7 @@
 #include <cstring>
 #include <functional>
 #include <map>
+#include <memory>
 #include <string>
 #include <thread>
 #include <vector>
@@ -766,13 +767,17 @@ extern "C" int qs_batch_create(int n_circ, const int *n_qubits, const qs_gate *g
     }
     std::vector<BatchCirc> hc(n_circ);
     if (!r) {
-        std::vector<uint16_t> hm(mat_total);
-        parallel(n_circ, [&](int c) {
-            for (size_t b = 0; b < plans[c]->blocks.size(); ++b)
-                qs_plan_block_bf16(plans[c], b, hm.data() + mat_off[c] + b * 2 * 64 * 64);
+        // BF16 conversion on the host threads (into a buffer every element of
+        // which it writes, so left uninitialised) while this thread allocates
+        std::unique_ptr<uint16_t[]> hm(new uint16_t[std::max<size_t>(mat_total, 1)]);
+        std::thread convert([&] {
+            parallel(n_circ, [&](int c) {
+                for (size_t b = 0; b < plans[c]->blocks.size(); ++b)
+                    qs_plan_block_bf16(plans[c], b, hm.get() + mat_off[c] + b * 2 * 64 * 64);
+            });
         });
         e = cudaMalloc(&B->d_states, B->state_bytes);
-        if (e == cudaSuccess) e = cudaMalloc(&B->d_mats, std::max<size_t>(hm.size() * 2, 16));
+        if (e == cudaSuccess) e = cudaMalloc(&B->d_mats, std::max<size_t>(mat_total * 2, 16));
         if (e == cudaSuccess) e = cudaMalloc(&B->d_layouts, std::max<size_t>(layouts.size() * sizeof(Layout), 16));
         if (e == cudaSuccess) e = cudaMalloc(&B->d_loads, std::max<size_t>(loads.size() * sizeof(LoadMap), 16));
         if (e == cudaSuccess && want_tmem)
@@ -781,7 +786,8 @@ extern "C" int qs_batch_create(int n_circ, const int *n_qubits, const qs_gate *g
         if (e == cudaSuccess) e = cudaMalloc(&B->d_order, sizeof(int32_t) * n_circ);
         if (e == cudaSuccess) e = cudaMalloc((void **)&B->d_zz, std::max<size_t>(B->zz_count, 1) * sizeof(double));
         if (e == cudaSuccess) e = cudaMalloc((void **)&B->d_head, 2 * sizeof(int32_t));
-        if (e == cudaSuccess) e = cudaMemcpy(B->d_mats, hm.data(), hm.size() * 2, cudaMemcpyHostToDevice);
+        convert.join();
+        if (e == cudaSuccess) e = cudaMemcpy(B->d_mats, hm.get(), mat_total * 2, cudaMemcpyHostToDevice);
         if (e == cudaSuccess && !layouts.empty())
             e = cudaMemcpy(B->d_layouts, layouts.data(), layouts.size() * sizeof(Layout), cudaMemcpyHostToDevice);
         if (e == cudaSuccess && !loads.empty())
