@@ -1432,6 +1432,35 @@ def run_kernels(args):
     b = Batch(sweep)
     timed("k_batch: 512 circuits of 10-22 qubits", lambda: b.run(), sweep_bytes(sweep))
     b.close()
+    # the plan of a circuit and then of its inverse: the state returns to |0..0>
+    # and the inverse plan's closing rescale (k_norm_fix) restores the norm its
+    # last pass drifted
+    fwd = circuits.random_layers(n, 16, SEED + 1, iswap_frac=0.1)
+    inv = np.array(fwd[::-1], copy=True)
+    inv["dagger"] ^= 1
+    pf, pi = FusionPlan(n, fwd), FusionPlan(n, inv)
+    npass = pf.num_launches() + pi.num_launches()
+    timed(f"round trip: a 16-layer circuit's plan and its inverse's ({npass} passes, then k_norm_fix)",
+          lambda: (pf.apply(sv), pi.apply(sv), None)[2], 2 * S * N * npass)
+    pf.close()
+    pi.close()
+    # a sharded state: two local shards of n - 1 qubits; a gate on the qubit at
+    # the global position first swaps it in (k_swap_halves: each shard trades
+    # half of its slice in place), then runs on both shards
+    ranks = np.arange(2, dtype=np.int32)
+    hs = C.c_void_p()
+    check(L.qs_sharded_create(n, 1, 0, ranks.ctypes.data_as(C.POINTER(C.c_int)), 2, None, None, C.byref(hs)))
+    spos = np.empty(n, dtype=np.int32)
+
+    def global_gate():
+        check(L.qs_sharded_positions(hs, spos.ctypes.data_as(C.POINTER(C.c_int))))
+        q = int(np.nonzero(spos == n - 1)[0][0])
+        gg = circuits.make_gates([("RY", (q,), 0.3)])
+        check(L.qs_sharded_apply(hs, C.c_void_p(gg.ctypes.data), 1))
+
+    timed(f"k_swap_halves + k_pair: a gate on the global qubit of {n} qubits over 2 local shards "
+          f"(one in-place swap of half of each shard, then the gate)", global_gate, 2 * S * N // 2 + 2 * S * N)
+    L.qs_sharded_destroy(hs)
     other.close()
     sv.close()
     print(json.dumps({"workload": f"kernels-{n}q-c64", "peak_gbs": peak, "peak_source": peak_kind,

@@ -113,6 +113,7 @@ def lib():
         "qs_sharded_apply": (i, [vp, vp, sz]),
         "qs_sharded_shard": (i, [vp, i, C.POINTER(vp)]),
         "qs_sharded_positions": (i, [vp, ip]),
+        "qs_sharded_set_peer": (i, [vp, i, vp, vp, vp]),
         "qs_sharded_info": (i, [vp, C.POINTER(sz), C.POINTER(sz)]),
         "qs_sharded_destroy": (i, [vp]),
         "qs_release_spare": (i, [vp]),
