@@ -19,7 +19,6 @@
 #include <cstring>
 #include <functional>
 #include <map>
-#include <memory>
 #include <string>
 #include <thread>
 #include <vector>
@@ -767,15 +766,6 @@ extern "C" int qs_batch_create(int n_circ, const int *n_qubits, const qs_gate *g
     }
     std::vector<BatchCirc> hc(n_circ);
     if (!r) {
-        // BF16 conversion on the host threads (into a buffer every element of
-        // which it writes, so left uninitialised) while this thread allocates
-        std::unique_ptr<uint16_t[]> hm(new uint16_t[std::max<size_t>(mat_total, 1)]);
-        std::thread convert([&] {
-            parallel(n_circ, [&](int c) {
-                for (size_t b = 0; b < plans[c]->blocks.size(); ++b)
-                    qs_plan_block_bf16(plans[c], b, hm.get() + mat_off[c] + b * 2 * 64 * 64);
-            });
-        });
         e = cudaMalloc(&B->d_states, B->state_bytes);
         if (e == cudaSuccess) e = cudaMalloc(&B->d_mats, std::max<size_t>(mat_total * 2, 16));
         if (e == cudaSuccess) e = cudaMalloc(&B->d_layouts, std::max<size_t>(layouts.size() * sizeof(Layout), 16));
@@ -786,8 +776,49 @@ extern "C" int qs_batch_create(int n_circ, const int *n_qubits, const qs_gate *g
         if (e == cudaSuccess) e = cudaMalloc(&B->d_order, sizeof(int32_t) * n_circ);
         if (e == cudaSuccess) e = cudaMalloc((void **)&B->d_zz, std::max<size_t>(B->zz_count, 1) * sizeof(double));
         if (e == cudaSuccess) e = cudaMalloc((void **)&B->d_head, 2 * sizeof(int32_t));
-        convert.join();
-        if (e == cudaSuccess) e = cudaMemcpy(B->d_mats, hm.get(), mat_total * 2, cudaMemcpyHostToDevice);
+        // The block matrices as BF16: a run of consecutive circuits at a time
+        // is converted on the host threads into one of two pinned buffers
+        // while the other's copy to the device is in flight.
+        constexpr size_t kPerBlock = 2 * 64 * 64;     // BF16 values of one block (hi, lo)
+        size_t chunk = 32ull << 20;                    // bytes per pinned buffer, at least one circuit's
+        for (int c = 0; c < n_circ; ++c) chunk = std::max(chunk, plans[c]->blocks.size() * kPerBlock * 2);
+        uint16_t *pin[2] = {nullptr, nullptr};
+        cudaEvent_t copied[2] = {nullptr, nullptr};
+        cudaStream_t up = nullptr;
+        if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&up, cudaStreamNonBlocking);
+        for (int k = 0; k < 2 && e == cudaSuccess; ++k) {
+            e = cudaHostAlloc((void **)&pin[k], chunk, cudaHostAllocDefault);
+            if (e == cudaSuccess) e = cudaEventCreateWithFlags(&copied[k], cudaEventDisableTiming);
+        }
+        bool in_flight[2] = {false, false};
+        for (int c0 = 0, k = 0; c0 < n_circ && e == cudaSuccess; k ^= 1) {
+            int c1 = c0;
+            while (c1 < n_circ && (mat_off[c1] + plans[c1]->blocks.size() * kPerBlock - mat_off[c0]) * 2 <= chunk) ++c1;
+            if (in_flight[k] && (e = cudaEventSynchronize(copied[k])) != cudaSuccess) break;
+            uint16_t *buf = pin[k];
+            const size_t base = mat_off[c0];
+            parallel(c1 - c0, [&](int i) {
+                const int c = c0 + i;
+                for (size_t b = 0; b < plans[c]->blocks.size(); ++b)
+                    qs_plan_block_bf16(plans[c], b, buf + (mat_off[c] - base) + b * kPerBlock);
+            });
+            const size_t elems = (c1 < n_circ ? mat_off[c1] : mat_total) - base;
+            if (elems) {
+                e = cudaMemcpyAsync(static_cast<uint16_t *>(B->d_mats) + base, buf, elems * 2, cudaMemcpyHostToDevice, up);
+                if (e == cudaSuccess) e = cudaEventRecord(copied[k], up);
+                in_flight[k] = e == cudaSuccess;
+            }
+            c0 = c1;
+        }
+        if (up) {
+            const cudaError_t e2 = cudaStreamSynchronize(up);
+            if (e == cudaSuccess) e = e2;
+        }
+        for (int k = 0; k < 2; ++k) {
+            if (copied[k]) cudaEventDestroy(copied[k]);
+            if (pin[k]) cudaFreeHost(pin[k]);
+        }
+        if (up) cudaStreamDestroy(up);
         if (e == cudaSuccess && !layouts.empty())
             e = cudaMemcpy(B->d_layouts, layouts.data(), layouts.size() * sizeof(Layout), cudaMemcpyHostToDevice);
         if (e == cudaSuccess && !loads.empty())
