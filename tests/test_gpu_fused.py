@@ -66,6 +66,17 @@ def test_fused_every_gate_kind(need_gpu, kernel):
     check_fused(12, every_gate_circuit(12, 9), init=random_state(12, 3), kernel=kernel)
 
 
+@pytest.mark.parametrize("kernel", KERNELS)
+@pytest.mark.parametrize("max_k", [3, 4])
+def test_fusion_width_below_five(need_gpu, kernel, max_k):
+    """Blocks of at most 3 or 4 qubits (fusion width 4 is the batch
+    autotuner's other choice), applied as widened 5-qubit blocks."""
+    n = 17
+    g = np.concatenate([circuits.random_layers(n, 6, 600 + max_k, iswap_frac=0.2),
+                        circuits.vqe_ansatz(n, 2, seed=max_k)])
+    check_fused(n, g, init=random_state(n, 50 + max_k), kernel=kernel, max_k=max_k)
+
+
 @pytest.mark.parametrize("max_sub", [1, 2, 3])
 @pytest.mark.parametrize("low", [1, 3, 5])
 def test_tiled_options(need_gpu, max_sub, low):

@@ -282,3 +282,19 @@ def test_tmem_layout_shape_of_the_32q_bench_plan(emu):
     assert vec.value >= 20, vec.value                       # 11 before the write order favoured the stores
     assert st.value / passes <= 80, st.value / passes       # 120 lines per warp and tile before
     assert cp.value / passes <= 72, cp.value / passes
+
+
+@pytest.mark.parametrize("remap", [0, 1])
+@pytest.mark.parametrize("max_k", [2, 3, 4])
+def test_fusion_width_below_five(emu, max_k, remap):
+    """Blocks of at most 2, 3 or 4 qubits (4 is the batch autotuner's other
+    fusion width), widened to 5-qubit blocks: both tiled kernels' index math
+    with the widened block unitaries reproduces the oracle."""
+    n = 16
+    g = np.concatenate([circuits.random_layers(n, 6, 500 + max_k, iswap_frac=0.2), circuits.vqe_ansatz(n, 2, seed=max_k)])
+    init = random_state(n, 40 + max_k)
+    err, npass = run_emu(emu, n, g, init, remap, max_k=max_k)
+    assert npass >= 2 and err < 1e-10, err
+    err, took, left, _, cclash, xclash = run_tmem_emu(emu, n, g, init, remap, max_k=max_k)
+    assert err < 1e-10 and took > 0 and left == 0, err
+    assert cclash == 0 and xclash == 0
